@@ -1,0 +1,369 @@
+#!/usr/bin/env python
+"""Benchmark of toaster's GPU path-tracing path on B200: Mpaths/s on the mixed scene.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload: the mixed scene (2,048 seeded triangles + 128 spheres, 50/30/20 diffuse / metal /
+dielectric, 16 emissive triangles, 1024x512 FP32 sky with a 0.5-degree sun of radiance 1e4) at
+1280x720, 64 samples per pixel, 8 bounces. One step = one full frame (921,600 pixels x 64 paths).
+
+`value` is device time (CUDA events on the library's stream) over exactly K frames with the
+scene resident in HBM; L2 is flushed (a 256 MiB write) before every timed frame. `e2e` is the
+same metric through the public C ABI with host buffers: each step uploads the scene records
+from pinned host memory (the library rebuilds the hierarchy and the environment tables),
+renders, and reads the float4 image back into pinned host memory; it is timed with the host
+clock. Multi-GPU runs are independent replicas (the path has no cross-rank exchange).
+`--impl reference` times the oracle (a C++ restatement of the reference CPU renderer, the
+reference itself being Rust that cannot be built here) on all host threads over a strided row
+sample of the same frame.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "Mpaths/s (1280x720, 8 bounces)"
+UNIT = "Mpaths/s"
+WORKLOAD = ("mixed scene: 2,048 seeded triangles + 128 spheres (50/30/20 diffuse/metal/dielectric, 16 emissive "
+            "triangles), 1024x512 FP32 sky + 0.5-degree sun (1e4), 1280x720, 64 spp, 8 bounces")
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--cpu-seconds", type=float, default=10.0, help="target wall time of one CPU sample")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def dist_env():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def measured_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        try:
+            d = json.loads(p.read_text())
+            return float(d["hbm_gbs"]), "measured"
+        except Exception:
+            pass
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.device = device_index
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            out, _ = self.proc.communicate(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+            out, _ = self.proc.communicate()
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in out.strip().splitlines():
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = max(mx, float(parts[2]))
+            except ValueError:
+                continue
+            for name, flag in zip(names, parts[5:9]):
+                if flag.lower() == "active":
+                    reasons.add(name)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_sample(scene, target_seconds: float, threads: int = 0):
+    """Times the oracle on evenly strided rows sized to about `target_seconds` of wall time."""
+    import oracle
+
+    o = oracle.Oracle(scene)
+    h, w, spp = scene.height, scene.width, scene.samples
+    t0 = time.perf_counter()
+    o.render(seed=1, rows=(h // 2, h // 2 + 1), row_step=1, threads=threads)
+    probe = time.perf_counter() - t0
+    rows_wanted = max(2, min(h, int(target_seconds / max(probe, 1e-4))))
+    step = max(1, h // rows_wanted)
+    t0 = time.perf_counter()
+    mean, _, counts = o.render(seed=2, rows=(0, h), row_step=step, threads=threads, counts=True)
+    dt = time.perf_counter() - t0
+    nrows = mean.shape[0]
+    paths = nrows * w * spp
+    return {
+        "mpaths_s": paths / dt / 1e6,
+        "seconds": dt,
+        "paths": paths,
+        "rows": nrows,
+        "row_step": step,
+        "cores": oracle.binding.num_threads() if threads <= 0 else threads,
+        "counts": [int(c) for c in counts],
+    }
+
+
+def algorithmic_bytes_per_ray(counts):
+    """Reference traversal work per ray: child boxes tested (root + 2 per interior visit) x 32 B,
+    triangle tests x 36 B (v0, e1, e2), sphere tests x 16 B (centre, radius), counted by the
+    oracle's ordered traversal over the frame's own ray mix (primary, bounce and shadow rays)."""
+    rays, _, spheres, tris, interior, _ = counts
+    return ((rays + 2 * interior) * 32 + tris * 36 + spheres * 16) / max(rays, 1)
+
+
+def run_reference(args):
+    world, rank, _ = dist_env()
+    if rank != 0:
+        return 0
+    from toaster_b200 import configs
+    import oracle
+
+    scene = configs.mixed()
+    samples = []
+    for i in range(args.warmup + args.steps):
+        s = cpu_sample(scene, args.cpu_seconds if i >= args.warmup else min(2.0, args.cpu_seconds))
+        if i >= args.warmup:
+            samples.append(s)
+    value = statistics.median([s["mpaths_s"] for s in samples])
+    line = {
+        "impl": "reference",
+        "metric": METRIC,
+        "value": value,
+        "unit": UNIT,
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": statistics.median([s["seconds"] * 1e3 for s in samples]),
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic",
+        "config": {"workload": WORKLOAD, "width": 1280, "height": 720, "spp": 64, "max_bounces": 8},
+        "cpu_baseline": {
+            "value": value, "unit": UNIT, "cores": samples[0]["cores"], "kind": "port",
+            "sample": f"every {samples[0]['row_step']}th row ({samples[0]['rows']} rows x 1280 px x 64 spp) per step; "
+                      "oracle = C++ restatement of crates/toaster-cpu (reference is Rust, unbuildable here)"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def pinned_copy(arr, keep):
+    import numpy as np
+    import torch
+
+    if arr is None:
+        return None
+    t = torch.empty(max(arr.nbytes, 1), dtype=torch.uint8, pin_memory=True)
+    keep.append(t)
+    view = t.numpy()[: arr.nbytes].view(arr.dtype).reshape(arr.shape)
+    view[...] = arr
+    return view
+
+
+def run_ours(args):
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+
+    from toaster_b200 import build, configs
+    from toaster_b200.renderer import GpuRenderer
+    from toaster_b200.scene import SceneGpuData, scene_to_gpu
+
+    world, rank, local = dist_env()
+    if world > 1:
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        dist.init_process_group("nccl", device_id=torch.device("cuda", local),
+                                timeout=__import__("datetime").timedelta(seconds=300))
+    torch.cuda.set_device(local)
+    build.build()
+    scene = configs.mixed()
+    data = scene_to_gpu(scene)
+    w, h, spp = scene.width, scene.height, scene.samples
+    paths_per_step = w * h * spp
+
+    r = GpuRenderer(local)
+    stream = torch.cuda.Stream(device=local)
+    r.set_stream(stream.cuda_stream)
+    r.upload(data)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local}")
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    for i in range(args.warmup):
+        r.render(frame_index=0)
+    torch.cuda.synchronize()
+
+    # ---------------- device-timed steps (scene resident)
+    clocks = ClockSampler(local)
+    barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    step_ms, kernel_ms, rays = [], [], []
+    for k in range(args.steps):
+        with torch.cuda.stream(stream):
+            flush.zero_()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        r.render(frame_index=0)
+        e1.record(stream)
+        e1.synchronize()
+        step_ms.append(e0.elapsed_time(e1))
+        st = r.stats()
+        kernel_ms.append(st["kernel_ms"])
+        rays.append(st["rays"])
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    barrier()
+    total_ms = sum(step_ms)
+    if world > 1:
+        t = torch.tensor([total_ms], dtype=torch.float64, device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    value = world * paths_per_step * args.steps / (total_ms * 1e-3) / 1e6
+
+    # ---------------- end-to-end through the C ABI with pinned host buffers
+    keep = []
+    pinned = SceneGpuData(**{k: pinned_copy(v, keep) if isinstance(v, np.ndarray) else v
+                             for k, v in data.__dict__.items()})
+    h2d = pinned.host_bytes()
+    out = pinned_copy(np.zeros((h, w, 4), np.float32), keep)
+    d2h = out.nbytes
+    r2 = GpuRenderer(local)
+    r2.upload(pinned)
+    r2.render(frame_index=0)
+    r2.readback(out)
+    barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for k in range(args.steps):
+        r2.upload(pinned)
+        r2.render(frame_index=0)
+        r2.readback(out)
+    e2e_s = time.perf_counter() - t0
+    barrier()
+    if world > 1:
+        t = torch.tensor([e2e_s], dtype=torch.float64, device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e_value = world * paths_per_step * args.steps / e2e_s / 1e6
+    assert np.all(np.isfinite(out)), "non-finite pixels in the benchmark image"
+    r2.close()
+
+    line = None
+    if rank == 0:
+        mean_kernel_ms = statistics.mean(kernel_ms)
+        mean_rays = statistics.mean(rays)
+        cpu = None
+        if world == 1 and not args.no_cpu_baseline:
+            cpu = cpu_sample(scene, args.cpu_seconds)
+        peak, peak_kind = measured_peaks()
+        roofline = None
+        if cpu is not None:
+            bpr = algorithmic_bytes_per_ray(cpu["counts"])
+            achieved = bpr * mean_rays / (mean_kernel_ms * 1e-3) / 1e9
+            roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                        "traffic": read_traffic(mean_rays), "peak_source": peak_kind,
+                        "kernel": "render_kernel", "bytes_per_ray": bpr, "rays_per_launch": mean_rays,
+                        "kernel_ms": mean_kernel_ms}
+        line = {
+            "metric": METRIC,
+            "value": value,
+            "unit": UNIT,
+            "n_gpus": world,
+            "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": total_ms / args.steps,
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f32",
+            "data": "synthetic",
+            "config": {"workload": WORKLOAD, "width": w, "height": h, "spp": spp, "max_bounces": scene.max_bounces,
+                       "l2": "flushed before every timed step (256 MiB write)", "parallelism": f"replicas x{world}"},
+            "mrays_per_s": world * mean_rays * args.steps / (total_ms * 1e-3) / 1e6,
+            "kernel_ms": mean_kernel_ms,
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+                    "timing": "host clock over K steps of upload + render + readback"},
+            "gpu_launches": args.steps,
+            "clocks": clk,
+        }
+        if roofline is not None:
+            line["roofline"] = roofline
+        if cpu is not None:
+            line["cpu_baseline"] = {
+                "value": cpu["mpaths_s"], "unit": UNIT, "cores": cpu["cores"], "kind": "port",
+                "sample": f"oracle (C++ restatement of crates/toaster-cpu) on every {cpu['row_step']}th row "
+                          f"({cpu['rows']} rows x {w} px x {spp} spp, {cpu['seconds']:.1f} s)"}
+        print(json.dumps(line), flush=True)
+    r.set_stream(0)
+    r.close()
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+def read_traffic(rays_per_launch):
+    """DRAM bytes per launch from the committed ncu summary (scaled by rays), or None."""
+    p = ROOT / "profiles" / "render_kernel_traffic.json"
+    if not p.exists():
+        return None
+    try:
+        d = json.loads(p.read_text())
+        return d["dram_bytes_per_ray"] * rays_per_launch
+    except Exception:
+        return None
+
+
+def main():
+    args = parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,226 @@
+/*
+ * toaster_cuda.h — C ABI of the B200 (sm_100a) path-tracing backend for toaster.
+ *
+ * This library replaces the `toaster-gpu` compute path (wgpu + shaders/pathtrace_spheres.wgsl).
+ * It consumes the same packed scene records that `toaster_gpu::scene_upload::scene_to_gpu`
+ * produces (crates/toaster-gpu/src/gpu_types.rs, byte-identical #[repr(C)] layouts) and returns
+ * the same linear-HDR float4 image, row-major with y down and alpha = 1.
+ *
+ * Conventions
+ *   - Every tc_* function returns TC_OK (0) or a negative TC_ERR_* code; tc_last_error() gives
+ *     the message. The same checks that toaster-gpu performs with anyhow::ensure! are made here
+ *     and reported as TC_ERR_INVALID.
+ *   - Host pointers are copied; the library owns every device buffer and one CUDA stream per
+ *     context. Calls are synchronous unless their name ends in _async. One context per thread.
+ *   - There is no CPU fallback: without a usable sm_100 GPU, tc_create fails.
+ */
+#ifndef TOASTER_CUDA_H
+#define TOASTER_CUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define TC_ABI_VERSION 1
+
+enum tc_status {
+  TC_OK = 0,
+  TC_ERR_INVALID = -1,    /* bad argument or scene contents */
+  TC_ERR_CUDA = -2,       /* CUDA runtime or launch failure */
+  TC_ERR_NO_DEVICE = -3,  /* no sm_100 device at the requested ordinal */
+  TC_ERR_STATE = -4,      /* call out of order (e.g. render before upload) */
+  TC_ERR_DEVICE_STATUS = -5 /* a kernel reported a bounded-wait or capacity failure */
+};
+
+/* ---------------------------------------------------------------- scene records
+ * Byte-compatible with crates/toaster-gpu/src/gpu_types.rs (sizes pinned by its test
+ * gpu_types_match_wgsl_layout_sizes, gpu_types.rs:200-211). */
+
+/* GpuRenderParams (gpu_types.rs:8-56), 96 bytes. */
+typedef struct tc_gpu_render_params {
+  uint32_t width, height, samples, max_bounces;
+  uint32_t sphere_count, triangle_count, material_count, frame_index;
+  uint32_t background_kind; /* 0 sky, 1 black, 2 environment */
+  uint32_t light_count;
+  float total_light_weight;
+  uint32_t _pad0;
+  uint32_t environment_width, environment_height;
+  float environment_intensity, environment_rotation_degrees;
+  uint32_t accumulated_samples;
+  uint32_t _pad1[3];
+  uint32_t bvh_node_count, bvh_primitive_count;
+  uint32_t _pad2[2];
+} tc_gpu_render_params;
+
+/* GpuCamera (gpu_types.rs:61-70), 64 bytes: origin, lower-left corner, horizontal, vertical. */
+typedef struct tc_gpu_camera {
+  float origin[4], lower_left_corner[4], horizontal[4], vertical[4];
+} tc_gpu_camera;
+
+/* GpuSphere (gpu_types.rs:75-83), 32 bytes. */
+typedef struct tc_gpu_sphere {
+  float center_radius[4];
+  uint32_t material_index, _pad0[3];
+} tc_gpu_sphere;
+
+/* GpuTriangle (gpu_types.rs:88-100), 64 bytes. */
+typedef struct tc_gpu_triangle {
+  float v0[4], v1[4], v2[4];
+  uint32_t material_index, _pad0[3];
+} tc_gpu_triangle;
+
+/* GpuTriangleAttributes (gpu_types.rs:105-123), 80 bytes; flags bit0 normals, bit1 uvs. */
+typedef struct tc_gpu_triangle_attributes {
+  float n0[4], n1[4], n2[4];
+  float uv0[2], uv1[2], uv2[2];
+  uint32_t flags, _pad0;
+} tc_gpu_triangle_attributes;
+
+/* GpuMaterial (gpu_types.rs:128-143), 48 bytes; kind 0 diffuse, 1 metal, 2 dielectric,
+ * 3 emissive; params = (roughness, ior, emission strength, unused). */
+typedef struct tc_gpu_material {
+  uint32_t kind, texture_offset, texture_width, texture_height;
+  float albedo[4];
+  float params[4];
+} tc_gpu_material;
+
+/* GpuLight (gpu_types.rs:148-167), 96 bytes; kind 0 triangle, 1 sphere;
+ * area_weight_cumulative = (area, weight, cumulative weight, unused). */
+typedef struct tc_gpu_light {
+  uint32_t kind, material_index, _pad0[2];
+  float v0[4], v1[4], v2[4], center_radius[4];
+  float area_weight_cumulative[4];
+} tc_gpu_light;
+
+/* GpuBvhNode (gpu_types.rs:172-184), 48 bytes; primitive_count > 0 marks a leaf. */
+typedef struct tc_gpu_bvh_node {
+  float min[4], max[4];
+  uint32_t first_or_right, primitive_count, _pad[2];
+} tc_gpu_bvh_node;
+
+/* GpuPrimitiveRef (gpu_types.rs:189-194), 8 bytes; kind 0 sphere, 1 triangle. */
+typedef struct tc_gpu_primitive_ref {
+  uint32_t kind, index;
+} tc_gpu_primitive_ref;
+
+/* SceneGpuData (crates/toaster-gpu/src/scene_upload.rs:17-40) as pointers and counts.
+ * bvh_nodes / bvh_primitives may be NULL: the library then builds the same median-split
+ * hierarchy itself (crates/toaster-bvh/src/bvh.rs:92-154). environment_pixels holds
+ * float4 texels (linear RGB, lane w ignored: the library builds its own 2-D CDF). */
+typedef struct tc_scene_data {
+  tc_gpu_render_params params;
+  tc_gpu_camera camera;
+  const tc_gpu_sphere* spheres;
+  size_t sphere_count;
+  const tc_gpu_triangle* triangles;
+  size_t triangle_count;
+  const tc_gpu_triangle_attributes* triangle_attributes;
+  size_t triangle_attribute_count;
+  const tc_gpu_material* materials;
+  size_t material_count;
+  const tc_gpu_light* lights;
+  size_t light_count;
+  const tc_gpu_bvh_node* bvh_nodes;
+  size_t bvh_node_count;
+  const tc_gpu_primitive_ref* bvh_primitives;
+  size_t bvh_primitive_count;
+  const uint32_t* texture_pixels;
+  size_t texture_pixel_count;
+  const float* environment_pixels;
+  size_t environment_pixel_count;
+} tc_scene_data;
+
+/* Per-dispatch options beyond GpuRenderParams. Zero-initialised means defaults. */
+typedef struct tc_render_options {
+  uint32_t block_size;       /* threads per block for the path kernel; 0 = tuned default */
+  uint32_t samples_per_item; /* samples one lane traces for a pixel before taking new work; 0 = default */
+  uint32_t keep_moments;     /* 1: also accumulate per-pixel sums of squared samples (FP64) */
+  uint32_t guiding;          /* 1: learned path guiding (requires tc_guiding_* setup) */
+  uint32_t _reserved[4];
+} tc_render_options;
+
+/* Counters of the most recent tc_render / tc_trace_* call. */
+typedef struct tc_stats {
+  uint64_t paths;            /* camera paths traced */
+  uint64_t rays;             /* extension + shadow rays */
+  uint64_t extension_rays;
+  uint64_t shadow_rays;
+  float kernel_ms;           /* device time of the main kernel (CUDA events) */
+  float total_ms;            /* device time of the whole call including copies */
+  uint32_t bvh_depth;        /* deepest leaf of the uploaded hierarchy */
+  uint32_t status_flags;     /* device status word (0 = clean) */
+} tc_stats;
+
+typedef struct tc_context tc_context;
+
+/* Library and device --------------------------------------------------------------------- */
+int tc_abi_version(void);
+/* Message of the last failure on this thread when ctx is NULL (e.g. after tc_create). */
+const char* tc_last_error(const tc_context* ctx);
+
+/* Replaces toaster-gpu create_gpu_context (crates/toaster-gpu/src/device.rs:49-100). */
+int tc_create(int device_ordinal, tc_context** out_ctx);
+int tc_destroy(tc_context* ctx);
+
+/* Makes the context enqueue its work on `stream` (a cudaStream_t of the context's device owned
+ * by the caller), or on its own stream again when NULL. Lets a host time calls with its own
+ * CUDA events. No reference counterpart (wgpu owns its queue). */
+int tc_set_stream(tc_context* ctx, void* stream);
+
+/* Replaces create_scene_gpu_buffers + the queue.write_buffer uploads
+ * (crates/toaster-gpu/src/buffers.rs:117-271, path_tracer.rs:676-721). */
+int tc_upload_scene(tc_context* ctx, const tc_scene_data* scene);
+
+/* Replaces the camera write_buffer (path_tracer.rs:680-684). */
+int tc_set_camera(tc_context* ctx, const tc_gpu_camera* camera);
+
+/* Replaces dispatch_compute_2d (crates/toaster-gpu/src/dispatch.rs:28-60): traces
+ * params->samples paths per pixel. params->accumulated_samples == 0 starts a new image;
+ * otherwise it must equal the samples already accumulated (progressive mode,
+ * path_tracer.rs:900-923). options may be NULL. */
+int tc_render(tc_context* ctx, const tc_gpu_render_params* params, const tc_render_options* options);
+
+/* Replaces readback_pixels (crates/toaster-gpu/src/readback.rs:8-25): writes width*height
+ * float4 linear-HDR averages into rgba (n_floats >= 4*width*height). */
+int tc_readback(tc_context* ctx, float* rgba, size_t n_floats);
+
+/* Per-pixel FP64 running sums (3 per pixel) and, when keep_moments was set, sums of squared
+ * sample values (3 per pixel). Either pointer may be NULL. *samples receives the count. */
+int tc_readback_sums(tc_context* ctx, double* sum, double* sum_sq, size_t n_doubles, uint32_t* samples);
+
+/* Closest hit for n host rays (origin.xyz, direction.xyz; 6 floats each) with minimum
+ * distance tmin: prim[i] = kind << 31 | scene index, with the GpuPrimitiveRef kind codes
+ * (0 sphere, 1 triangle), or TC_MISS; t[i] = hit distance or +inf. Traversal and
+ * intersection follow crates/toaster-cpu/src/intersect.rs:172-263 bit for bit. */
+#define TC_MISS 0xFFFFFFFFu
+#define TC_PRIM_TRIANGLE_BIT 0x80000000u
+int tc_trace_closest(tc_context* ctx, const float* rays, size_t n, float tmin, uint32_t* prim, float* t);
+
+/* Same as tc_trace_closest on device-resident buffers, enqueued on `stream` (a cudaStream_t,
+ * NULL = the context stream); nothing is synchronised. */
+int tc_trace_closest_device_async(tc_context* ctx, const float* d_rays, size_t n, float tmin, uint32_t* d_prim,
+                                  float* d_t, void* stream);
+
+int tc_get_stats(const tc_context* ctx, tc_stats* out);
+
+/* Host-only helpers (no GPU needed) -------------------------------------------------------- */
+
+/* Builds the median-split hierarchy of crates/toaster-bvh for the given spheres and triangles
+ * (spheres first, triangles padded by 1e-5, scene_upload.rs:296-346) and writes it in the
+ * reference's flat layout. Capacities: nodes >= 2*(n_spheres+n_triangles)-1, prims >= n.
+ * Returns the node count (>= 0) or a negative error. */
+long tc_build_bvh_host(const tc_gpu_sphere* spheres, size_t n_spheres, const tc_gpu_triangle* triangles,
+                       size_t n_triangles, tc_gpu_bvh_node* nodes, size_t node_capacity,
+                       tc_gpu_primitive_ref* prims, size_t prim_capacity);
+
+/* Byte sizes of the record types as compiled into the library (layout check). */
+int tc_record_sizes(uint32_t* out, size_t n);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* TOASTER_CUDA_H */

@@ -1,0 +1,29 @@
+"""toaster_b200 — a B200-native (sm_100a) CUDA backend for toaster's GPU path-tracing path.
+
+Scene in (toaster's JSON format or packed ``gpu_types`` records), linear-HDR float4 image out,
+through the C ABI in include/toaster_cuda.h. See ``renderer`` for the host API.
+"""
+
+from . import gpu_types
+from .scene import EnvironmentMap, Material, Scene, SceneGpuData, load_scene, make_camera, scene_to_gpu
+
+__all__ = [
+    "gpu_types",
+    "EnvironmentMap",
+    "Material",
+    "Scene",
+    "SceneGpuData",
+    "load_scene",
+    "make_camera",
+    "scene_to_gpu",
+]
+
+
+def __getattr__(name):
+    # The renderer needs the built CUDA library; import it on first use only.
+    if name in {"GpuRenderer", "render_scene_gpu", "render_gpu_progressive", "benchmark_gpu_scene",
+                "progressive_batch"}:
+        from . import renderer
+
+        return getattr(renderer, name)
+    raise AttributeError(name)

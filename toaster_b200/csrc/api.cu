@@ -1,0 +1,666 @@
+// Host runtime and C ABI of the toaster B200 path tracer (see include/toaster_cuda.h).
+//
+// Ownership follows the reference boundary (crates/toaster-gpu/src/path_tracer.rs:518-849):
+// the caller owns host arrays, the context owns every device buffer and one stream, and each
+// call is synchronous like dispatch_compute_2d's device.poll(Wait) (dispatch.rs:57).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/toaster_cuda.h"
+#include "bvh_build.h"
+#include "device_scene.h"
+#include "layout.h"
+
+static_assert(sizeof(tc_gpu_render_params) == 96, "GpuRenderParams is 96 bytes");
+static_assert(sizeof(tc_gpu_camera) == 64, "GpuCamera is 64 bytes");
+static_assert(sizeof(tc_gpu_sphere) == 32, "GpuSphere is 32 bytes");
+static_assert(sizeof(tc_gpu_triangle) == 64, "GpuTriangle is 64 bytes");
+static_assert(sizeof(tc_gpu_triangle_attributes) == 80, "GpuTriangleAttributes is 80 bytes");
+static_assert(sizeof(tc_gpu_material) == 48, "GpuMaterial is 48 bytes");
+static_assert(sizeof(tc_gpu_light) == 96, "GpuLight is 96 bytes");
+static_assert(sizeof(tc_gpu_bvh_node) == 48, "GpuBvhNode is 48 bytes");
+static_assert(sizeof(tc_gpu_primitive_ref) == 8, "GpuPrimitiveRef is 8 bytes");
+
+namespace {
+
+thread_local std::string g_thread_error;
+
+struct DevBuf {
+  void* ptr = nullptr;
+  size_t bytes = 0;
+  DevBuf() = default;
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  ~DevBuf() { release(); }
+  void release() {
+    if (ptr) cudaFree(ptr);
+    ptr = nullptr;
+    bytes = 0;
+  }
+  // Grows to at least `n` bytes (contents are not preserved).
+  cudaError_t reserve(size_t n) {
+    if (n <= bytes && ptr) return cudaSuccess;
+    release();
+    if (n == 0) return cudaSuccess;
+    cudaError_t e = cudaMalloc(&ptr, n);
+    if (e == cudaSuccess) bytes = n;
+    else ptr = nullptr;
+    return e;
+  }
+  template <class T>
+  T* as() const { return static_cast<T*>(ptr); }
+};
+
+}  // namespace
+
+struct tc_context {
+  int device = 0;
+  int sm_count = 0;
+  cudaStream_t stream = nullptr;        // stream used by every call
+  cudaStream_t own_stream = nullptr;    // the context's own stream
+  cudaEvent_t ev_begin = nullptr, ev_kernel0 = nullptr, ev_kernel1 = nullptr, ev_end = nullptr;
+  std::string error;
+
+  // Scene
+  bool has_scene = false;
+  tcb::DevScene scene{};
+  DevBuf pairs, prims, materials, lights, attributes, texels;
+  DevBuf env_rgb, env_marginal, env_conditional, env_pdf, env_row_sums, env_total;
+  uint32_t sphere_count = 0, triangle_count = 0, material_count = 0, light_count = 0, bvh_prims = 0;
+  uint32_t bvh_depth = 0;
+
+  // Accumulation state (progressive contract of path_tracer.rs:900-923)
+  uint32_t width = 0, height = 0, accumulated = 0;
+  bool has_moments = false;
+  DevBuf accum, accum_sq, image, work_counter, counters;
+
+  // Parity scratch
+  DevBuf ray_buf, prim_buf, t_buf;
+
+  tc_stats stats{};
+};
+
+namespace {
+
+int fail(tc_context* ctx, int code, const std::string& msg) {
+  if (ctx) ctx->error = msg;
+  g_thread_error = msg;
+  return code;
+}
+
+int cuda_fail(tc_context* ctx, cudaError_t e, const char* what) {
+  return fail(ctx, TC_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+#define TC_CUDA(ctx, call)                                     \
+  do {                                                         \
+    cudaError_t _e = (call);                                   \
+    if (_e != cudaSuccess) return cuda_fail((ctx), _e, #call); \
+  } while (0)
+
+template <class T>
+cudaError_t upload(DevBuf& buf, const T* src, size_t count, cudaStream_t stream) {
+  const size_t bytes = sizeof(T) * count;
+  if (bytes == 0) return cudaSuccess;
+  cudaError_t e = buf.reserve(bytes);
+  if (e != cudaSuccess) return e;
+  return cudaMemcpyAsync(buf.ptr, src, bytes, cudaMemcpyHostToDevice, stream);
+}
+
+// Walker alias table (Vose's construction) over light weights, built in double precision.
+void build_alias(const std::vector<double>& w, std::vector<float>& prob, std::vector<uint32_t>& alias) {
+  const size_t n = w.size();
+  prob.assign(n, 1.0f);
+  alias.resize(n);
+  for (size_t i = 0; i < n; ++i) alias[i] = uint32_t(i);
+  double total = 0.0;
+  for (double x : w) total += x;
+  if (n == 0 || !(total > 0.0)) return;
+  std::vector<double> q(n);
+  std::vector<uint32_t> small, large;
+  for (size_t i = 0; i < n; ++i) {
+    q[i] = w[i] * double(n) / total;
+    (q[i] < 1.0 ? small : large).push_back(uint32_t(i));
+  }
+  while (!small.empty() && !large.empty()) {
+    const uint32_t s = small.back(), l = large.back();
+    small.pop_back();
+    prob[s] = float(q[s]);
+    alias[s] = l;
+    q[l] = (q[l] + q[s]) - 1.0;
+    if (q[l] < 1.0) {
+      large.pop_back();
+      small.push_back(l);
+    }
+  }
+  for (uint32_t i : large) prob[i] = 1.0f;
+  for (uint32_t i : small) prob[i] = 1.0f;
+}
+
+bool finite3(const float* v) { return std::isfinite(v[0]) && std::isfinite(v[1]) && std::isfinite(v[2]); }
+
+}  // namespace
+
+extern "C" {
+
+int tc_abi_version(void) { return TC_ABI_VERSION; }
+
+const char* tc_last_error(const tc_context* ctx) {
+  if (ctx) return ctx->error.c_str();
+  return g_thread_error.c_str();
+}
+
+int tc_record_sizes(uint32_t* out, size_t n) {
+  const uint32_t sizes[9] = {uint32_t(sizeof(tc_gpu_render_params)), uint32_t(sizeof(tc_gpu_camera)),
+                             uint32_t(sizeof(tc_gpu_sphere)),         uint32_t(sizeof(tc_gpu_triangle)),
+                             uint32_t(sizeof(tc_gpu_triangle_attributes)), uint32_t(sizeof(tc_gpu_material)),
+                             uint32_t(sizeof(tc_gpu_light)),          uint32_t(sizeof(tc_gpu_bvh_node)),
+                             uint32_t(sizeof(tc_gpu_primitive_ref))};
+  if (!out || n < 9) return fail(nullptr, TC_ERR_INVALID, "tc_record_sizes needs room for 9 values");
+  std::memcpy(out, sizes, sizeof(sizes));
+  return TC_OK;
+}
+
+int tc_create(int device_ordinal, tc_context** out_ctx) {
+  if (!out_ctx) return fail(nullptr, TC_ERR_INVALID, "out_ctx is null");
+  *out_ctx = nullptr;
+  int count = 0;
+  cudaError_t e = cudaGetDeviceCount(&count);
+  if (e != cudaSuccess || count == 0)
+    return fail(nullptr, TC_ERR_NO_DEVICE, std::string("no CUDA device: ") + cudaGetErrorString(e));
+  if (device_ordinal < 0 || device_ordinal >= count)
+    return fail(nullptr, TC_ERR_NO_DEVICE, "device ordinal " + std::to_string(device_ordinal) + " out of range");
+  cudaDeviceProp prop;
+  e = cudaGetDeviceProperties(&prop, device_ordinal);
+  if (e != cudaSuccess) return fail(nullptr, TC_ERR_NO_DEVICE, cudaGetErrorString(e));
+  if (prop.major != 10)
+    return fail(nullptr, TC_ERR_NO_DEVICE,
+                std::string("device ") + prop.name + " is not sm_100 (compute capability " +
+                    std::to_string(prop.major) + "." + std::to_string(prop.minor) + ")");
+  e = cudaSetDevice(device_ordinal);
+  if (e != cudaSuccess) return fail(nullptr, TC_ERR_CUDA, cudaGetErrorString(e));
+  auto* ctx = new tc_context();
+  ctx->device = device_ordinal;
+  ctx->sm_count = prop.multiProcessorCount;
+  if ((e = cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking)) != cudaSuccess ||
+      (e = cudaEventCreate(&ctx->ev_begin)) != cudaSuccess || (e = cudaEventCreate(&ctx->ev_kernel0)) != cudaSuccess ||
+      (e = cudaEventCreate(&ctx->ev_kernel1)) != cudaSuccess || (e = cudaEventCreate(&ctx->ev_end)) != cudaSuccess) {
+    std::string msg = std::string("context setup failed: ") + cudaGetErrorString(e);
+    tc_destroy(ctx);
+    return fail(nullptr, TC_ERR_CUDA, msg);
+  }
+  ctx->stream = ctx->own_stream;
+  if ((e = ctx->work_counter.reserve(sizeof(unsigned long long))) != cudaSuccess ||
+      (e = ctx->counters.reserve(4 * sizeof(unsigned long long))) != cudaSuccess) {
+    std::string msg = std::string("context allocation failed: ") + cudaGetErrorString(e);
+    tc_destroy(ctx);
+    return fail(nullptr, TC_ERR_CUDA, msg);
+  }
+  *out_ctx = ctx;
+  return TC_OK;
+}
+
+int tc_destroy(tc_context* ctx) {
+  if (!ctx) return TC_OK;
+  cudaSetDevice(ctx->device);
+  if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  if (ctx->own_stream && ctx->own_stream != ctx->stream) cudaStreamSynchronize(ctx->own_stream);
+  if (ctx->ev_begin) cudaEventDestroy(ctx->ev_begin);
+  if (ctx->ev_kernel0) cudaEventDestroy(ctx->ev_kernel0);
+  if (ctx->ev_kernel1) cudaEventDestroy(ctx->ev_kernel1);
+  if (ctx->ev_end) cudaEventDestroy(ctx->ev_end);
+  if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
+  delete ctx;
+  return TC_OK;
+}
+
+int tc_set_stream(tc_context* ctx, void* stream) {
+  if (!ctx) return fail(nullptr, TC_ERR_INVALID, "context is null");
+  TC_CUDA(ctx, cudaSetDevice(ctx->device));
+  TC_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  ctx->stream = stream ? static_cast<cudaStream_t>(stream) : ctx->own_stream;
+  return TC_OK;
+}
+
+int tc_upload_scene(tc_context* ctx, const tc_scene_data* sd) {
+  if (!ctx) return fail(nullptr, TC_ERR_INVALID, "context is null");
+  if (!sd) return fail(ctx, TC_ERR_INVALID, "scene is null");
+  TC_CUDA(ctx, cudaSetDevice(ctx->device));
+  // Validation mirrors scene_to_gpu_inner (crates/toaster-gpu/src/scene_upload.rs:84-98).
+  if (sd->sphere_count == 0 && sd->triangle_count == 0)
+    return fail(ctx, TC_ERR_INVALID, "GPU renderer requires at least one object");
+  if (sd->material_count == 0 || !sd->materials)
+    return fail(ctx, TC_ERR_INVALID, "GPU renderer requires at least one material");
+  if ((sd->sphere_count && !sd->spheres) || (sd->triangle_count && !sd->triangles))
+    return fail(ctx, TC_ERR_INVALID, "geometry pointer is null for a nonzero count");
+  if (sd->triangle_attributes && sd->triangle_attribute_count != sd->triangle_count)
+    return fail(ctx, TC_ERR_INVALID, "triangle attribute count must match triangle count");
+  if (sd->sphere_count + sd->triangle_count > tcb::kMaxPrimitives)
+    return fail(ctx, TC_ERR_INVALID, "too many primitives for GPU");
+  const uint32_t n_mat = uint32_t(sd->material_count);
+  for (size_t i = 0; i < sd->sphere_count; ++i) {
+    const tc_gpu_sphere& s = sd->spheres[i];
+    if (s.material_index >= n_mat) return fail(ctx, TC_ERR_INVALID, "sphere " + std::to_string(i) + " references an unknown material");
+    if (!std::isfinite(s.center_radius[3]) || !(s.center_radius[3] > 0.0f) || !finite3(s.center_radius))
+      return fail(ctx, TC_ERR_INVALID, "sphere " + std::to_string(i) + " must have a finite center and positive radius");
+  }
+  for (size_t i = 0; i < sd->triangle_count; ++i) {
+    const tc_gpu_triangle& t = sd->triangles[i];
+    if (t.material_index >= n_mat) return fail(ctx, TC_ERR_INVALID, "triangle " + std::to_string(i) + " references an unknown material");
+    if (!finite3(t.v0) || !finite3(t.v1) || !finite3(t.v2))
+      return fail(ctx, TC_ERR_INVALID, "triangle " + std::to_string(i) + " vertices must be finite");
+  }
+  const uint32_t bg = sd->params.background_kind;
+  if (bg > 2u) return fail(ctx, TC_ERR_INVALID, "background kind must be 0 (sky), 1 (black) or 2 (environment)");
+  const uint32_t ew = sd->params.environment_width, eh = sd->params.environment_height;
+  const bool has_env = ew > 0 && eh > 0;
+  if (bg == 2u && (!has_env || !sd->environment_pixels))
+    return fail(ctx, TC_ERR_INVALID, "environment background requires an environment map");
+  if (has_env && sd->environment_pixels && sd->environment_pixel_count != size_t(ew) * eh)
+    return fail(ctx, TC_ERR_INVALID, "environment contains " + std::to_string(sd->environment_pixel_count) +
+                                         " pixels but " + std::to_string(size_t(ew) * eh) + " were expected");
+
+  // Materials.
+  std::vector<tcb::DevMaterial> mats(n_mat);
+  for (uint32_t i = 0; i < n_mat; ++i) {
+    const tc_gpu_material& m = sd->materials[i];
+    if (m.kind > 3u) return fail(ctx, TC_ERR_INVALID, "material " + std::to_string(i) + " has an unknown kind");
+    if (m.texture_width && m.texture_height &&
+        (!sd->texture_pixels || size_t(m.texture_offset) + size_t(m.texture_width) * m.texture_height > sd->texture_pixel_count))
+      return fail(ctx, TC_ERR_INVALID, "material " + std::to_string(i) + " texture lies outside the texture atlas");
+    tcb::DevMaterial d{};
+    d.kind = m.kind;
+    for (int c = 0; c < 3; ++c) {
+      d.albedo[c] = m.albedo[c];
+      d.emission[c] = m.kind == tcb::kEmissive ? m.albedo[c] * m.params[2] : 0.0f;
+    }
+    d.roughness = std::min(std::max(m.params[0], 0.0f), 1.0f);
+    d.ior = m.params[1];
+    if (m.kind == tcb::kDielectric && !(d.ior > 0.0f))
+      return fail(ctx, TC_ERR_INVALID, "material " + std::to_string(i) + ": dielectric ior must be positive");
+    d.tex_offset = m.texture_offset;
+    d.tex_width = m.texture_width;
+    d.tex_height = m.texture_height;
+    mats[i] = d;
+  }
+
+  // Hierarchy: the caller's (reference layout) or a fresh median-split build.
+  std::vector<tcb::SphereIn> sph(sd->sphere_count);
+  std::vector<uint32_t> sph_mat(sd->sphere_count);
+  for (size_t i = 0; i < sd->sphere_count; ++i) {
+    const tc_gpu_sphere& s = sd->spheres[i];
+    sph[i] = tcb::SphereIn{{s.center_radius[0], s.center_radius[1], s.center_radius[2]}, s.center_radius[3]};
+    sph_mat[i] = s.material_index;
+  }
+  std::vector<tcb::TriangleIn> tri(sd->triangle_count);
+  std::vector<uint32_t> tri_mat(sd->triangle_count), tri_flags(sd->triangle_count, 0u);
+  for (size_t i = 0; i < sd->triangle_count; ++i) {
+    const tc_gpu_triangle& t = sd->triangles[i];
+    for (int c = 0; c < 3; ++c) {
+      tri[i].v[0][c] = t.v0[c];
+      tri[i].v[1][c] = t.v1[c];
+      tri[i].v[2][c] = t.v2[c];
+    }
+    tri_mat[i] = t.material_index;
+    if (sd->triangle_attributes) tri_flags[i] = sd->triangle_attributes[i].flags & 3u;
+  }
+  tcb::FlatHierarchy flat;
+  if (sd->bvh_nodes && sd->bvh_node_count) {
+    if (!sd->bvh_primitives || sd->bvh_primitive_count != sd->sphere_count + sd->triangle_count)
+      return fail(ctx, TC_ERR_INVALID, "BVH primitive references must cover every sphere and triangle");
+    flat.nodes.resize(sd->bvh_node_count);
+    for (size_t i = 0; i < sd->bvh_node_count; ++i) {
+      const tc_gpu_bvh_node& n = sd->bvh_nodes[i];
+      tcb::FlatNode& f = flat.nodes[i];
+      for (int c = 0; c < 3; ++c) {
+        f.min[c] = n.min[c];
+        f.max[c] = n.max[c];
+      }
+      f.first_or_right = n.first_or_right;
+      f.count = n.primitive_count;
+    }
+    flat.prims.resize(sd->bvh_primitive_count);
+    for (size_t i = 0; i < sd->bvh_primitive_count; ++i)
+      flat.prims[i] = tcb::PrimRef{sd->bvh_primitives[i].kind, sd->bvh_primitives[i].index};
+  } else {
+    flat = tcb::build_median_split(sph.data(), sph.size(), tri.data(), tri.size());
+  }
+  tcb::DeviceHierarchy dh;
+  std::string err;
+  if (!tcb::to_device_layout(flat, sph.data(), sph_mat.data(), sph.size(), tri.data(), tri_mat.data(),
+                             tri_flags.data(), tri.size(), dh, err))
+    return fail(ctx, TC_ERR_INVALID, err);
+
+  // Lights: alias table over the GpuLight weights (light.rs:57-113 distribution).
+  std::vector<tcb::DevLight> lights(sd->light_count);
+  if (sd->light_count) {
+    if (!sd->lights) return fail(ctx, TC_ERR_INVALID, "light pointer is null for a nonzero count");
+    std::vector<double> w(sd->light_count);
+    double total = 0.0;
+    for (size_t i = 0; i < sd->light_count; ++i) {
+      w[i] = std::max(0.0, double(sd->lights[i].area_weight_cumulative[1]));
+      total += w[i];
+    }
+    if (!(total > 0.0)) return fail(ctx, TC_ERR_INVALID, "lights have no positive weight");
+    std::vector<float> prob;
+    std::vector<uint32_t> alias;
+    build_alias(w, prob, alias);
+    for (size_t i = 0; i < sd->light_count; ++i) {
+      const tc_gpu_light& l = sd->lights[i];
+      if (l.material_index >= n_mat) return fail(ctx, TC_ERR_INVALID, "light " + std::to_string(i) + " references an unknown material");
+      const tc_gpu_material& m = sd->materials[l.material_index];
+      tcb::DevLight d{};
+      d.kind = l.kind;
+      const float area = l.area_weight_cumulative[0];
+      if (!(area > 0.0f)) return fail(ctx, TC_ERR_INVALID, "light " + std::to_string(i) + " has no area");
+      d.pdf_area = float((w[i] / total) / double(area));
+      for (int c = 0; c < 3; ++c) d.emission[c] = m.albedo[c] * m.params[2];
+      if (l.kind == 0) {
+        float e1[3], e2[3];
+        for (int c = 0; c < 3; ++c) {
+          d.p0[c] = l.v0[c];
+          e1[c] = l.v1[c] - l.v0[c];
+          e2[c] = l.v2[c] - l.v0[c];
+          d.e1[c] = e1[c];
+          d.e2[c] = e2[c];
+        }
+        const float nx = e1[1] * e2[2] - e2[1] * e1[2], ny = e1[2] * e2[0] - e2[2] * e1[0],
+                    nz = e1[0] * e2[1] - e2[0] * e1[1];
+        const float inv = 1.0f / std::sqrt(nx * nx + ny * ny + nz * nz);
+        d.normal[0] = nx * inv;
+        d.normal[1] = ny * inv;
+        d.normal[2] = nz * inv;
+      } else if (l.kind == 1) {
+        for (int c = 0; c < 3; ++c) d.p0[c] = l.center_radius[c];
+        d.radius = l.center_radius[3];
+      } else {
+        return fail(ctx, TC_ERR_INVALID, "light " + std::to_string(i) + " kind must be 0 (triangle) or 1 (sphere)");
+      }
+      d.alias_prob = prob[i];
+      d.alias = alias[i];
+      lights[i] = d;
+    }
+  }
+
+  // Upload.
+  cudaStream_t st = ctx->stream;
+  TC_CUDA(ctx, upload(ctx->pairs, dh.pairs.data(), dh.pairs.size(), st));
+  TC_CUDA(ctx, upload(ctx->prims, dh.prims.data(), dh.prims.size(), st));
+  TC_CUDA(ctx, upload(ctx->materials, mats.data(), mats.size(), st));
+  TC_CUDA(ctx, upload(ctx->lights, lights.data(), lights.size(), st));
+  bool any_attr = false;
+  for (uint32_t f : tri_flags) any_attr |= f != 0u;
+  if (any_attr) TC_CUDA(ctx, upload(ctx->attributes, sd->triangle_attributes, sd->triangle_count, st));
+  if (sd->texture_pixels && sd->texture_pixel_count)
+    TC_CUDA(ctx, upload(ctx->texels, sd->texture_pixels, sd->texture_pixel_count, st));
+
+  tcb::DevScene& s = ctx->scene;
+  s = tcb::DevScene{};
+  s.pairs = ctx->pairs.as<tcb::PairNode>();
+  s.prims = ctx->prims.as<tcb::PrimRecord>();
+  s.root = dh.root;
+  s.materials = ctx->materials.as<tcb::DevMaterial>();
+  s.material_count = n_mat;
+  s.lights = sd->light_count ? ctx->lights.as<tcb::DevLight>() : nullptr;
+  s.light_count = uint32_t(sd->light_count);
+  s.attributes = any_attr ? ctx->attributes.as<float4>() : nullptr;
+  s.texels = (sd->texture_pixels && sd->texture_pixel_count) ? ctx->texels.as<uint32_t>() : nullptr;
+  s.background = bg;
+  if (has_env && sd->environment_pixels) {
+    const size_t n = size_t(ew) * eh;
+    TC_CUDA(ctx, upload(ctx->env_rgb, reinterpret_cast<const float4*>(sd->environment_pixels), n, st));
+    TC_CUDA(ctx, ctx->env_marginal.reserve(sizeof(float) * eh));
+    TC_CUDA(ctx, ctx->env_conditional.reserve(sizeof(float) * n));
+    TC_CUDA(ctx, ctx->env_pdf.reserve(sizeof(float) * n));
+    TC_CUDA(ctx, ctx->env_row_sums.reserve(sizeof(double) * eh));
+    TC_CUDA(ctx, ctx->env_total.reserve(sizeof(double)));
+    TC_CUDA(ctx, tcb::launch_env_tables(ctx->env_rgb.as<float4>(), ew, eh, sd->params.environment_intensity,
+                                        ctx->env_marginal.as<float>(), ctx->env_conditional.as<float>(),
+                                        ctx->env_pdf.as<float>(), ctx->env_row_sums.as<double>(),
+                                        ctx->env_total.as<double>(), st));
+    double total = 0.0;
+    TC_CUDA(ctx, cudaMemcpyAsync(&total, ctx->env_total.ptr, sizeof(double), cudaMemcpyDeviceToHost, st));
+    TC_CUDA(ctx, cudaStreamSynchronize(st));
+    s.env_rgb = ctx->env_rgb.as<float4>();
+    s.env_marginal = ctx->env_marginal.as<float>();
+    s.env_conditional = ctx->env_conditional.as<float>();
+    s.env_pdf = ctx->env_pdf.as<float>();
+    s.env_width = ew;
+    s.env_height = eh;
+    s.env_intensity = sd->params.environment_intensity;
+    float rot = std::fmod(sd->params.environment_rotation_degrees, 360.0f);
+    if (rot < 0.0f) rot += 360.0f;
+    s.env_rotation_turns = rot / 360.0f;
+    s.env_sampleable = (total > 0.0 && std::isfinite(total)) ? 1u : 0u;
+  }
+  for (int c = 0; c < 3; ++c) {
+    s.cam_origin[c] = sd->camera.origin[c];
+    s.cam_lower_left[c] = sd->camera.lower_left_corner[c];
+    s.cam_horizontal[c] = sd->camera.horizontal[c];
+    s.cam_vertical[c] = sd->camera.vertical[c];
+  }
+  TC_CUDA(ctx, cudaStreamSynchronize(st));
+  ctx->has_scene = true;
+  ctx->sphere_count = uint32_t(sd->sphere_count);
+  ctx->triangle_count = uint32_t(sd->triangle_count);
+  ctx->material_count = n_mat;
+  ctx->light_count = uint32_t(sd->light_count);
+  ctx->bvh_prims = uint32_t(flat.prims.size());
+  ctx->bvh_depth = dh.depth;
+  ctx->stats.bvh_depth = dh.depth;
+  return TC_OK;
+}
+
+int tc_set_camera(tc_context* ctx, const tc_gpu_camera* cam) {
+  if (!ctx) return fail(nullptr, TC_ERR_INVALID, "context is null");
+  if (!cam) return fail(ctx, TC_ERR_INVALID, "camera is null");
+  if (!ctx->has_scene) return fail(ctx, TC_ERR_STATE, "tc_set_camera before tc_upload_scene");
+  for (int c = 0; c < 3; ++c) {
+    ctx->scene.cam_origin[c] = cam->origin[c];
+    ctx->scene.cam_lower_left[c] = cam->lower_left_corner[c];
+    ctx->scene.cam_horizontal[c] = cam->horizontal[c];
+    ctx->scene.cam_vertical[c] = cam->vertical[c];
+  }
+  return TC_OK;
+}
+
+int tc_render(tc_context* ctx, const tc_gpu_render_params* p, const tc_render_options* opt) {
+  if (!ctx) return fail(nullptr, TC_ERR_INVALID, "context is null");
+  if (!p) return fail(ctx, TC_ERR_INVALID, "render params are null");
+  if (!ctx->has_scene) return fail(ctx, TC_ERR_STATE, "tc_render before tc_upload_scene");
+  if (p->width == 0 || p->height == 0) return fail(ctx, TC_ERR_INVALID, "render dimensions must be nonzero");
+  if (p->samples == 0) return fail(ctx, TC_ERR_INVALID, "sample batch must be greater than zero");
+  if (uint64_t(p->width) * p->height > (1ull << 31)) return fail(ctx, TC_ERR_INVALID, "image is too large");
+  TC_CUDA(ctx, cudaSetDevice(ctx->device));
+  tc_render_options o{};
+  if (opt) o = *opt;
+  const bool moments = o.keep_moments != 0;
+  if (o.guiding) return fail(ctx, TC_ERR_STATE, "guided rendering needs a trained guiding network");
+  const uint32_t npix = p->width * p->height;
+  cudaStream_t st = ctx->stream;
+  TC_CUDA(ctx, cudaEventRecord(ctx->ev_begin, st));
+  if (p->accumulated_samples == 0) {
+    if (ctx->width != p->width || ctx->height != p->height || !ctx->accum.ptr) {
+      TC_CUDA(ctx, ctx->accum.reserve(sizeof(double) * 3 * npix));
+      TC_CUDA(ctx, ctx->image.reserve(sizeof(float4) * npix));
+    }
+    if (moments) TC_CUDA(ctx, ctx->accum_sq.reserve(sizeof(double) * 3 * npix));
+    TC_CUDA(ctx, cudaMemsetAsync(ctx->accum.ptr, 0, sizeof(double) * 3 * npix, st));
+    if (moments) TC_CUDA(ctx, cudaMemsetAsync(ctx->accum_sq.ptr, 0, sizeof(double) * 3 * npix, st));
+    ctx->width = p->width;
+    ctx->height = p->height;
+    ctx->accumulated = 0;
+    ctx->has_moments = moments;
+  } else {
+    if (p->width != ctx->width || p->height != ctx->height)
+      return fail(ctx, TC_ERR_STATE, "progressive batch changes the image size");
+    if (p->accumulated_samples != ctx->accumulated)
+      return fail(ctx, TC_ERR_STATE, "accumulated_samples " + std::to_string(p->accumulated_samples) +
+                                          " does not match the " + std::to_string(ctx->accumulated) +
+                                          " samples held by the context");
+    if (moments && !ctx->has_moments)
+      return fail(ctx, TC_ERR_STATE, "keep_moments must be set from the first batch of an accumulation");
+  }
+  if (uint64_t(ctx->accumulated) + p->samples > 0xFFFFFFFFull)
+    return fail(ctx, TC_ERR_INVALID, "progressive accumulated sample count overflowed");
+
+  tcb::RenderLaunch L{};
+  L.scene = ctx->scene;
+  L.width = p->width;
+  L.height = p->height;
+  L.samples = p->samples;
+  L.max_bounces = p->max_bounces;
+  L.frame_index = p->frame_index;
+  L.sample_base = ctx->accumulated;
+  L.samples_per_item = std::min<uint32_t>(o.samples_per_item ? o.samples_per_item : 4u, p->samples);
+  L.items_per_pixel = (p->samples + L.samples_per_item - 1) / L.samples_per_item;
+  L.total_items = uint64_t(npix) * L.items_per_pixel;
+  L.accum = ctx->accum.as<double>();
+  L.accum_sq = moments ? ctx->accum_sq.as<double>() : nullptr;
+  L.work_counter = ctx->work_counter.as<unsigned long long>();
+  L.counters = ctx->counters.as<unsigned long long>();
+  TC_CUDA(ctx, cudaMemsetAsync(ctx->work_counter.ptr, 0, sizeof(unsigned long long), st));
+  TC_CUDA(ctx, cudaMemsetAsync(ctx->counters.ptr, 0, 4 * sizeof(unsigned long long), st));
+  const int block = o.block_size ? int(o.block_size) : 128;
+  if (block % 32 != 0 || block < 32 || block > 256)
+    return fail(ctx, TC_ERR_INVALID, "block_size must be a multiple of 32 in [32, 256]");
+  int per_sm = tcb::render_max_blocks_per_sm(block, moments);
+  if (per_sm <= 0) return fail(ctx, TC_ERR_CUDA, "render kernel cannot be resident with this block size");
+  const int grid = per_sm * ctx->sm_count;
+  TC_CUDA(ctx, cudaEventRecord(ctx->ev_kernel0, st));
+  TC_CUDA(ctx, tcb::launch_render(L, block, grid, moments, st));
+  TC_CUDA(ctx, cudaEventRecord(ctx->ev_kernel1, st));
+  unsigned long long counters[4] = {0, 0, 0, 0};
+  TC_CUDA(ctx, cudaMemcpyAsync(counters, ctx->counters.ptr, sizeof(counters), cudaMemcpyDeviceToHost, st));
+  TC_CUDA(ctx, cudaEventRecord(ctx->ev_end, st));
+  TC_CUDA(ctx, cudaStreamSynchronize(st));
+  ctx->accumulated += p->samples;
+  ctx->stats.paths = counters[0];
+  ctx->stats.extension_rays = counters[1];
+  ctx->stats.shadow_rays = counters[2];
+  ctx->stats.rays = counters[1] + counters[2];
+  cudaEventElapsedTime(&ctx->stats.kernel_ms, ctx->ev_kernel0, ctx->ev_kernel1);
+  cudaEventElapsedTime(&ctx->stats.total_ms, ctx->ev_begin, ctx->ev_end);
+  if (counters[0] != uint64_t(npix) * p->samples)
+    return fail(ctx, TC_ERR_DEVICE_STATUS, "path kernel completed " + std::to_string(counters[0]) + " of " +
+                                                std::to_string(uint64_t(npix) * p->samples) + " paths");
+  return TC_OK;
+}
+
+int tc_readback(tc_context* ctx, float* rgba, size_t n_floats) {
+  if (!ctx) return fail(nullptr, TC_ERR_INVALID, "context is null");
+  if (!rgba) return fail(ctx, TC_ERR_INVALID, "output buffer is null");
+  if (ctx->accumulated == 0) return fail(ctx, TC_ERR_STATE, "tc_readback before tc_render");
+  const size_t npix = size_t(ctx->width) * ctx->height;
+  if (n_floats < 4 * npix) return fail(ctx, TC_ERR_INVALID, "output buffer holds fewer than 4*width*height floats");
+  TC_CUDA(ctx, cudaSetDevice(ctx->device));
+  TC_CUDA(ctx, tcb::launch_resolve(ctx->accum.as<double>(), uint32_t(npix), 1.0 / double(ctx->accumulated),
+                                   ctx->image.as<float4>(), ctx->stream));
+  TC_CUDA(ctx, cudaMemcpyAsync(rgba, ctx->image.ptr, sizeof(float4) * npix, cudaMemcpyDeviceToHost, ctx->stream));
+  TC_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return TC_OK;
+}
+
+int tc_readback_sums(tc_context* ctx, double* sum, double* sum_sq, size_t n_doubles, uint32_t* samples) {
+  if (!ctx) return fail(nullptr, TC_ERR_INVALID, "context is null");
+  if (ctx->accumulated == 0) return fail(ctx, TC_ERR_STATE, "tc_readback_sums before tc_render");
+  const size_t n = size_t(3) * ctx->width * ctx->height;
+  if ((sum || sum_sq) && n_doubles < n) return fail(ctx, TC_ERR_INVALID, "buffer holds fewer than 3*width*height doubles");
+  if (sum_sq && !ctx->has_moments) return fail(ctx, TC_ERR_STATE, "moments were not kept for this accumulation");
+  TC_CUDA(ctx, cudaSetDevice(ctx->device));
+  if (sum) TC_CUDA(ctx, cudaMemcpyAsync(sum, ctx->accum.ptr, sizeof(double) * n, cudaMemcpyDeviceToHost, ctx->stream));
+  if (sum_sq)
+    TC_CUDA(ctx, cudaMemcpyAsync(sum_sq, ctx->accum_sq.ptr, sizeof(double) * n, cudaMemcpyDeviceToHost, ctx->stream));
+  TC_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  if (samples) *samples = ctx->accumulated;
+  return TC_OK;
+}
+
+int tc_trace_closest_device_async(tc_context* ctx, const float* d_rays, size_t n, float tmin, uint32_t* d_prim,
+                                  float* d_t, void* stream) {
+  if (!ctx) return fail(nullptr, TC_ERR_INVALID, "context is null");
+  if (!ctx->has_scene) return fail(ctx, TC_ERR_STATE, "trace before tc_upload_scene");
+  if (n && (!d_rays || !d_prim || !d_t)) return fail(ctx, TC_ERR_INVALID, "ray or output pointer is null");
+  TC_CUDA(ctx, cudaSetDevice(ctx->device));
+  cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : ctx->stream;
+  TC_CUDA(ctx, tcb::launch_trace_closest(ctx->scene, d_rays, n, tmin, d_prim, d_t, st));
+  return TC_OK;
+}
+
+int tc_trace_closest(tc_context* ctx, const float* rays, size_t n, float tmin, uint32_t* prim, float* t) {
+  if (!ctx) return fail(nullptr, TC_ERR_INVALID, "context is null");
+  if (!ctx->has_scene) return fail(ctx, TC_ERR_STATE, "trace before tc_upload_scene");
+  if (n == 0) return TC_OK;
+  if (!rays || !prim || !t) return fail(ctx, TC_ERR_INVALID, "ray or output pointer is null");
+  TC_CUDA(ctx, cudaSetDevice(ctx->device));
+  cudaStream_t st = ctx->stream;
+  TC_CUDA(ctx, ctx->ray_buf.reserve(sizeof(float) * 6 * n));
+  TC_CUDA(ctx, ctx->prim_buf.reserve(sizeof(uint32_t) * n));
+  TC_CUDA(ctx, ctx->t_buf.reserve(sizeof(float) * n));
+  TC_CUDA(ctx, cudaEventRecord(ctx->ev_begin, st));
+  TC_CUDA(ctx, cudaMemcpyAsync(ctx->ray_buf.ptr, rays, sizeof(float) * 6 * n, cudaMemcpyHostToDevice, st));
+  TC_CUDA(ctx, cudaEventRecord(ctx->ev_kernel0, st));
+  TC_CUDA(ctx, tcb::launch_trace_closest(ctx->scene, ctx->ray_buf.as<float>(), n, tmin, ctx->prim_buf.as<uint32_t>(),
+                                         ctx->t_buf.as<float>(), st));
+  TC_CUDA(ctx, cudaEventRecord(ctx->ev_kernel1, st));
+  TC_CUDA(ctx, cudaMemcpyAsync(prim, ctx->prim_buf.ptr, sizeof(uint32_t) * n, cudaMemcpyDeviceToHost, st));
+  TC_CUDA(ctx, cudaMemcpyAsync(t, ctx->t_buf.ptr, sizeof(float) * n, cudaMemcpyDeviceToHost, st));
+  TC_CUDA(ctx, cudaEventRecord(ctx->ev_end, st));
+  TC_CUDA(ctx, cudaStreamSynchronize(st));
+  cudaEventElapsedTime(&ctx->stats.kernel_ms, ctx->ev_kernel0, ctx->ev_kernel1);
+  cudaEventElapsedTime(&ctx->stats.total_ms, ctx->ev_begin, ctx->ev_end);
+  ctx->stats.rays = n;
+  ctx->stats.extension_rays = n;
+  ctx->stats.shadow_rays = 0;
+  ctx->stats.paths = 0;
+  return TC_OK;
+}
+
+int tc_get_stats(const tc_context* ctx, tc_stats* out) {
+  if (!ctx || !out) return fail(nullptr, TC_ERR_INVALID, "context or output is null");
+  *out = ctx->stats;
+  return TC_OK;
+}
+
+long tc_build_bvh_host(const tc_gpu_sphere* spheres, size_t n_spheres, const tc_gpu_triangle* triangles,
+                       size_t n_triangles, tc_gpu_bvh_node* nodes, size_t node_capacity, tc_gpu_primitive_ref* prims,
+                       size_t prim_capacity) {
+  if ((n_spheres && !spheres) || (n_triangles && !triangles))
+    return fail(nullptr, TC_ERR_INVALID, "geometry pointer is null for a nonzero count");
+  std::vector<tcb::SphereIn> sph(n_spheres);
+  for (size_t i = 0; i < n_spheres; ++i)
+    sph[i] = tcb::SphereIn{{spheres[i].center_radius[0], spheres[i].center_radius[1], spheres[i].center_radius[2]},
+                           spheres[i].center_radius[3]};
+  std::vector<tcb::TriangleIn> tri(n_triangles);
+  for (size_t i = 0; i < n_triangles; ++i)
+    for (int c = 0; c < 3; ++c) {
+      tri[i].v[0][c] = triangles[i].v0[c];
+      tri[i].v[1][c] = triangles[i].v1[c];
+      tri[i].v[2][c] = triangles[i].v2[c];
+    }
+  tcb::FlatHierarchy flat = tcb::build_median_split(sph.data(), sph.size(), tri.data(), tri.size());
+  if (flat.nodes.size() > node_capacity || flat.prims.size() > prim_capacity)
+    return fail(nullptr, TC_ERR_INVALID, "output capacity is too small for the hierarchy");
+  if ((!nodes && !flat.nodes.empty()) || (!prims && !flat.prims.empty()))
+    return fail(nullptr, TC_ERR_INVALID, "output pointer is null");
+  for (size_t i = 0; i < flat.nodes.size(); ++i) {
+    tc_gpu_bvh_node& o = nodes[i];
+    std::memset(&o, 0, sizeof(o));
+    for (int c = 0; c < 3; ++c) {
+      o.min[c] = flat.nodes[i].min[c];
+      o.max[c] = flat.nodes[i].max[c];
+    }
+    o.first_or_right = flat.nodes[i].first_or_right;
+    o.primitive_count = flat.nodes[i].count;
+  }
+  for (size_t i = 0; i < flat.prims.size(); ++i) prims[i] = tc_gpu_primitive_ref{flat.prims[i].kind, flat.prims[i].index};
+  return long(flat.nodes.size());
+}
+
+}  // extern "C"

@@ -1,0 +1,66 @@
+// Kernel-facing view of one uploaded scene and the launch interface between the host runtime
+// (api.cu) and the kernels (kernels.cu).
+#ifndef TOASTER_B200_DEVICE_SCENE_H
+#define TOASTER_B200_DEVICE_SCENE_H
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "layout.h"
+
+namespace tcb {
+
+struct DevScene {
+  const PairNode* pairs;
+  const PrimRecord* prims;
+  ChildRec root;
+  const DevMaterial* materials;
+  uint32_t material_count;
+  uint32_t light_count;
+  const DevLight* lights;
+  const float4* attributes;  // GpuTriangleAttributes as 5 float4 per triangle, or null
+  const uint32_t* texels;    // packed RGBA8 texture atlas, or null
+  // Environment (lat-long): RGB texels, marginal row CDF (H), conditional row CDFs (W*H) and the
+  // per-texel solid-angle density numerator p(x,y)*W*H/(2*pi^2) (W*H), all FP32 built from FP64
+  // prefix sums.
+  const float4* env_rgb;
+  const float* env_marginal;
+  const float* env_conditional;
+  const float* env_pdf;
+  uint32_t env_width, env_height;
+  float env_intensity;
+  float env_rotation_turns;  // rotation_degrees / 360
+  uint32_t env_sampleable;   // 1 when the importance distribution has positive mass
+  uint32_t background;       // 0 sky, 1 black, 2 environment
+  float cam_origin[3], cam_lower_left[3], cam_horizontal[3], cam_vertical[3];
+};
+
+struct RenderLaunch {
+  DevScene scene;
+  uint32_t width, height, samples, max_bounces;
+  uint32_t frame_index;
+  uint32_t sample_base;        // samples already accumulated (decorrelates progressive batches)
+  uint32_t samples_per_item;   // samples a lane traces for one pixel before fetching new work
+  uint32_t items_per_pixel;
+  uint64_t total_items;
+  double* accum;               // 3 doubles per pixel (running sums)
+  double* accum_sq;            // 3 doubles per pixel or null
+  unsigned long long* work_counter;
+  unsigned long long* counters;  // [0] paths, [1] extension rays, [2] shadow rays
+};
+
+// Launchers implemented in kernels.cu. All enqueue on `stream` and return the launch error.
+cudaError_t launch_trace_closest(const DevScene& s, const float* rays, uint64_t n, float tmin, uint32_t* prim,
+                                 float* t, cudaStream_t stream);
+cudaError_t launch_render(const RenderLaunch& r, int block_size, int grid_size, bool moments, cudaStream_t stream);
+int render_max_blocks_per_sm(int block_size, bool moments);
+cudaError_t launch_resolve(const double* accum, uint32_t pixels, double inv_samples, float4* out,
+                           cudaStream_t stream);
+// Environment importance tables from RGB texels; `row_sums` is FP64 scratch of H entries.
+cudaError_t launch_env_tables(const float4* rgb, uint32_t w, uint32_t h, float intensity, float* marginal,
+                              float* conditional, float* pdf, double* row_sums, double* total_out,
+                              cudaStream_t stream);
+
+}  // namespace tcb
+
+#endif

@@ -1,0 +1,735 @@
+// CUDA kernels of the toaster B200 path tracer (sm_100a).
+//
+//   trace_closest_kernel  closest-hit parity hook: one ray per thread, exact traversal
+//   render_kernel         persistent path-tracing megakernel (camera rays, BSDFs, NEE over area
+//                         lights and the environment, MIS, FP64 per-pixel accumulation)
+//   env_* kernels         FP64 prefix sums for the 2-D environment importance distribution
+//   resolve_kernel        FP64 sums -> linear-HDR float4 averages
+//
+// The estimator is the one of crates/toaster-cpu/src/integrator.rs:99-244, written as an
+// iterative state machine so that every lane issues exactly one ray per loop iteration
+// (extension, light shadow or environment shadow). All lanes therefore run the traversal loop
+// together; idle lanes are refilled with new (pixel, sample-range) work items through one
+// warp-aggregated atomic (ballot + popc + shuffle) instead of idling until the warp drains.
+#include <cuda_runtime.h>
+#include <math_constants.h>
+#include <stdint.h>
+
+#include "device_scene.h"
+#include "traverse.cuh"
+
+namespace tcb {
+
+constexpr float kPiF = 3.14159265358979323846f;
+constexpr float kRayEps = 0.001f;           // integrator.rs:11 RAY_EPSILON
+constexpr float kOneMinusEps = 0.99999994f;  // 1 - f32::EPSILON (environment.rs:281-287)
+
+// ------------------------------------------------------------------------ small vector math
+struct V3 {
+  float x, y, z;
+};
+__device__ __forceinline__ V3 mk(float x, float y, float z) { return V3{x, y, z}; }
+__device__ __forceinline__ V3 operator+(V3 a, V3 b) { return V3{a.x + b.x, a.y + b.y, a.z + b.z}; }
+__device__ __forceinline__ V3 operator-(V3 a, V3 b) { return V3{a.x - b.x, a.y - b.y, a.z - b.z}; }
+__device__ __forceinline__ V3 operator-(V3 a) { return V3{-a.x, -a.y, -a.z}; }
+__device__ __forceinline__ V3 operator*(V3 a, V3 b) { return V3{a.x * b.x, a.y * b.y, a.z * b.z}; }
+__device__ __forceinline__ V3 operator*(V3 a, float s) { return V3{a.x * s, a.y * s, a.z * s}; }
+__device__ __forceinline__ V3 operator*(float s, V3 a) { return V3{a.x * s, a.y * s, a.z * s}; }
+__device__ __forceinline__ float dot(V3 a, V3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+__device__ __forceinline__ V3 cross(V3 a, V3 b) {
+  return V3{a.y * b.z - b.y * a.z, a.z * b.x - b.z * a.x, a.x * b.y - b.x * a.y};
+}
+__device__ __forceinline__ V3 normalize(V3 a) { return a * rsqrtf(dot(a, a)); }
+__device__ __forceinline__ V3 lerp3(V3 a, V3 b, float s) { return a + (b - a) * s; }
+
+// ------------------------------------------------------------------------ random numbers
+// PCG32 (O'Neill 2014, XSH-RR) seeded per (frame, pixel, sample) through SplitMix64, so any
+// sample of any pixel can be regenerated independently of scheduling.
+__device__ __forceinline__ uint64_t splitmix64(uint64_t x) {
+  x += 0x9E3779B97F4A7C15ull;
+  x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
+  x = (x ^ (x >> 27)) * 0x94D049BB133111EBull;
+  return x ^ (x >> 31);
+}
+struct Pcg {
+  uint64_t state, inc;
+  __device__ __forceinline__ void seed(uint32_t frame, uint32_t pixel, uint32_t sample) {
+    const uint64_t k = splitmix64(splitmix64((uint64_t(frame) << 32) ^ pixel ^ 0xA0761D6478BD642Full) ^ sample);
+    state = k;
+    inc = splitmix64(k) | 1ull;
+  }
+  __device__ __forceinline__ uint32_t next() {
+    const uint64_t old = state;
+    state = old * 6364136223846793005ull + inc;
+    const uint32_t xs = uint32_t(((old >> 18u) ^ old) >> 27u);
+    const uint32_t rot = uint32_t(old >> 59u);
+    return (xs >> rot) | (xs << ((32u - rot) & 31u));
+  }
+  __device__ __forceinline__ float uniform() { return float(next() >> 8) * (1.0f / 16777216.0f); }
+};
+
+// ------------------------------------------------------------------------ environment
+__device__ __forceinline__ float unit_interval(float v) { return fminf(fmaxf(v, 0.0f), kOneMinusEps); }
+
+__device__ __forceinline__ float rem_euclid1(float a) {
+  float r = fmodf(a, 1.0f);
+  return r < 0.0f ? r + 1.0f : r;
+}
+
+// environment.rs:237-241: horizontal wrap, vertical clamp.
+__device__ __forceinline__ V3 env_texel(const DevScene& s, int x, int y) {
+  const int w = int(s.env_width), h = int(s.env_height);
+  x %= w;
+  if (x < 0) x += w;
+  y = min(max(y, 0), h - 1);
+  const float4 t = __ldg(s.env_rgb + size_t(y) * s.env_width + x);
+  return mk(t.x, t.y, t.z);
+}
+
+// environment.rs:132-152: bilinear lat-long lookup times intensity.
+__device__ V3 env_radiance(const DevScene& s, V3 d) {
+  const float l2 = dot(d, d);
+  if (!(l2 > 0.0f) || isinf(l2)) return mk(0.f, 0.f, 0.f);
+  d = d * rsqrtf(l2);
+  const float u = rem_euclid1(atan2f(d.z, d.x) / (2.0f * kPiF) + 0.5f + s.env_rotation_turns);
+  const float v = acosf(fminf(fmaxf(d.y, -1.0f), 1.0f)) / kPiF;
+  const float x = u * float(s.env_width) - 0.5f;
+  const float y = v * float(s.env_height) - 0.5f;
+  const float fx = floorf(x), fy = floorf(y);
+  const int x0 = int(fx), y0 = int(fy);
+  const float ax = x - fx, ay = y - fy;
+  const V3 top = lerp3(env_texel(s, x0, y0), env_texel(s, x0 + 1, y0), ax);
+  const V3 bottom = lerp3(env_texel(s, x0, y0 + 1), env_texel(s, x0 + 1, y0 + 1), ax);
+  return lerp3(top, bottom, ay) * s.env_intensity;
+}
+
+// environment.rs:193-200 and :225-234: density per steradian of the importance distribution.
+__device__ float env_pdf(const DevScene& s, V3 d) {
+  if (!s.env_sampleable) return 0.0f;
+  const float l2 = dot(d, d);
+  if (!(l2 > 0.0f) || isinf(l2)) return 0.0f;
+  d = d * rsqrtf(l2);
+  const float u = rem_euclid1(atan2f(d.z, d.x) / (2.0f * kPiF) + 0.5f + s.env_rotation_turns);
+  const float theta = acosf(fminf(fmaxf(d.y, -1.0f), 1.0f));
+  const float v = theta / kPiF;
+  const uint32_t x = uint32_t(floorf(u * float(s.env_width))) % s.env_width;
+  const uint32_t y = min(uint32_t(floorf(v * float(s.env_height))), s.env_height - 1);
+  const float p = __ldg(s.env_pdf + size_t(y) * s.env_width + x);
+  const float st = sinf(theta);
+  return (p > 0.0f && st > 0.0f) ? p / st : 0.0f;
+}
+
+// First index in [0, n) whose CDF value is > x (the reference's partition_point(c <= x)).
+__device__ __forceinline__ uint32_t upper_bound(const float* cdf, uint32_t n, float x) {
+  uint32_t lo = 0, hi = n;
+  while (lo < hi) {
+    const uint32_t mid = (lo + hi) >> 1;
+    if (__ldg(cdf + mid) <= x) lo = mid + 1;
+    else hi = mid;
+  }
+  return lo;
+}
+
+// environment.rs:159-189 with the flat CDF split into a marginal row CDF and conditional column
+// CDFs: the same texel probabilities, found with two short searches instead of one long one.
+__device__ bool env_sample(const DevScene& s, float u1, float u2, float u3, V3& dir, V3& rad, float& pdf) {
+  if (!s.env_sampleable) return false;
+  const float sel = unit_interval(u1);
+  const uint32_t y = min(upper_bound(s.env_marginal, s.env_height, sel), s.env_height - 1);
+  const float lo = y ? __ldg(s.env_marginal + y - 1) : 0.0f;
+  const float hi = __ldg(s.env_marginal + y);
+  const float sel2 = unit_interval((sel - lo) / (hi - lo));
+  const float* row = s.env_conditional + size_t(y) * s.env_width;
+  const uint32_t x = min(upper_bound(row, s.env_width, sel2), s.env_width - 1);
+  const float u = (float(x) + unit_interval(u2)) / float(s.env_width);
+  const float v = (float(y) + unit_interval(u3)) / float(s.env_height);
+  const float theta = kPiF * v;
+  const float phi = 2.0f * kPiF * (u - 0.5f - s.env_rotation_turns);
+  float st, ct, sp, cp;
+  sincosf(theta, &st, &ct);
+  sincosf(phi, &sp, &cp);
+  dir = mk(st * cp, ct, st * sp);
+  const float p = __ldg(s.env_pdf + size_t(y) * s.env_width + x);
+  pdf = (p > 0.0f && st > 0.0f) ? p / st : 0.0f;
+  rad = env_radiance(s, dir);
+  return true;
+}
+
+// ------------------------------------------------------------------------ materials
+__device__ __forceinline__ float srgb_to_linear(float v) {
+  return v <= 0.04045f ? v / 12.92f : powf((v + 0.055f) / 1.055f, 2.4f);
+}
+__device__ V3 texel_linear(const DevScene& s, const DevMaterial& m, int x, int y) {
+  const int w = int(m.tex_width), h = int(m.tex_height);
+  x %= w; if (x < 0) x += w;
+  y %= h; if (y < 0) y += h;
+  const uint32_t px = __ldg(s.texels + m.tex_offset + uint32_t(y) * m.tex_width + uint32_t(x));
+  const float k = 1.0f / 255.0f;
+  return mk(srgb_to_linear(float(px & 255u) * k), srgb_to_linear(float((px >> 8) & 255u) * k),
+            srgb_to_linear(float((px >> 16) & 255u) * k));
+}
+// Textured diffuse albedo (integrator.rs:340-350; pathtrace_spheres.wgsl:247-273).
+__device__ V3 base_color(const DevScene& s, const DevMaterial& m, float tu, float tv) {
+  const V3 a = mk(m.albedo[0], m.albedo[1], m.albedo[2]);
+  if (m.tex_width == 0 || m.tex_height == 0 || s.texels == nullptr) return a;
+  const float u = tu - floorf(tu), v = tv - floorf(tv);
+  const float px = u * float(m.tex_width) - 0.5f, py = v * float(m.tex_height) - 0.5f;
+  const int bx = int(floorf(px)), by = int(floorf(py));
+  const float ax = px - floorf(px), ay = py - floorf(py);
+  const V3 top = lerp3(texel_linear(s, m, bx, by), texel_linear(s, m, bx + 1, by), ax);
+  const V3 bottom = lerp3(texel_linear(s, m, bx, by + 1), texel_linear(s, m, bx + 1, by + 1), ax);
+  return a * lerp3(top, bottom, ay);
+}
+
+__device__ __forceinline__ V3 uniform_sphere(float u1, float u2) {
+  const float z = 1.0f - 2.0f * u1;
+  const float r = sqrtf(fmaxf(0.0f, 1.0f - z * z));
+  float sp, cp;
+  sincosf(2.0f * kPiF * u2, &sp, &cp);
+  return mk(r * cp, r * sp, z);
+}
+// Uniform point in the unit ball: the distribution of random_in_unit_sphere (integrator.rs:377).
+__device__ __forceinline__ V3 uniform_ball(float u1, float u2, float u3) {
+  return uniform_sphere(u1, u2) * cbrtf(u3);
+}
+__device__ __forceinline__ V3 reflect(V3 d, V3 n) { return d - 2.0f * dot(d, n) * n; }
+__device__ __forceinline__ V3 refract(V3 d, V3 n, float ratio) {
+  const float ct = fminf(dot(-d, n), 1.0f);
+  const V3 perp = ratio * (d + ct * n);
+  const V3 par = -sqrtf(fabsf(1.0f - dot(perp, perp))) * n;
+  return perp + par;
+}
+__device__ __forceinline__ float schlick(float cosine, float ratio) {
+  float r0 = (1.0f - ratio) / (1.0f + ratio);
+  r0 = r0 * r0;
+  const float m = 1.0f - cosine;
+  return r0 + (1.0f - r0) * (m * m * m * m * m);
+}
+__device__ __forceinline__ float power_heuristic(float a, float b) {
+  const float a2 = a * a, b2 = b * b, d = a2 + b2;
+  return d > 0.0f ? a2 / d : 0.0f;
+}
+
+// ------------------------------------------------------------------------ parity kernel
+__global__ void trace_closest_kernel(const DevScene s, const float* __restrict__ rays, uint64_t n, float tmin,
+                                     uint32_t* __restrict__ prim, float* __restrict__ tout) {
+  const uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float* r = rays + 6 * i;
+  const RayQ q = make_ray(r[0], r[1], r[2], r[3], r[4], r[5]);
+  TraceResult tr;
+  uint32_t visits = 0;
+  const bool hit = trace_ray(s.pairs, s.prims, s.root, q, tmin, CUDART_INF_F, false, tr, visits);
+  prim[i] = hit ? (tr.tag & ~kTagLast) : 0xFFFFFFFFu;
+  tout[i] = hit ? tr.t : CUDART_INF_F;
+}
+
+cudaError_t launch_trace_closest(const DevScene& s, const float* rays, uint64_t n, float tmin, uint32_t* prim,
+                                 float* t, cudaStream_t stream) {
+  if (n == 0) return cudaSuccess;
+  const int block = 128;
+  const uint64_t grid = (n + block - 1) / block;
+  trace_closest_kernel<<<unsigned(grid), block, 0, stream>>>(s, rays, n, tmin, prim, t);
+  return cudaGetLastError();
+}
+
+// ------------------------------------------------------------------------ path kernel
+enum Phase : int { kIdle = 0, kExtend = 1, kShadowLight = 2, kShadowEnv = 3, kScatter = 4 };
+
+struct Lane {
+  V3 ro, rd;         // next ray
+  V3 thr;            // path throughput
+  V3 rad;            // radiance of the current sample
+  V3 hp, hn, alb;    // diffuse vertex: point, shading normal, albedo
+  V3 pend;           // contribution of the pending shadow ray if unoccluded
+  V3 acc;            // radiance sum of the current work item
+  V3 acc2;           // squared-sample sum of the current work item
+  float bsdf_pdf;    // solid-angle pdf of the last diffuse bounce, < 0 for none
+  float tmax;        // distance limit of the pending ray
+  int phase;
+  int depth;         // remaining depth (ray_color_inner's remaining_depth)
+  bool include_emission;
+  uint32_t pixel, item_samples, item_done, sample;
+  Pcg rng;
+};
+
+__device__ __forceinline__ void start_sample(const RenderLaunch& L, Lane& ln) {
+  const DevScene& s = L.scene;
+  ln.rng.seed(L.frame_index, ln.pixel, ln.sample);
+  const uint32_t x = ln.pixel % L.width, y = ln.pixel / L.width;
+  const float u = (float(x) + ln.rng.uniform()) / float(L.width);
+  const float v = 1.0f - (float(y) + ln.rng.uniform()) / float(L.height);
+  const V3 o = mk(s.cam_origin[0], s.cam_origin[1], s.cam_origin[2]);
+  const V3 ll = mk(s.cam_lower_left[0], s.cam_lower_left[1], s.cam_lower_left[2]);
+  const V3 h = mk(s.cam_horizontal[0], s.cam_horizontal[1], s.cam_horizontal[2]);
+  const V3 vv = mk(s.cam_vertical[0], s.cam_vertical[1], s.cam_vertical[2]);
+  ln.ro = o;
+  ln.rd = normalize(ll + u * h + v * vv - o);
+  ln.thr = mk(1.f, 1.f, 1.f);
+  ln.rad = mk(0.f, 0.f, 0.f);
+  ln.depth = int(L.max_bounces);
+  ln.include_emission = true;
+  ln.bsdf_pdf = -1.0f;
+  ln.phase = kExtend;
+}
+
+template <bool kMoments>
+__device__ __forceinline__ void finish_sample(const RenderLaunch& L, Lane& ln, uint32_t& n_paths) {
+  ln.acc = ln.acc + ln.rad;
+  if (kMoments) ln.acc2 = ln.acc2 + ln.rad * ln.rad;
+  ++n_paths;
+  ++ln.item_done;
+  ++ln.sample;
+  if (ln.item_done >= ln.item_samples) {
+    double* a = L.accum + size_t(3) * ln.pixel;
+    atomicAdd(a, double(ln.acc.x));
+    atomicAdd(a + 1, double(ln.acc.y));
+    atomicAdd(a + 2, double(ln.acc.z));
+    if (kMoments) {
+      double* q = L.accum_sq + size_t(3) * ln.pixel;
+      atomicAdd(q, double(ln.acc2.x));
+      atomicAdd(q + 1, double(ln.acc2.y));
+      atomicAdd(q + 2, double(ln.acc2.z));
+    }
+    ln.phase = kIdle;
+  } else {
+    start_sample(L, ln);
+  }
+}
+
+// Light-sampling shadow ray (integrator.rs:168-205); false when the sample contributes nothing.
+__device__ __forceinline__ bool prepare_light_shadow(const DevScene& s, Lane& ln) {
+  if (s.light_count == 0) return false;
+  const float u1 = ln.rng.uniform(), u2 = ln.rng.uniform(), u3 = ln.rng.uniform();
+  const float scaled = u1 * float(s.light_count);
+  uint32_t i = min(uint32_t(scaled), s.light_count - 1);
+  const DevLight* Lt = s.lights + i;
+  if (scaled - float(i) >= __ldg(&Lt->alias_prob)) Lt = s.lights + __ldg(&Lt->alias);
+  const DevLight lt = *Lt;
+  V3 pos, nrm;
+  if (lt.kind == 0) {
+    const float su = sqrtf(u2);
+    const float w1 = su * (1.0f - u3), w2 = su * u3;
+    pos = mk(lt.p0[0], lt.p0[1], lt.p0[2]) + mk(lt.e1[0], lt.e1[1], lt.e1[2]) * w1 + mk(lt.e2[0], lt.e2[1], lt.e2[2]) * w2;
+    nrm = mk(lt.normal[0], lt.normal[1], lt.normal[2]);
+  } else {
+    nrm = uniform_sphere(u2, u3);
+    pos = mk(lt.p0[0], lt.p0[1], lt.p0[2]) + nrm * lt.radius;
+  }
+  const V3 so = ln.hp + ln.hn * kRayEps;
+  const V3 to = pos - so;
+  const float d2 = dot(to, to);
+  if (d2 <= kRayEps * kRayEps) return false;
+  const float dist = sqrtf(d2);
+  const V3 dir = to * (1.0f / dist);
+  const float cs = fmaxf(dot(ln.hn, dir), 0.0f);
+  const float cl = fmaxf(dot(nrm, -dir), 0.0f);
+  if (cs <= 0.0f || cl <= 0.0f) return false;
+  const float scale = cs * cl / (kPiF * d2 * lt.pdf_area);
+  ln.pend = ln.thr * ln.alb * mk(lt.emission[0], lt.emission[1], lt.emission[2]) * scale;
+  ln.ro = so;
+  ln.rd = dir;
+  // Occluded iff the closest hit lies strictly before dist - 2*eps (integrator.rs:196-199).
+  ln.tmax = nextafterf(dist - 2.0f * kRayEps, -CUDART_INF_F);
+  return true;
+}
+
+// Environment-sampling shadow ray with the power heuristic (integrator.rs:208-244).
+__device__ __forceinline__ bool prepare_env_shadow(const DevScene& s, Lane& ln) {
+  if (s.background != 2u || !s.env_sampleable) return false;
+  const float u1 = ln.rng.uniform(), u2 = ln.rng.uniform(), u3 = ln.rng.uniform();
+  V3 dir, rad;
+  float pdf;
+  if (!env_sample(s, u1, u2, u3, dir, rad, pdf)) return false;
+  const float cs = fmaxf(dot(ln.hn, dir), 0.0f);
+  if (cs <= 0.0f || pdf <= 0.0f) return false;
+  const float mis = power_heuristic(pdf, cs / kPiF);
+  ln.pend = ln.thr * ln.alb * rad * (cs * mis / (kPiF * pdf));
+  ln.ro = ln.hp + ln.hn * kRayEps;
+  ln.rd = dir;
+  ln.tmax = CUDART_INF_F;
+  return true;
+}
+
+__device__ __forceinline__ V3 background(const DevScene& s, V3 d, float bsdf_pdf) {
+  if (s.background == 0u) {
+    const V3 dn = normalize(d);
+    return lerp3(mk(1.f, 1.f, 1.f), mk(0.35f, 0.65f, 1.0f), 0.5f * (dn.y + 1.0f));
+  }
+  if (s.background != 2u || s.env_width == 0) return mk(0.f, 0.f, 0.f);
+  const V3 r = env_radiance(s, d);
+  const float w = bsdf_pdf >= 0.0f ? power_heuristic(bsdf_pdf, env_pdf(s, d)) : 1.0f;
+  return r * w;
+}
+
+template <bool kMoments>
+__device__ __forceinline__ void shade_hit(const RenderLaunch& L, Lane& ln, const TraceResult& tr, uint32_t& n_paths) {
+  const DevScene& s = L.scene;
+  const float4* p = reinterpret_cast<const float4*>(s.prims + tr.rec);
+  const float4 A = __ldg(p), B = __ldg(p + 1);
+  const V3 hp = ln.ro + ln.rd * tr.t;
+  V3 nrm;
+  float tu = 0.0f, tv = 0.0f;
+  bool front;
+  uint32_t mat;
+  if (tr.tag & kTagTriangle) {
+    const float4 C = __ldg(p + 2);
+    const V3 e1 = mk(B.x, B.y, B.z), e2 = mk(C.x, C.y, C.z);
+    const V3 gn = normalize(cross(e1, e2));
+    front = dot(ln.rd, gn) < 0.0f;
+    V3 outward = gn;
+    const uint32_t flags = __float_as_uint(C.w);
+    if (flags != 0u && s.attributes != nullptr) {
+      // Barycentrics for attribute interpolation (intersect.rs:124-135).
+      const V3 sv = ln.ro - mk(A.x, A.y, A.z);
+      const V3 pv = cross(ln.rd, e2);
+      const float inv = 1.0f / dot(e1, pv);
+      const float u = dot(sv, pv) * inv;
+      const V3 qv = cross(sv, e1);
+      const float v = dot(ln.rd, qv) * inv;
+      const float w0 = 1.0f - u - v;
+      const float4* at = s.attributes + size_t(5) * (tr.tag & kTagIndexMask);
+      if (flags & 1u) {
+        const float4 n0 = __ldg(at), n1 = __ldg(at + 1), n2 = __ldg(at + 2);
+        outward = normalize(mk(n0.x, n0.y, n0.z) * w0 + mk(n1.x, n1.y, n1.z) * u + mk(n2.x, n2.y, n2.z) * v);
+        if (dot(outward, gn) < 0.0f) outward = -outward;
+      }
+      if (flags & 2u) {
+        const float4 uv01 = __ldg(at + 3), uv2 = __ldg(at + 4);
+        tu = w0 * uv01.x + u * uv01.z + v * uv2.x;
+        tv = w0 * uv01.y + u * uv01.w + v * uv2.y;
+      }
+    }
+    nrm = front ? outward : -outward;
+    mat = __float_as_uint(B.w);
+  } else {
+    const V3 outward = (hp - mk(A.x, A.y, A.z)) * (1.0f / B.x);
+    front = dot(ln.rd, outward) < 0.0f;
+    nrm = front ? outward : -outward;
+    mat = __float_as_uint(B.w);
+  }
+  const DevMaterial m = s.materials[mat];
+  if (m.kind == kEmissive) {
+    if (ln.include_emission) ln.rad = ln.rad + ln.thr * mk(m.emission[0], m.emission[1], m.emission[2]);
+    finish_sample<kMoments>(L, ln, n_paths);
+    return;
+  }
+  if (m.kind == kDiffuse) {
+    ln.hp = hp;
+    ln.hn = nrm;
+    ln.alb = base_color(s, m, tu, tv);
+    ln.phase = kShadowLight;
+    return;
+  }
+  if (m.kind == kMetal) {
+    const V3 refl = reflect(normalize(ln.rd), nrm);
+    const V3 ball = uniform_ball(ln.rng.uniform(), ln.rng.uniform(), ln.rng.uniform());
+    const V3 dir = refl + ball * m.roughness;
+    if (dot(dir, nrm) <= 0.0f) {
+      finish_sample<kMoments>(L, ln, n_paths);
+      return;
+    }
+    ln.ro = hp;
+    ln.rd = normalize(dir);
+    ln.thr = ln.thr * mk(m.albedo[0], m.albedo[1], m.albedo[2]);
+  } else {  // dielectric (integrator.rs:315-334)
+    const float ratio = front ? 1.0f / m.ior : m.ior;
+    const V3 unit = normalize(ln.rd);
+    const float ct = fminf(dot(-unit, nrm), 1.0f);
+    const float st = sqrtf(1.0f - ct * ct);
+    const bool cannot = ratio * st > 1.0f;
+    V3 dir;
+    if (cannot || schlick(ct, ratio) > ln.rng.uniform()) dir = reflect(unit, nrm);
+    else dir = refract(unit, nrm, ratio);
+    ln.ro = hp;
+    ln.rd = normalize(dir);
+  }
+  ln.include_emission = true;
+  ln.bsdf_pdf = -1.0f;
+  ln.depth -= 1;
+  ln.phase = kExtend;
+}
+
+template <bool kMoments>
+__global__ void __launch_bounds__(256) render_kernel(const RenderLaunch L) {
+  const DevScene& s = L.scene;
+  const unsigned lane = threadIdx.x & 31u;
+  const uint32_t npix = L.width * L.height;
+  Lane ln;
+  ln.phase = kIdle;
+  ln.acc = ln.acc2 = mk(0.f, 0.f, 0.f);
+  bool finished = false;
+  uint32_t n_paths = 0, n_ext = 0, n_shadow = 0, node_visits = 0;
+
+  for (;;) {
+    // Refill idle lanes: one atomic per warp for all of them.
+    const bool want = !finished && ln.phase == kIdle;
+    const unsigned want_mask = __ballot_sync(0xffffffffu, want);
+    if (want_mask) {
+      const int leader = __ffs(want_mask) - 1;
+      unsigned long long base = 0;
+      if (int(lane) == leader) base = atomicAdd(L.work_counter, (unsigned long long)__popc(want_mask));
+      base = __shfl_sync(0xffffffffu, base, leader);
+      if (want) {
+        const uint64_t item = base + __popc(want_mask & ((1u << lane) - 1u));
+        if (item >= L.total_items) {
+          finished = true;
+        } else {
+          const uint32_t chunk = uint32_t(item / npix);
+          ln.pixel = uint32_t(item - uint64_t(chunk) * npix);
+          const uint32_t first = chunk * L.samples_per_item;
+          ln.item_samples = min(L.samples_per_item, L.samples - first);
+          ln.item_done = 0;
+          ln.sample = L.sample_base + first;
+          ln.acc = mk(0.f, 0.f, 0.f);
+          if (kMoments) ln.acc2 = mk(0.f, 0.f, 0.f);
+          start_sample(L, ln);
+        }
+      }
+    }
+    if (__all_sync(0xffffffffu, finished)) break;
+
+    // Advance the lane's state machine to its next ray.
+    bool have = false;
+    bool any_hit = false;
+    while (!finished && !have && ln.phase != kIdle) {
+      switch (ln.phase) {
+        case kExtend:
+          if (ln.depth <= 0) {
+            finish_sample<kMoments>(L, ln, n_paths);
+          } else {
+            have = true;
+            any_hit = false;
+            ln.tmax = CUDART_INF_F;
+          }
+          break;
+        case kShadowLight:
+          if (prepare_light_shadow(s, ln)) { have = true; any_hit = true; }
+          else ln.phase = kShadowEnv;
+          break;
+        case kShadowEnv:
+          if (prepare_env_shadow(s, ln)) { have = true; any_hit = true; }
+          else ln.phase = kScatter;
+          break;
+        default: {  // kScatter: cosine-weighted diffuse bounce (integrator.rs:277-289)
+          ln.depth -= 1;
+          if (ln.depth <= 0) {
+            finish_sample<kMoments>(L, ln, n_paths);
+            break;
+          }
+          V3 dir = ln.hn + uniform_sphere(ln.rng.uniform(), ln.rng.uniform());
+          if (dot(dir, dir) < 1e-8f) dir = ln.hn;
+          dir = normalize(dir);
+          ln.ro = ln.hp;
+          ln.rd = dir;
+          ln.thr = ln.thr * ln.alb;
+          ln.include_emission = false;
+          ln.bsdf_pdf = fmaxf(dot(ln.hn, dir), 0.0f) / kPiF;
+          ln.phase = kExtend;
+          break;
+        }
+      }
+    }
+
+    TraceResult tr;
+    bool hit = false;
+    if (have) {
+      const RayQ q = make_ray(ln.ro.x, ln.ro.y, ln.ro.z, ln.rd.x, ln.rd.y, ln.rd.z);
+      hit = trace_ray(s.pairs, s.prims, s.root, q, kRayEps, ln.tmax, any_hit, tr, node_visits);
+      if (ln.phase == kShadowLight) {
+        ++n_shadow;
+        if (!hit) ln.rad = ln.rad + ln.pend;
+        ln.phase = kShadowEnv;
+      } else if (ln.phase == kShadowEnv) {
+        ++n_shadow;
+        if (!hit) ln.rad = ln.rad + ln.pend;
+        ln.phase = kScatter;
+      } else {
+        ++n_ext;
+        if (!hit) {
+          ln.rad = ln.rad + ln.thr * background(s, ln.rd, ln.bsdf_pdf);
+          finish_sample<kMoments>(L, ln, n_paths);
+        } else {
+          shade_hit<kMoments>(L, ln, tr, n_paths);
+        }
+      }
+    }
+  }
+
+  // Per-launch counters: one atomic per warp.
+  const unsigned long long tp = __reduce_add_sync(0xffffffffu, n_paths);
+  const unsigned long long te = __reduce_add_sync(0xffffffffu, n_ext);
+  const unsigned long long ts = __reduce_add_sync(0xffffffffu, n_shadow);
+  if (lane == 0) {
+    atomicAdd(L.counters + 0, tp);
+    atomicAdd(L.counters + 1, te);
+    atomicAdd(L.counters + 2, ts);
+  }
+}
+
+cudaError_t launch_render(const RenderLaunch& r, int block_size, int grid_size, bool moments, cudaStream_t stream) {
+  if (moments) render_kernel<true><<<grid_size, block_size, 0, stream>>>(r);
+  else render_kernel<false><<<grid_size, block_size, 0, stream>>>(r);
+  return cudaGetLastError();
+}
+
+int render_max_blocks_per_sm(int block_size, bool moments) {
+  int blocks = 0;
+  cudaError_t e = moments
+      ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, render_kernel<true>, block_size, 0)
+      : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, render_kernel<false>, block_size, 0);
+  return e == cudaSuccess ? blocks : 0;
+}
+
+// ------------------------------------------------------------------------ resolve
+__global__ void resolve_kernel(const double* __restrict__ accum, uint32_t pixels, double inv_samples,
+                               float4* __restrict__ out) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= pixels) return;
+  const double* a = accum + size_t(3) * i;
+  out[i] = make_float4(float(a[0] * inv_samples), float(a[1] * inv_samples), float(a[2] * inv_samples), 1.0f);
+}
+
+cudaError_t launch_resolve(const double* accum, uint32_t pixels, double inv_samples, float4* out,
+                           cudaStream_t stream) {
+  if (pixels == 0) return cudaSuccess;
+  resolve_kernel<<<(pixels + 255) / 256, 256, 0, stream>>>(accum, pixels, inv_samples, out);
+  return cudaGetLastError();
+}
+
+// ------------------------------------------------------------------------ environment tables
+// Weights follow environment.rs:245-260: luminance * sin(theta_row_centre) * intensity in FP64.
+// Row kernel: one block per row; FP64 block reduction for the row sum, then an FP64 inclusive
+// scan written as the normalised conditional CDF (last entry forced to 1).
+constexpr int kEnvBlock = 256;
+
+__device__ __forceinline__ double env_weight(const float4 t, double sin_theta, double intensity) {
+  const double lum = 0.2126 * double(t.x) + 0.7152 * double(t.y) + 0.0722 * double(t.z);
+  return lum * sin_theta * intensity;
+}
+
+__device__ double block_sum(double v, double* sh) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (lane == 0) sh[warp] = v;
+  __syncthreads();
+  double total = 0.0;
+  if (threadIdx.x == 0) {
+    for (int w = 0; w < kEnvBlock / 32; ++w) total += sh[w];
+    sh[kEnvBlock / 32] = total;
+  }
+  __syncthreads();
+  total = sh[kEnvBlock / 32];
+  __syncthreads();
+  return total;
+}
+
+// Inclusive scan of one value per thread across the block (FP64); returns the prefix.
+__device__ double block_scan(double v, double* sh) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (int o = 1; o < 32; o <<= 1) {
+    const double n = __shfl_up_sync(0xffffffffu, v, o);
+    if (lane >= o) v += n;
+  }
+  if (lane == 31) sh[warp] = v;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double run = 0.0;
+    for (int w = 0; w < kEnvBlock / 32; ++w) {
+      const double t = sh[w];
+      sh[w] = run;
+      run += t;
+    }
+  }
+  __syncthreads();
+  v += sh[warp];
+  __syncthreads();
+  return v;
+}
+
+__global__ void env_rows_kernel(const float4* __restrict__ rgb, uint32_t w, uint32_t h, double intensity,
+                                float* __restrict__ conditional, double* __restrict__ row_sums) {
+  __shared__ double sh[kEnvBlock / 32 + 1];
+  __shared__ double tile_end;
+  const uint32_t y = blockIdx.x;
+  const double sin_theta = sin(CUDART_PI * (double(y) + 0.5) / double(h));
+  const float4* row = rgb + size_t(y) * w;
+  double local = 0.0;
+  for (uint32_t x = threadIdx.x; x < w; x += kEnvBlock) local += env_weight(row[x], sin_theta, intensity);
+  const double total = block_sum(local, sh);
+  if (threadIdx.x == 0) row_sums[y] = total;
+  float* out = conditional + size_t(y) * w;
+  if (!(total > 0.0) || !isfinite(total)) {
+    for (uint32_t x = threadIdx.x; x < w; x += kEnvBlock) out[x] = float(double(x + 1) / double(w));
+    return;
+  }
+  double carry = 0.0;
+  for (uint32_t base = 0; base < w; base += kEnvBlock) {
+    const uint32_t x = base + threadIdx.x;
+    const double v = x < w ? env_weight(row[x], sin_theta, intensity) : 0.0;
+    const double incl = block_scan(v, sh) + carry;
+    if (x < w) out[x] = (x == w - 1) ? 1.0f : float(incl / total);
+    // The carry into the next tile is the inclusive value of the tile's last thread.
+    if (threadIdx.x == kEnvBlock - 1) tile_end = incl;
+    __syncthreads();
+    carry = tile_end;
+    __syncthreads();
+  }
+}
+
+__global__ void env_marginal_kernel(const double* __restrict__ row_sums, uint32_t h, float* __restrict__ marginal,
+                                    double* __restrict__ total_out) {
+  __shared__ double sh[kEnvBlock / 32 + 1];
+  double local = 0.0;
+  for (uint32_t y = threadIdx.x; y < h; y += kEnvBlock) local += row_sums[y];
+  const double total = block_sum(local, sh);
+  if (threadIdx.x == 0) *total_out = total;
+  if (!(total > 0.0) || !isfinite(total)) {
+    for (uint32_t y = threadIdx.x; y < h; y += kEnvBlock) marginal[y] = 0.0f;
+    return;
+  }
+  __shared__ double tile_end;
+  double carry = 0.0;
+  for (uint32_t base = 0; base < h; base += kEnvBlock) {
+    const uint32_t y = base + threadIdx.x;
+    const double v = y < h ? row_sums[y] : 0.0;
+    const double incl = block_scan(v, sh) + carry;
+    if (y < h) marginal[y] = (y == h - 1) ? 1.0f : float(incl / total);
+    if (threadIdx.x == kEnvBlock - 1) tile_end = incl;
+    __syncthreads();
+    carry = tile_end;
+    __syncthreads();
+  }
+}
+
+// Per-texel numerator of the solid-angle density: P(row) * P(column | row) * W * H / (2 pi^2),
+// both probabilities taken from the stored FP32 CDFs the sampler inverts.
+__global__ void env_pdf_kernel(const float* __restrict__ marginal, const float* __restrict__ conditional,
+                               uint32_t w, uint32_t h, const double* __restrict__ total, float* __restrict__ pdf) {
+  const size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= size_t(w) * h) return;
+  const double t = *total;
+  if (!(t > 0.0) || !isfinite(t)) {
+    pdf[i] = 0.0f;
+    return;
+  }
+  const uint32_t y = uint32_t(i / w), x = uint32_t(i - size_t(y) * w);
+  const double py = double(marginal[y]) - (y ? double(marginal[y - 1]) : 0.0);
+  const float* row = conditional + size_t(y) * w;
+  const double px = double(row[x]) - (x ? double(row[x - 1]) : 0.0);
+  const double p = fmax(py, 0.0) * fmax(px, 0.0);
+  pdf[i] = float(p * double(w) * double(h) / (2.0 * CUDART_PI * CUDART_PI));
+}
+
+cudaError_t launch_env_tables(const float4* rgb, uint32_t w, uint32_t h, float intensity, float* marginal,
+                              float* conditional, float* pdf, double* row_sums, double* total_out,
+                              cudaStream_t stream) {
+  if (w == 0 || h == 0) return cudaSuccess;
+  env_rows_kernel<<<h, kEnvBlock, 0, stream>>>(rgb, w, h, double(intensity), conditional, row_sums);
+  env_marginal_kernel<<<1, kEnvBlock, 0, stream>>>(row_sums, h, marginal, total_out);
+  const size_t n = size_t(w) * h;
+  env_pdf_kernel<<<unsigned((n + 255) / 256), 256, 0, stream>>>(marginal, conditional, w, h, total_out, pdf);
+  return cudaGetLastError();
+}
+
+}  // namespace tcb

@@ -1,0 +1,201 @@
+// Ray/primitive tests and ordered BVH traversal (device).
+//
+// Every operation that decides a hit or its distance uses explicitly rounded IEEE intrinsics
+// (__fadd_rn, __fsub_rn, __fmul_rn, __frcp_rn, __fdiv_rn, __fsqrt_rn) so the compiler cannot
+// fuse them into FMAs. This reproduces, bit for bit, the f32 arithmetic of
+//   crates/toaster-bvh/src/aabb.rs:74-110            (slab test)
+//   crates/toaster-cpu/src/intersect.rs:28-68        (sphere)
+//   crates/toaster-cpu/src/intersect.rs:87-120       (Moller-Trumbore)
+//   crates/toaster-cpu/src/intersect.rs:172-263,322  (ordered traversal, entry distance)
+// assuming glam's scalar Vec3 (dot left to right, cross = a.y*b.z - b.y*a.z ...).
+#ifndef TOASTER_B200_TRAVERSE_CUH
+#define TOASTER_B200_TRAVERSE_CUH
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "layout.h"
+
+namespace tcb {
+
+struct RayQ {
+  float ox, oy, oz;
+  float dx, dy, dz;
+  float ix, iy, iz;   // 1/d, IEEE (f32::recip)
+  bool sx, sy, sz;    // direction sign bits: choose the near plane without a swap
+};
+
+__device__ __forceinline__ RayQ make_ray(float ox, float oy, float oz, float dx, float dy, float dz) {
+  RayQ r;
+  r.ox = ox; r.oy = oy; r.oz = oz;
+  r.dx = dx; r.dy = dy; r.dz = dz;
+  r.ix = __frcp_rn(dx); r.iy = __frcp_rn(dy); r.iz = __frcp_rn(dz);
+  r.sx = signbit(dx); r.sy = signbit(dy); r.sz = signbit(dz);
+  return r;
+}
+
+// Slab test of one child box against [tmin, closest]. Returns the hit flag; `entry` is the
+// reference's entry_distance (intersect.rs:322-338) and `tn` = max(tmin, entry), the value the
+// reference's pop-time re-test compares against `closest`.
+//
+// Equivalence with aabb.rs: for a finite 1/d the near plane is fixed by the sign of d, and
+// rounding is monotone, so the reference's `if near > far swap` picks the same pair. For an
+// infinite 1/d (the reference's "parallel" branch) the products are +-inf when the origin is
+// outside the slab (forcing a miss) and -inf/NaN when inside (dropped by fmaxf/fminf), which is
+// exactly "reject if o < lo || o > hi, else skip the axis".
+__device__ __forceinline__ bool box_test(float lox, float loy, float loz, float hix, float hiy, float hiz,
+                                         const RayQ& r, float tmin, float closest, float& entry, float& tn) {
+  const float ax = __fmul_rn(__fsub_rn(lox, r.ox), r.ix);
+  const float bx = __fmul_rn(__fsub_rn(hix, r.ox), r.ix);
+  const float ay = __fmul_rn(__fsub_rn(loy, r.oy), r.iy);
+  const float by = __fmul_rn(__fsub_rn(hiy, r.oy), r.iy);
+  const float az = __fmul_rn(__fsub_rn(loz, r.oz), r.iz);
+  const float bz = __fmul_rn(__fsub_rn(hiz, r.oz), r.iz);
+  const float nx = r.sx ? bx : ax, fx = r.sx ? ax : bx;
+  const float ny = r.sy ? by : ay, fy = r.sy ? ay : by;
+  const float nz = r.sz ? bz : az, fz = r.sz ? az : bz;
+  entry = fmaxf(fmaxf(nx, ny), nz);
+  tn = fmaxf(entry, tmin);
+  const float tf = fminf(fminf(fx, fy), fminf(fz, closest));
+  return tf >= tn;
+}
+
+// intersect.rs:87-120: double-sided Moller-Trumbore with eps 1e-8 and inclusive [tmin, tmax].
+__device__ __forceinline__ bool hit_triangle(const RayQ& r, float4 A, float4 B, float4 C, float tmin, float tmax,
+                                             float& t_out) {
+  const float e1x = B.x, e1y = B.y, e1z = B.z;
+  const float e2x = C.x, e2y = C.y, e2z = C.z;
+  // p = d x e2
+  const float px = __fsub_rn(__fmul_rn(r.dy, e2z), __fmul_rn(e2y, r.dz));
+  const float py = __fsub_rn(__fmul_rn(r.dz, e2x), __fmul_rn(e2z, r.dx));
+  const float pz = __fsub_rn(__fmul_rn(r.dx, e2y), __fmul_rn(e2x, r.dy));
+  const float det = __fadd_rn(__fadd_rn(__fmul_rn(e1x, px), __fmul_rn(e1y, py)), __fmul_rn(e1z, pz));
+  if (fabsf(det) < 1e-8f) return false;
+  const float inv = __frcp_rn(det);
+  const float sx = __fsub_rn(r.ox, A.x), sy = __fsub_rn(r.oy, A.y), sz = __fsub_rn(r.oz, A.z);
+  const float u = __fmul_rn(__fadd_rn(__fadd_rn(__fmul_rn(sx, px), __fmul_rn(sy, py)), __fmul_rn(sz, pz)), inv);
+  if (!(u >= 0.0f && u <= 1.0f)) return false;
+  // q = s x e1
+  const float qx = __fsub_rn(__fmul_rn(sy, e1z), __fmul_rn(e1y, sz));
+  const float qy = __fsub_rn(__fmul_rn(sz, e1x), __fmul_rn(e1z, sx));
+  const float qz = __fsub_rn(__fmul_rn(sx, e1y), __fmul_rn(e1x, sy));
+  const float v = __fmul_rn(__fadd_rn(__fadd_rn(__fmul_rn(r.dx, qx), __fmul_rn(r.dy, qy)), __fmul_rn(r.dz, qz)), inv);
+  if (v < 0.0f || __fadd_rn(u, v) > 1.0f) return false;
+  const float t = __fmul_rn(__fadd_rn(__fadd_rn(__fmul_rn(e2x, qx), __fmul_rn(e2y, qy)), __fmul_rn(e2z, qz)), inv);
+  if (t < tmin || t > tmax) return false;
+  t_out = t;
+  return true;
+}
+
+// intersect.rs:28-50: half-b quadratic, near root else far root, inclusive [tmin, tmax].
+__device__ __forceinline__ bool hit_sphere(const RayQ& r, float4 A, float4 B, float tmin, float tmax,
+                                           float& t_out) {
+  const float ox = __fsub_rn(r.ox, A.x), oy = __fsub_rn(r.oy, A.y), oz = __fsub_rn(r.oz, A.z);
+  const float a = __fadd_rn(__fadd_rn(__fmul_rn(r.dx, r.dx), __fmul_rn(r.dy, r.dy)), __fmul_rn(r.dz, r.dz));
+  const float hb = __fadd_rn(__fadd_rn(__fmul_rn(ox, r.dx), __fmul_rn(oy, r.dy)), __fmul_rn(oz, r.dz));
+  const float c = __fsub_rn(__fadd_rn(__fadd_rn(__fmul_rn(ox, ox), __fmul_rn(oy, oy)), __fmul_rn(oz, oz)), B.y);
+  const float disc = __fsub_rn(__fmul_rn(hb, hb), __fmul_rn(a, c));
+  if (disc < 0.0f) return false;
+  const float sq = __fsqrt_rn(disc);
+  float t = __fdiv_rn(__fsub_rn(-hb, sq), a);
+  if (t < tmin || t > tmax) {
+    t = __fdiv_rn(__fadd_rn(-hb, sq), a);
+    if (t < tmin || t > tmax) return false;
+  }
+  t_out = t;
+  return true;
+}
+
+struct TraceResult {
+  float t;        // closest accepted distance (or tmax when nothing was accepted)
+  uint32_t tag;   // PrimRecord tag of the accepted primitive
+  uint32_t rec;   // PrimRecord index of the accepted primitive
+};
+
+// Ordered closest-hit traversal (any_hit = false) or first-hit occlusion query (any_hit = true)
+// over the sibling-pair hierarchy, returning whether a primitive was accepted in [tmin, tmax].
+//
+// Closest-hit mode reproduces intersect.rs:172-263 exactly: children are tested against the
+// current closest distance; when both are hit the one with the smaller entry distance is taken
+// first (strictly smaller; ties take the right child first, as the reference's push order
+// does); a stacked child is re-tested on pop, which for a box that passed at push time reduces
+// to `tn <= closest`; leaf primitives are tested in leaf order and accepted on `t <= closest`.
+// Stack depth never exceeds the hierarchy depth, which the host checks against kMaxStack.
+__device__ __forceinline__ bool trace_ray(const PairNode* __restrict__ pairs, const PrimRecord* __restrict__ prims,
+                                          const ChildRec& root, const RayQ& r, float tmin, float tmax,
+                                          bool any_hit, TraceResult& res, uint32_t& node_visits) {
+  float closest = tmax;
+  bool found = false;
+  float entry, tn;
+  if (!box_test(root.min_x, root.min_y, root.min_z, root.max_x, root.max_y, root.max_z, r, tmin, closest, entry, tn))
+    return false;
+  uint32_t st_ref[kMaxStack];
+  float st_tn[kMaxStack];
+  int sp = 0;
+  uint32_t cur = root.link;
+  for (;;) {
+    if (cur & kLeafBit) {
+      uint32_t k = cur & ~kLeafBit;
+      for (;;) {
+        const float4* p = reinterpret_cast<const float4*>(prims + k);
+        const float4 A = __ldg(p);
+        const float4 B = __ldg(p + 1);
+        const uint32_t tag = __float_as_uint(A.w);
+        float t;
+        bool ok;
+        if (tag & kTagTriangle) {
+          const float4 C = __ldg(p + 2);
+          ok = hit_triangle(r, A, B, C, tmin, closest, t);
+        } else {
+          ok = hit_sphere(r, A, B, tmin, closest, t);
+        }
+        if (ok) {
+          closest = t;
+          found = true;
+          res.tag = tag;
+          res.rec = k;
+          if (any_hit) {
+            res.t = closest;
+            return true;
+          }
+        }
+        if (tag & kTagLast) break;
+        ++k;
+      }
+    } else {
+      ++node_visits;
+      const float4* q = reinterpret_cast<const float4*>(pairs + cur);
+      const float4 a0 = __ldg(q), a1 = __ldg(q + 1), b0 = __ldg(q + 2), b1 = __ldg(q + 3);
+      float ea, ta, eb, tb;
+      const bool ha = box_test(a0.x, a0.y, a0.z, a1.x, a1.y, a1.z, r, tmin, closest, ea, ta);
+      const bool hb = box_test(b0.x, b0.y, b0.z, b1.x, b1.y, b1.z, r, tmin, closest, eb, tb);
+      const uint32_t la = __float_as_uint(a0.w), lb = __float_as_uint(b0.w);
+      if (ha && hb) {
+        const bool a_first = ea < eb;
+        st_ref[sp] = a_first ? lb : la;
+        st_tn[sp] = a_first ? tb : ta;
+        ++sp;
+        cur = a_first ? la : lb;
+        continue;
+      }
+      if (ha) { cur = la; continue; }
+      if (hb) { cur = lb; continue; }
+    }
+    bool popped = false;
+    while (sp > 0) {
+      --sp;
+      if (st_tn[sp] <= closest) {
+        cur = st_ref[sp];
+        popped = true;
+        break;
+      }
+    }
+    if (!popped) break;
+  }
+  res.t = closest;
+  return found;
+}
+
+}  // namespace tcb
+
+#endif

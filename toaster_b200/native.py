@@ -1,0 +1,168 @@
+"""ctypes binding of the C ABI in include/toaster_cuda.h.
+
+The shared library is built in-tree (``toaster_b200/lib/libtoaster_cuda.so``) by
+``toaster_b200.build``. There is no fallback: importing a GPU entry point without the library
+raises, and creating a context without an sm_100 device fails with the library's message.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+from pathlib import Path
+
+import numpy as np
+
+from . import gpu_types as gt
+
+LIB_DIR = Path(__file__).resolve().parent / "lib"
+LIB_PATH = LIB_DIR / "libtoaster_cuda.so"
+
+TC_OK = 0
+TC_MISS = 0xFFFFFFFF
+TC_PRIM_TRIANGLE_BIT = 0x80000000
+
+# Exported symbols declared in include/toaster_cuda.h.
+EXPORTED_SYMBOLS = (
+    "tc_abi_version",
+    "tc_last_error",
+    "tc_create",
+    "tc_destroy",
+    "tc_set_stream",
+    "tc_upload_scene",
+    "tc_set_camera",
+    "tc_render",
+    "tc_readback",
+    "tc_readback_sums",
+    "tc_trace_closest",
+    "tc_trace_closest_device_async",
+    "tc_get_stats",
+    "tc_build_bvh_host",
+    "tc_record_sizes",
+)
+
+
+class TcError(RuntimeError):
+    """A tc_* call returned a nonzero status."""
+
+    def __init__(self, code: int, message: str):
+        super().__init__(f"toaster_cuda error {code}: {message}")
+        self.code = code
+
+
+class SceneData(ctypes.Structure):
+    _fields_ = [
+        ("params", ctypes.c_uint8 * 96),
+        ("camera", ctypes.c_uint8 * 64),
+        ("spheres", ctypes.c_void_p),
+        ("sphere_count", ctypes.c_size_t),
+        ("triangles", ctypes.c_void_p),
+        ("triangle_count", ctypes.c_size_t),
+        ("triangle_attributes", ctypes.c_void_p),
+        ("triangle_attribute_count", ctypes.c_size_t),
+        ("materials", ctypes.c_void_p),
+        ("material_count", ctypes.c_size_t),
+        ("lights", ctypes.c_void_p),
+        ("light_count", ctypes.c_size_t),
+        ("bvh_nodes", ctypes.c_void_p),
+        ("bvh_node_count", ctypes.c_size_t),
+        ("bvh_primitives", ctypes.c_void_p),
+        ("bvh_primitive_count", ctypes.c_size_t),
+        ("texture_pixels", ctypes.c_void_p),
+        ("texture_pixel_count", ctypes.c_size_t),
+        ("environment_pixels", ctypes.c_void_p),
+        ("environment_pixel_count", ctypes.c_size_t),
+    ]
+
+
+class RenderOptions(ctypes.Structure):
+    _fields_ = [
+        ("block_size", ctypes.c_uint32),
+        ("samples_per_item", ctypes.c_uint32),
+        ("keep_moments", ctypes.c_uint32),
+        ("guiding", ctypes.c_uint32),
+        ("_reserved", ctypes.c_uint32 * 4),
+    ]
+
+
+class Stats(ctypes.Structure):
+    _fields_ = [
+        ("paths", ctypes.c_uint64),
+        ("rays", ctypes.c_uint64),
+        ("extension_rays", ctypes.c_uint64),
+        ("shadow_rays", ctypes.c_uint64),
+        ("kernel_ms", ctypes.c_float),
+        ("total_ms", ctypes.c_float),
+        ("bvh_depth", ctypes.c_uint32),
+        ("status_flags", ctypes.c_uint32),
+    ]
+
+
+_LIB = None
+
+
+def load_library(path: os.PathLike | None = None) -> ctypes.CDLL:
+    """Loads (once) and returns the CUDA library; raises if it has not been built."""
+    global _LIB
+    if _LIB is not None and path is None:
+        return _LIB
+    p = Path(path) if path is not None else LIB_PATH
+    if not p.exists():
+        raise RuntimeError(f"{p} is missing: build it with `python -m toaster_b200.build` (no CPU fallback exists)")
+    lib = ctypes.CDLL(str(p))
+    vp, sz, u32, i32, f32 = ctypes.c_void_p, ctypes.c_size_t, ctypes.c_uint32, ctypes.c_int, ctypes.c_float
+    lib.tc_abi_version.restype = i32
+    lib.tc_last_error.argtypes = [vp]
+    lib.tc_last_error.restype = ctypes.c_char_p
+    lib.tc_create.argtypes = [i32, ctypes.POINTER(vp)]
+    lib.tc_destroy.argtypes = [vp]
+    lib.tc_set_stream.argtypes = [vp, vp]
+    lib.tc_upload_scene.argtypes = [vp, ctypes.POINTER(SceneData)]
+    lib.tc_set_camera.argtypes = [vp, vp]
+    lib.tc_render.argtypes = [vp, vp, ctypes.POINTER(RenderOptions)]
+    lib.tc_readback.argtypes = [vp, vp, sz]
+    lib.tc_readback_sums.argtypes = [vp, vp, vp, sz, ctypes.POINTER(u32)]
+    lib.tc_trace_closest.argtypes = [vp, vp, sz, f32, vp, vp]
+    lib.tc_trace_closest_device_async.argtypes = [vp, vp, sz, f32, vp, vp, vp]
+    lib.tc_get_stats.argtypes = [vp, ctypes.POINTER(Stats)]
+    lib.tc_build_bvh_host.argtypes = [vp, sz, vp, sz, vp, sz, vp, sz]
+    lib.tc_build_bvh_host.restype = ctypes.c_long
+    lib.tc_record_sizes.argtypes = [ctypes.POINTER(u32), sz]
+    for name in EXPORTED_SYMBOLS:
+        if not hasattr(lib, name):
+            raise RuntimeError(f"{p} does not export {name}")
+    if path is None:
+        _LIB = lib
+    return lib
+
+
+def _ptr(a: np.ndarray | None):
+    return None if a is None or a.size == 0 else a.ctypes.data
+
+
+def check(lib, ctx, code: int) -> None:
+    if code != TC_OK:
+        msg = lib.tc_last_error(ctx)
+        raise TcError(code, msg.decode() if msg else "")
+
+
+def build_bvh_host(spheres: np.ndarray, triangles: np.ndarray):
+    """Reference-layout hierarchy built by the library's host builder (no GPU needed)."""
+    lib = load_library()
+    spheres = np.ascontiguousarray(spheres, gt.SPHERE)
+    triangles = np.ascontiguousarray(triangles, gt.TRIANGLE)
+    n = len(spheres) + len(triangles)
+    nodes = np.zeros(max(2 * n - 1, 1), gt.BVH_NODE)
+    prims = np.zeros(max(n, 1), gt.PRIMITIVE_REF)
+    count = lib.tc_build_bvh_host(_ptr(spheres), len(spheres), _ptr(triangles), len(triangles),
+                                  nodes.ctypes.data, len(nodes), prims.ctypes.data, len(prims))
+    if count < 0:
+        raise TcError(int(count), lib.tc_last_error(None).decode())
+    return nodes[:count].copy(), prims[:n].copy()
+
+
+def record_sizes() -> list:
+    lib = load_library()
+    out = (ctypes.c_uint32 * 9)()
+    check(lib, None, lib.tc_record_sizes(out, 9))
+    return list(out)

@@ -1,0 +1,233 @@
+"""Host-side renderer API over the CUDA library, mirroring the public ``toaster_gpu`` surface.
+
+``render_scene_gpu``, ``render_gpu_progressive`` and ``benchmark_gpu_scene`` correspond to
+``render_scene_gpu`` / ``render_gpu_progressive_with_sink`` / ``benchmark_gpu_scene`` in
+crates/toaster-gpu/src/path_tracer.rs (lib.rs:28-37), with the same frame-seed, progressive
+batching and validation rules. Images are linear-HDR float4 (alpha = 1), row-major, y down.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import dataclasses
+import time
+from typing import Optional
+
+import numpy as np
+
+from . import gpu_types as gt
+from . import native
+from .scene import Scene, SceneGpuData, scene_to_gpu
+
+
+def progressive_batch(requested_samples: int, accumulated_samples: int, target_samples: int) -> Optional[int]:
+    """Next batch clamped to the remaining target, or None when complete (path_tracer.rs:900-923)."""
+    if requested_samples <= 0:
+        raise ValueError("sample batch must be greater than zero")
+    if target_samples <= 0:
+        raise ValueError("sample target must be greater than zero")
+    if accumulated_samples > target_samples:
+        raise ValueError("accumulated samples exceed the progressive target")
+    if accumulated_samples == target_samples:
+        return None
+    return min(requested_samples, target_samples - accumulated_samples)
+
+
+def render_frame_seed(frame: int, static_independent: bool) -> int:
+    """Benchmark frames reuse seed 0; animated frames use their index (path_tracer.rs:892-897)."""
+    return 0 if static_independent else frame
+
+
+class GpuRenderer:
+    """One CUDA context (device buffers + stream) holding one uploaded scene."""
+
+    def __init__(self, device: int = 0):
+        self._lib = native.load_library()
+        ctx = ctypes.c_void_p()
+        native.check(self._lib, None, self._lib.tc_create(device, ctypes.byref(ctx)))
+        self._ctx = ctx
+        self.width = 0
+        self.height = 0
+        self.accumulated = 0
+        self._params = None
+
+    def close(self) -> None:
+        if self._ctx:
+            self._lib.tc_destroy(self._ctx)
+            self._ctx = ctypes.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, code: int) -> None:
+        native.check(self._lib, self._ctx, code)
+
+    def upload(self, data: SceneGpuData) -> None:
+        """Copies packed scene records to the device and builds hierarchy and sampling tables."""
+        sd = native.SceneData()
+        ctypes.memmove(sd.params, data.params.ctypes.data, 96)
+        ctypes.memmove(sd.camera, data.camera.ctypes.data, 64)
+        keep = []
+
+        def arr(a, dtype):
+            if a is None or len(a) == 0:
+                return None, 0
+            a = np.ascontiguousarray(a, dtype)
+            keep.append(a)
+            return a.ctypes.data, len(a)
+
+        sd.spheres, sd.sphere_count = arr(data.spheres, gt.SPHERE)
+        sd.triangles, sd.triangle_count = arr(data.triangles, gt.TRIANGLE)
+        sd.triangle_attributes, sd.triangle_attribute_count = arr(data.triangle_attributes, gt.TRIANGLE_ATTRIBUTES)
+        sd.materials, sd.material_count = arr(data.materials, gt.MATERIAL)
+        sd.lights, sd.light_count = arr(data.lights, gt.LIGHT)
+        sd.bvh_nodes, sd.bvh_node_count = arr(data.bvh_nodes, gt.BVH_NODE)
+        sd.bvh_primitives, sd.bvh_primitive_count = arr(data.bvh_primitives, gt.PRIMITIVE_REF)
+        sd.texture_pixels, sd.texture_pixel_count = arr(data.texture_pixels, np.uint32)
+        if data.environment_pixels is not None:
+            env = np.ascontiguousarray(data.environment_pixels, np.float32).reshape(-1, 4)
+            keep.append(env)
+            sd.environment_pixels, sd.environment_pixel_count = env.ctypes.data, env.shape[0]
+        self._check(self._lib.tc_upload_scene(self._ctx, ctypes.byref(sd)))
+        self._params = data.params.copy()
+        self.accumulated = 0
+
+    def set_stream(self, stream: int) -> None:
+        """Enqueue on a caller-owned cudaStream_t (0 = the context's own stream)."""
+        self._check(self._lib.tc_set_stream(self._ctx, stream or None))
+
+    def set_camera(self, camera: np.ndarray) -> None:
+        cam = np.ascontiguousarray(camera, gt.CAMERA)
+        self._check(self._lib.tc_set_camera(self._ctx, cam.ctypes.data))
+
+    def render(self, samples: Optional[int] = None, max_bounces: Optional[int] = None, width: Optional[int] = None,
+               height: Optional[int] = None, frame_index: int = 0, accumulate: bool = False,
+               keep_moments: bool = False, block_size: int = 0, samples_per_item: int = 0) -> None:
+        """Traces ``samples`` paths per pixel; ``accumulate`` adds them to the previous batches."""
+        if self._params is None:
+            raise RuntimeError("render before upload")
+        p = self._params.copy()
+        if samples is not None:
+            p["samples"] = samples
+        if max_bounces is not None:
+            p["max_bounces"] = max_bounces
+        if width is not None:
+            p["width"] = width
+        if height is not None:
+            p["height"] = height
+        p["frame_index"] = frame_index
+        p["accumulated_samples"] = self.accumulated if accumulate else 0
+        opts = native.RenderOptions()
+        opts.block_size = block_size
+        opts.samples_per_item = samples_per_item
+        opts.keep_moments = 1 if keep_moments else 0
+        self._check(self._lib.tc_render(self._ctx, p.ctypes.data, ctypes.byref(opts)))
+        self.width, self.height = int(p["width"][0]), int(p["height"][0])
+        self.accumulated = (self.accumulated if accumulate else 0) + int(p["samples"][0])
+
+    def readback(self, out: Optional[np.ndarray] = None) -> np.ndarray:
+        """Linear-HDR float4 image (height, width, 4)."""
+        if out is None:
+            out = np.empty((self.height, self.width, 4), np.float32)
+        self._check(self._lib.tc_readback(self._ctx, out.ctypes.data, out.size))
+        return out
+
+    def readback_sums(self, moments: bool = False):
+        """FP64 per-pixel sums (and sums of squares when kept) plus the sample count."""
+        n = self.height * self.width * 3
+        s = np.empty((self.height, self.width, 3), np.float64)
+        q = np.empty((self.height, self.width, 3), np.float64) if moments else None
+        count = ctypes.c_uint32()
+        self._check(self._lib.tc_readback_sums(self._ctx, s.ctypes.data, None if q is None else q.ctypes.data, n,
+                                               ctypes.byref(count)))
+        return s, q, int(count.value)
+
+    def trace_closest(self, rays: np.ndarray, tmin: float = 0.001):
+        """Closest hit per ray: (prim = kind << 31 | index or TC_MISS, t)."""
+        rays = np.ascontiguousarray(rays, np.float32).reshape(-1, 6)
+        prim = np.empty(rays.shape[0], np.uint32)
+        t = np.empty(rays.shape[0], np.float32)
+        self._check(self._lib.tc_trace_closest(self._ctx, rays.ctypes.data, rays.shape[0], tmin, prim.ctypes.data,
+                                               t.ctypes.data))
+        return prim, t
+
+    def trace_closest_device(self, rays_ptr: int, n: int, prim_ptr: int, t_ptr: int, tmin: float = 0.001,
+                             stream: int = 0) -> None:
+        """Enqueues the parity traversal on device buffers (no synchronisation)."""
+        self._check(self._lib.tc_trace_closest_device_async(self._ctx, rays_ptr, n, tmin, prim_ptr, t_ptr,
+                                                            stream or None))
+
+    def stats(self) -> dict:
+        s = native.Stats()
+        self._check(self._lib.tc_get_stats(self._ctx, ctypes.byref(s)))
+        return {f: getattr(s, f) for f, _ in native.Stats._fields_}
+
+
+def render_scene_gpu(scene: Scene, device: int = 0, frame_index: int = 0) -> np.ndarray:
+    """Renders one frame of ``scene`` at its own settings and returns the HDR image."""
+    with GpuRenderer(device) as r:
+        r.upload(scene_to_gpu(scene))
+        r.render(frame_index=frame_index)
+        return r.readback()
+
+
+def render_gpu_progressive(scene: Scene, target_samples: int, batch_samples: Optional[int] = None,
+                           device: int = 0, callback=None) -> np.ndarray:
+    """Progressive accumulation to exactly ``target_samples`` (path_tracer.rs:428-458)."""
+    batch_samples = batch_samples or scene.samples
+    with GpuRenderer(device) as r:
+        r.upload(scene_to_gpu(scene))
+        frame = 0
+        while True:
+            n = progressive_batch(batch_samples, r.accumulated, target_samples)
+            if n is None:
+                break
+            r.render(samples=n, frame_index=render_frame_seed(frame, False), accumulate=frame > 0)
+            if callback is not None:
+                callback(frame, r)
+            frame += 1
+        return r.readback()
+
+
+@dataclasses.dataclass
+class GpuBenchmarkResult:
+    setup_time_s: float
+    frames: list  # per measured frame: dict of stage timings (ms)
+    final_image: np.ndarray
+
+
+def benchmark_gpu_scene(scene: Scene, warmup_frames: int, measured_frames: int, device: int = 0) -> GpuBenchmarkResult:
+    """Static independent frames at time 0 and seed 0 (path_tracer.rs:476-515)."""
+    if measured_frames <= 0:
+        raise ValueError("benchmark measured frame count must be greater than zero")
+    t0 = time.perf_counter()
+    r = GpuRenderer(device)
+    data = scene_to_gpu(scene)
+    r.upload(data)
+    setup = time.perf_counter() - t0
+    frames = []
+    image = None
+    try:
+        for frame in range(warmup_frames + measured_frames):
+            f0 = time.perf_counter()
+            r.render(frame_index=render_frame_seed(frame, True))
+            f1 = time.perf_counter()
+            image = r.readback()
+            f2 = time.perf_counter()
+            st = r.stats()
+            if frame >= warmup_frames:
+                frames.append({"dispatch_wait_ms": (f1 - f0) * 1e3, "readback_ms": (f2 - f1) * 1e3,
+                               "kernel_ms": st["kernel_ms"], "total_ms": (f2 - f0) * 1e3, "rays": st["rays"],
+                               "paths": st["paths"]})
+    finally:
+        r.close()
+    return GpuBenchmarkResult(setup, frames, image)
