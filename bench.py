@@ -46,6 +46,7 @@ def parse_args():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--cpu-seconds", type=float, default=10.0, help="target wall time of one CPU sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--spp", type=int, default=64, help="samples per pixel per frame (64 = the benchmark workload)")
     return ap.parse_args()
 
 
@@ -217,7 +218,7 @@ def run_ours(args):
                                 timeout=__import__("datetime").timedelta(seconds=300))
     torch.cuda.set_device(local)
     build.build()
-    scene = configs.mixed()
+    scene = configs.mixed(samples=args.spp)
     data = scene_to_gpu(scene)
     w, h, spp = scene.width, scene.height, scene.samples
     paths_per_step = w * h * spp

@@ -206,6 +206,12 @@ int tc_trace_closest_device_async(tc_context* ctx, const float* d_rays, size_t n
 
 int tc_get_stats(const tc_context* ctx, tc_stats* out);
 
+/* Tensor-core self-test (no reference counterpart): one 128 x n tile D = A * B^T with bf16 A
+ * (128 x k, row-major) and B (n x k, row-major) staged in shared memory as K-major
+ * (mn_major = 0) or MN-major (1) operands, FP32 accumulation in tensor memory. d receives
+ * 128 x n floats. 16 <= n <= 128 and 16 <= k <= 80, both multiples of 16. */
+int tc_umma_selftest(const uint16_t* a, const uint16_t* b, float* d, int n, int k, int a_mn_major, int b_mn_major);
+
 /* Host-only helpers (no GPU needed) -------------------------------------------------------- */
 
 /* Builds the median-split hierarchy of crates/toaster-bvh for the given spheres and triangles

@@ -125,8 +125,22 @@ def test_emissive_and_black_known_answers(renderer):  # integrator.rs:682-700 on
     assert np.array_equal(render_image(renderer, zero_depth, max_bounces=0)[..., :3], np.zeros((8, 8, 3), np.float32))
 
 
-def statistical_parity(renderer, scene, gpu_spp, cpu_spp, max_outside=0.02):
-    """Per-pixel luminance means within a 3-sigma band; global mean within 4 sigma."""
+def _blocks(x, b):
+    h, w = x.shape
+    h2, w2 = h // b * b, w // b * b
+    return x[:h2, :w2].reshape(h2 // b, b, w2 // b, b).sum(axis=(1, 3))
+
+
+def statistical_parity(renderer, scene, gpu_spp=4096, cpu_spp=256, block=2):
+    """GPU image vs the oracle's at the same scene.
+
+    Path-tracing samples are heavy-tailed (small lights, a 1e4 sun), so z-scores use the
+    per-pixel variance of the high-spp GPU run for both sides and are taken over 2x2 pixel
+    blocks. Thresholds were calibrated by running the oracle against itself with independent
+    seeds at the same sample counts (worst seen: 3.5% of blocks beyond 3 sigma, |median z| 0.21,
+    |global dz/se| 3.3): at most 6% of blocks outside 3 sigma, |median z| <= 0.35, global mean
+    within 6 standard errors and 3% relative.
+    """
     renderer.upload(scene_to_gpu(scene))
     renderer.render(samples=gpu_spp, keep_moments=True, frame_index=17)
     s, q, n = renderer.readback_sums(moments=True)
@@ -135,30 +149,33 @@ def statistical_parity(renderer, scene, gpu_spp, cpu_spp, max_outside=0.02):
     g_mean = s / n
     g_var = np.maximum(q / n - g_mean**2, 0.0) * n / (n - 1)
     cpu_scene = Scene(**{**scene.__dict__, "samples": cpu_spp})
-    o_mean, o_sq, _ = oracle.Oracle(cpu_scene).render(seed=3, moments=True)
-    o_mean = o_mean.astype(np.float64)
-    o_var = np.maximum(o_sq / cpu_spp - o_mean**2, 0.0) * cpu_spp / (cpu_spp - 1)
-    gl, ol = g_mean @ w, o_mean @ w
-    var = (g_var @ (w**2)) / gpu_spp + (o_var @ (w**2)) / cpu_spp
-    both_const = var == 0
-    assert np.allclose(gl[both_const], ol[both_const], atol=1e-5)
-    z = (gl - ol)[~both_const] / np.sqrt(var[~both_const])
-    outside = np.mean(np.abs(z) > 3.0)
-    assert outside <= max_outside, f"{outside:.4f} of pixels outside the 3-sigma band"
-    tot_se = math.sqrt(var.sum()) / var.size
-    assert abs(gl.mean() - ol.mean()) < 4 * tot_se + 1e-7, (gl.mean(), ol.mean(), tot_se)
+    o_mean, _, _ = oracle.Oracle(cpu_scene).render(seed=3)
+    gl, ol = g_mean @ w, o_mean.astype(np.float64) @ w
+    gv = g_var @ (w**2)
+    dm = _blocks(gl - ol, block) / block**2
+    var = _blocks(gv, block) * (1.0 / gpu_spp + 1.0 / cpu_spp) / block**4
+    const = var == 0
+    assert np.allclose(dm[const], 0.0, atol=1e-5)
+    z = dm[~const] / np.sqrt(var[~const])
+    outside = float(np.mean(np.abs(z) > 3.0))
+    assert outside <= 0.06, f"{outside:.4f} of blocks outside the 3-sigma band"
+    assert abs(float(np.median(z))) <= 0.35, f"median z {np.median(z):.3f}"
+    se = math.sqrt(gv.sum() * (1.0 / gpu_spp + 1.0 / cpu_spp)) / gv.size
+    dz = (gl.mean() - ol.mean()) / se
+    assert abs(dz) <= 6.0, f"global mean differs by {dz:.2f} standard errors"
+    assert abs(gl.mean() - ol.mean()) <= 0.03 * abs(ol.mean()), (gl.mean(), ol.mean())
     return outside
 
 
 def test_image_statistical_parity_plain_small(renderer):
     s = configs.plain_small()
     s.width, s.height = 80, 45
-    statistical_parity(renderer, s, gpu_spp=256, cpu_spp=64)
+    statistical_parity(renderer, s)
 
 
 def test_image_statistical_parity_mixed(renderer):
     s = configs.mixed(width=64, height=36, samples=64)
-    statistical_parity(renderer, s, gpu_spp=512, cpu_spp=64)
+    statistical_parity(renderer, s)
 
 
 def test_image_statistical_parity_sky_dielectric_metal(renderer):
@@ -168,7 +185,7 @@ def test_image_statistical_parity_sky_dielectric_metal(renderer):
               background=gt.SKY, materials=mats,
               sphere_centers=np.array([(-0.8, 0.5, 0), (0.8, 0.5, 0), (0, -100, 0), (0, 3, 0)], np.float32),
               sphere_radii=np.array([0.5, 0.5, 99.9, 0.4], np.float32), sphere_materials=np.array([0, 1, 2, 3], np.uint32))
-    statistical_parity(renderer, s, gpu_spp=512, cpu_spp=64)
+    statistical_parity(renderer, s)
 
 
 def test_progressive_accumulation_contract(renderer):
@@ -194,3 +211,28 @@ def test_invalid_scene_is_rejected(renderer):
     d.spheres["material_index"][0] = 10_000
     with pytest.raises(TcError, match="unknown material"):
         renderer.upload(d)
+
+
+def to_bf16_bits(x):
+    import torch
+
+    return torch.from_numpy(np.ascontiguousarray(x, np.float32)).to(torch.bfloat16).view(torch.int16).numpy().view(np.uint16)
+
+
+def from_bf16_bits(b):
+    import torch
+
+    return torch.from_numpy(b.view(np.int16)).view(torch.bfloat16).float().numpy()
+
+
+@pytest.mark.parametrize("a_mn,b_mn", [(False, False), (True, False), (False, True), (True, True)])
+@pytest.mark.parametrize("n,k", [(64, 80), (32, 64), (128, 16)])
+def test_tcgen05_tile_matches_fp32_matmul(native_lib, a_mn, b_mn, n, k):
+    from toaster_b200 import native
+
+    rng = np.random.default_rng(n * 1000 + k)
+    a = to_bf16_bits(rng.standard_normal((128, k)))
+    b = to_bf16_bits(rng.standard_normal((n, k)))
+    d = native.umma_selftest(a, b, a_mn, b_mn)
+    ref = from_bf16_bits(a).astype(np.float64) @ from_bf16_bits(b).astype(np.float64).T
+    assert np.allclose(d, ref, rtol=1e-3, atol=1e-3), np.abs(d - ref).max()

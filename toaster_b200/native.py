@@ -39,6 +39,7 @@ EXPORTED_SYMBOLS = (
     "tc_get_stats",
     "tc_build_bvh_host",
     "tc_record_sizes",
+    "tc_umma_selftest",
 )
 
 
@@ -128,6 +129,7 @@ def load_library(path: os.PathLike | None = None) -> ctypes.CDLL:
     lib.tc_build_bvh_host.argtypes = [vp, sz, vp, sz, vp, sz, vp, sz]
     lib.tc_build_bvh_host.restype = ctypes.c_long
     lib.tc_record_sizes.argtypes = [ctypes.POINTER(u32), sz]
+    lib.tc_umma_selftest.argtypes = [vp, vp, vp, i32, i32, i32, i32]
     for name in EXPORTED_SYMBOLS:
         if not hasattr(lib, name):
             raise RuntimeError(f"{p} does not export {name}")
@@ -159,6 +161,18 @@ def build_bvh_host(spheres: np.ndarray, triangles: np.ndarray):
     if count < 0:
         raise TcError(int(count), lib.tc_last_error(None).decode())
     return nodes[:count].copy(), prims[:n].copy()
+
+
+def umma_selftest(a: np.ndarray, b: np.ndarray, a_mn_major: bool = False, b_mn_major: bool = False) -> np.ndarray:
+    """D = A @ B.T on the tensor cores for bf16 bit patterns a (128 x k) and b (n x k)."""
+    lib = load_library()
+    a = np.ascontiguousarray(a, np.uint16)
+    b = np.ascontiguousarray(b, np.uint16)
+    n, k = b.shape
+    d = np.zeros((128, n), np.float32)
+    check(lib, None, lib.tc_umma_selftest(a.ctypes.data, b.ctypes.data, d.ctypes.data, n, k, int(a_mn_major),
+                                          int(b_mn_major)))
+    return d
 
 
 def record_sizes() -> list:
