@@ -206,6 +206,29 @@ int tc_trace_closest_device_async(tc_context* ctx, const float* d_rays, size_t n
 
 int tc_get_stats(const tc_context* ctx, tc_stats* out);
 
+/* Learned path guiding (no reference counterpart: toaster has no guiding) ----------------------
+ * An MLP maps an 80-wide encoding of a surface point (12-frequency Fourier features of
+ * (p - centre) * scale, plus the normal) through three 64-wide ReLU layers to an 8-lobe von
+ * Mises-Fisher mixture over directions. BF16 weights and activations, FP32 accumulation on the
+ * tcgen05 tensor cores, FP32 master weights and Adam. Parameters are packed as W1[64][80], b1[64],
+ * W2[64][64], b2[64], W3[64][64], b3[64], W4[32][64], b4[32] (15,584 floats); W1 columns 75..79
+ * are padding and stay zero. */
+#define TC_GUIDE_PARAMS 15584
+/* Sets the weights (resets the Adam state) and the encoding frame bounds = (cx, cy, cz, scale). */
+int tc_guide_set_params(tc_context* ctx, const float* params, const float* bounds);
+int tc_guide_get_params(tc_context* ctx, float* params);
+/* queries: n x 6 floats (position, normal); out: n x 40 floats = 8 x (mu.xyz, kappa) + 8 weights. */
+int tc_guide_infer(tc_context* ctx, const float* queries, size_t n, float* out);
+/* samples: n x 10 floats (position, normal, direction, weight). Writes the gradient of the mean
+ * weighted negative log-likelihood (TC_GUIDE_PARAMS floats) and the loss. */
+int tc_guide_loss_grad(tc_context* ctx, const float* samples, size_t n, float* grad, float* loss);
+/* One Adam step (beta 0.9/0.999, eps 1e-8) with the gradient of the last tc_guide_loss_grad. */
+int tc_guide_adam_step(tc_context* ctx, float lr);
+/* steps x (loss + gradient on `batch` samples + Adam) over the given samples, visited in a
+ * seeded random order. losses (optional) receives one value per step. */
+int tc_guide_train(tc_context* ctx, const float* samples, size_t n, uint32_t steps, uint32_t batch, float lr,
+                   uint64_t seed, float* losses);
+
 /* Tensor-core self-test (no reference counterpart): one 128 x n tile D = A * B^T with bf16 A
  * (128 x k, row-major) and B (n x k, row-major) staged in shared memory as K-major
  * (mn_major = 0) or MN-major (1) operands, FP32 accumulation in tensor memory. d receives

@@ -15,6 +15,7 @@
 #include "../../include/toaster_cuda.h"
 #include "bvh_build.h"
 #include "device_scene.h"
+#include "guide.h"
 #include "layout.h"
 
 static_assert(sizeof(tc_gpu_render_params) == 96, "GpuRenderParams is 96 bytes");
@@ -82,6 +83,11 @@ struct tc_context {
 
   // Parity scratch
   DevBuf ray_buf, prim_buf, t_buf;
+
+  // Path guiding
+  bool has_guide = false;
+  tcb::GuideDevice guide;
+  DevBuf g_params, g_m, g_v, g_grad, g_images, g_biases, g_status, g_in, g_out;
 
   tc_stats stats{};
 };
@@ -619,6 +625,192 @@ int tc_trace_closest(tc_context* ctx, const float* rays, size_t n, float tmin, u
   ctx->stats.extension_rays = n;
   ctx->stats.shadow_rays = 0;
   ctx->stats.paths = 0;
+  return TC_OK;
+}
+
+namespace {
+
+int guide_alloc(tc_context* ctx) {
+  if (ctx->has_guide) return TC_OK;
+  TC_CUDA(ctx, ctx->g_params.reserve(sizeof(float) * tcb::kGuideParams));
+  TC_CUDA(ctx, ctx->g_m.reserve(sizeof(float) * tcb::kGuideParams));
+  TC_CUDA(ctx, ctx->g_v.reserve(sizeof(float) * tcb::kGuideParams));
+  TC_CUDA(ctx, ctx->g_grad.reserve(sizeof(float) * (tcb::kGuideParams + 1)));
+  TC_CUDA(ctx, ctx->g_images.reserve(tcb::kImgBytes));
+  TC_CUDA(ctx, ctx->g_biases.reserve(sizeof(float) * 224));
+  TC_CUDA(ctx, ctx->g_status.reserve(sizeof(int)));
+  ctx->guide.params = ctx->g_params.as<float>();
+  ctx->guide.adam_m = ctx->g_m.as<float>();
+  ctx->guide.adam_v = ctx->g_v.as<float>();
+  ctx->guide.grad = ctx->g_grad.as<float>();
+  ctx->guide.images = ctx->g_images.as<uint8_t>();
+  ctx->guide.biases = ctx->g_biases.as<float>();
+  ctx->guide.status = ctx->g_status.as<int>();
+  ctx->has_guide = true;
+  return TC_OK;
+}
+
+int guide_check_status(tc_context* ctx) {
+  int status = 0;
+  TC_CUDA(ctx, cudaMemcpyAsync(&status, ctx->guide.status, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+  TC_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  if (status) {
+    cudaMemsetAsync(ctx->guide.status, 0, sizeof(int), ctx->stream);
+    return fail(ctx, TC_ERR_DEVICE_STATUS, "a guiding kernel gave up waiting for its tensor-core work");
+  }
+  return TC_OK;
+}
+
+// Samples as 3 float4 per sample (position + weight, normal, direction).
+void pack_samples(const float* s, size_t n, std::vector<float>& out) {
+  out.assign(n * 12, 0.0f);
+  for (size_t i = 0; i < n; ++i) {
+    const float* r = s + 10 * i;
+    float* o = out.data() + 12 * i;
+    o[0] = r[0]; o[1] = r[1]; o[2] = r[2]; o[3] = r[9];
+    o[4] = r[3]; o[5] = r[4]; o[6] = r[5];
+    o[8] = r[6]; o[9] = r[7]; o[10] = r[8];
+  }
+}
+
+}  // namespace
+
+int tc_guide_set_params(tc_context* ctx, const float* params, const float* bounds) {
+  if (!ctx) return fail(nullptr, TC_ERR_INVALID, "context is null");
+  if (!params || !bounds) return fail(ctx, TC_ERR_INVALID, "params or bounds is null");
+  if (!(bounds[3] > 0.0f) || !std::isfinite(bounds[3])) return fail(ctx, TC_ERR_INVALID, "bounds scale must be positive");
+  TC_CUDA(ctx, cudaSetDevice(ctx->device));
+  int rc = guide_alloc(ctx);
+  if (rc != TC_OK) return rc;
+  cudaStream_t st = ctx->stream;
+  TC_CUDA(ctx, cudaMemcpyAsync(ctx->guide.params, params, sizeof(float) * tcb::kGuideParams, cudaMemcpyHostToDevice, st));
+  TC_CUDA(ctx, cudaMemsetAsync(ctx->guide.adam_m, 0, sizeof(float) * tcb::kGuideParams, st));
+  TC_CUDA(ctx, cudaMemsetAsync(ctx->guide.adam_v, 0, sizeof(float) * tcb::kGuideParams, st));
+  TC_CUDA(ctx, cudaMemsetAsync(ctx->guide.grad, 0, sizeof(float) * (tcb::kGuideParams + 1), st));
+  TC_CUDA(ctx, cudaMemsetAsync(ctx->guide.status, 0, sizeof(int), st));
+  ctx->guide.bounds = tcb::GuideBounds{bounds[0], bounds[1], bounds[2], bounds[3]};
+  ctx->guide.adam_step = 0;
+  TC_CUDA(ctx, tcb::guide_refresh_images(ctx->guide, st));
+  TC_CUDA(ctx, cudaStreamSynchronize(st));
+  return TC_OK;
+}
+
+int tc_guide_get_params(tc_context* ctx, float* params) {
+  if (!ctx || !params) return fail(ctx, TC_ERR_INVALID, "context or output is null");
+  if (!ctx->has_guide) return fail(ctx, TC_ERR_STATE, "guiding parameters were never set");
+  TC_CUDA(ctx, cudaSetDevice(ctx->device));
+  TC_CUDA(ctx, cudaMemcpyAsync(params, ctx->guide.params, sizeof(float) * tcb::kGuideParams, cudaMemcpyDeviceToHost,
+                               ctx->stream));
+  TC_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return TC_OK;
+}
+
+int tc_guide_infer(tc_context* ctx, const float* queries, size_t n, float* out) {
+  if (!ctx) return fail(nullptr, TC_ERR_INVALID, "context is null");
+  if (!ctx->has_guide) return fail(ctx, TC_ERR_STATE, "guiding parameters were never set");
+  if (n == 0) return TC_OK;
+  if (!queries || !out) return fail(ctx, TC_ERR_INVALID, "query or output pointer is null");
+  TC_CUDA(ctx, cudaSetDevice(ctx->device));
+  std::vector<float> q(n * 8, 0.0f);
+  for (size_t i = 0; i < n; ++i)
+    for (int c = 0; c < 3; ++c) {
+      q[8 * i + c] = queries[6 * i + c];
+      q[8 * i + 4 + c] = queries[6 * i + 3 + c];
+    }
+  cudaStream_t st = ctx->stream;
+  TC_CUDA(ctx, ctx->g_in.reserve(sizeof(float) * q.size()));
+  TC_CUDA(ctx, ctx->g_out.reserve(sizeof(float4) * tcb::kGuideDecodedF4 * n));
+  TC_CUDA(ctx, cudaMemcpyAsync(ctx->g_in.ptr, q.data(), sizeof(float) * q.size(), cudaMemcpyHostToDevice, st));
+  TC_CUDA(ctx, cudaEventRecord(ctx->ev_kernel0, st));
+  TC_CUDA(ctx, tcb::guide_launch_infer(ctx->guide, ctx->g_in.as<float4>(), uint32_t(n), ctx->g_out.as<float4>(),
+                                       ctx->sm_count, st));
+  TC_CUDA(ctx, cudaEventRecord(ctx->ev_kernel1, st));
+  TC_CUDA(ctx, cudaMemcpyAsync(out, ctx->g_out.ptr, sizeof(float4) * tcb::kGuideDecodedF4 * n, cudaMemcpyDeviceToHost, st));
+  int rc = guide_check_status(ctx);
+  cudaEventElapsedTime(&ctx->stats.kernel_ms, ctx->ev_kernel0, ctx->ev_kernel1);
+  return rc;
+}
+
+int tc_guide_loss_grad(tc_context* ctx, const float* samples, size_t n, float* grad, float* loss) {
+  if (!ctx) return fail(nullptr, TC_ERR_INVALID, "context is null");
+  if (!ctx->has_guide) return fail(ctx, TC_ERR_STATE, "guiding parameters were never set");
+  if (n == 0 || !samples) return fail(ctx, TC_ERR_INVALID, "no samples");
+  TC_CUDA(ctx, cudaSetDevice(ctx->device));
+  std::vector<float> packed;
+  pack_samples(samples, n, packed);
+  cudaStream_t st = ctx->stream;
+  TC_CUDA(ctx, ctx->g_in.reserve(sizeof(float) * packed.size()));
+  TC_CUDA(ctx, cudaMemcpyAsync(ctx->g_in.ptr, packed.data(), sizeof(float) * packed.size(), cudaMemcpyHostToDevice, st));
+  TC_CUDA(ctx, cudaMemsetAsync(ctx->guide.grad, 0, sizeof(float) * (tcb::kGuideParams + 1), st));
+  TC_CUDA(ctx, cudaEventRecord(ctx->ev_kernel0, st));
+  TC_CUDA(ctx, tcb::guide_launch_loss_grad(ctx->guide, ctx->g_in.as<float4>(), uint32_t(n), 1.0f / float(n),
+                                           ctx->sm_count, st));
+  TC_CUDA(ctx, cudaEventRecord(ctx->ev_kernel1, st));
+  std::vector<float> g(tcb::kGuideParams + 1);
+  TC_CUDA(ctx, cudaMemcpyAsync(g.data(), ctx->guide.grad, sizeof(float) * g.size(), cudaMemcpyDeviceToHost, st));
+  int rc = guide_check_status(ctx);
+  cudaEventElapsedTime(&ctx->stats.kernel_ms, ctx->ev_kernel0, ctx->ev_kernel1);
+  if (rc != TC_OK) return rc;
+  if (grad) std::memcpy(grad, g.data(), sizeof(float) * tcb::kGuideParams);
+  if (loss) *loss = g[tcb::kGuideParams];
+  return TC_OK;
+}
+
+int tc_guide_adam_step(tc_context* ctx, float lr) {
+  if (!ctx) return fail(nullptr, TC_ERR_INVALID, "context is null");
+  if (!ctx->has_guide) return fail(ctx, TC_ERR_STATE, "guiding parameters were never set");
+  TC_CUDA(ctx, cudaSetDevice(ctx->device));
+  TC_CUDA(ctx, tcb::guide_launch_adam(ctx->guide, lr, ctx->stream));
+  TC_CUDA(ctx, cudaMemsetAsync(ctx->guide.grad + tcb::kGuideParams, 0, sizeof(float), ctx->stream));
+  TC_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return TC_OK;
+}
+
+int tc_guide_train(tc_context* ctx, const float* samples, size_t n, uint32_t steps, uint32_t batch, float lr,
+                   uint64_t seed, float* losses) {
+  if (!ctx) return fail(nullptr, TC_ERR_INVALID, "context is null");
+  if (!ctx->has_guide) return fail(ctx, TC_ERR_STATE, "guiding parameters were never set");
+  if (n == 0 || !samples || batch == 0) return fail(ctx, TC_ERR_INVALID, "no samples or zero batch");
+  TC_CUDA(ctx, cudaSetDevice(ctx->device));
+  // Seeded shuffle (SplitMix64-driven Fisher-Yates), then consecutive batches.
+  std::vector<uint32_t> order(n);
+  for (size_t i = 0; i < n; ++i) order[i] = uint32_t(i);
+  uint64_t x = seed;
+  auto next = [&x]() {
+    uint64_t z = (x += 0x9E3779B97F4A7C15ull);
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+  };
+  for (size_t i = n - 1; i > 0; --i) std::swap(order[i], order[size_t(next() % (i + 1))]);
+  std::vector<float> shuffled(n * 10);
+  for (size_t i = 0; i < n; ++i) std::memcpy(&shuffled[10 * i], samples + 10 * size_t(order[i]), 40);
+  std::vector<float> packed;
+  pack_samples(shuffled.data(), n, packed);
+  cudaStream_t st = ctx->stream;
+  TC_CUDA(ctx, ctx->g_in.reserve(sizeof(float) * packed.size()));
+  TC_CUDA(ctx, cudaMemcpyAsync(ctx->g_in.ptr, packed.data(), sizeof(float) * packed.size(), cudaMemcpyHostToDevice, st));
+  const uint32_t b = uint32_t(std::min<size_t>(batch, n));
+  std::vector<float> step_loss(steps, 0.0f);
+  TC_CUDA(ctx, ctx->g_out.reserve(sizeof(float) * std::max<uint32_t>(steps, 1)));
+  TC_CUDA(ctx, cudaEventRecord(ctx->ev_kernel0, st));
+  size_t cursor = 0;
+  for (uint32_t s = 0; s < steps; ++s) {
+    if (cursor + b > n) cursor = 0;
+    TC_CUDA(ctx, tcb::guide_launch_loss_grad(ctx->guide, ctx->g_in.as<float4>() + 3 * cursor, b, 1.0f / float(b),
+                                             ctx->sm_count, st));
+    TC_CUDA(ctx, cudaMemcpyAsync(ctx->g_out.as<float>() + s, ctx->guide.grad + tcb::kGuideParams, sizeof(float),
+                                 cudaMemcpyDeviceToDevice, st));
+    TC_CUDA(ctx, cudaMemsetAsync(ctx->guide.grad + tcb::kGuideParams, 0, sizeof(float), st));
+    TC_CUDA(ctx, tcb::guide_launch_adam(ctx->guide, lr, st));
+    cursor += b;
+  }
+  TC_CUDA(ctx, cudaEventRecord(ctx->ev_kernel1, st));
+  if (steps) TC_CUDA(ctx, cudaMemcpyAsync(step_loss.data(), ctx->g_out.ptr, sizeof(float) * steps, cudaMemcpyDeviceToHost, st));
+  int rc = guide_check_status(ctx);
+  cudaEventElapsedTime(&ctx->stats.kernel_ms, ctx->ev_kernel0, ctx->ev_kernel1);
+  if (rc != TC_OK) return rc;
+  if (losses) std::memcpy(losses, step_loss.data(), sizeof(float) * steps);
   return TC_OK;
 }
 

@@ -112,6 +112,8 @@ struct TraceResult {
   uint32_t rec;   // PrimRecord index of the accepted primitive
 };
 
+constexpr uint32_t kNoNode = 0xFFFFFFFFu;  // never a valid link (leaf links stay below 0xC0000000)
+
 // Ordered closest-hit traversal (any_hit = false) or first-hit occlusion query (any_hit = true)
 // over the sibling-pair hierarchy, returning whether a primitive was accepted in [tmin, tmax].
 //
@@ -121,6 +123,11 @@ struct TraceResult {
 // does); a stacked child is re-tested on pop, which for a box that passed at push time reduces
 // to `tn <= closest`; leaf primitives are tested in leaf order and accepted on `t <= closest`.
 // Stack depth never exceeds the hierarchy depth, which the host checks against kMaxStack.
+//
+// The loop is the "while-while" form: an inner loop descends through interior nodes until every
+// lane holds a leaf (or has finished), then the lanes test their leaves together. A single loop
+// structure with one reconvergence point per phase keeps the warp's lanes executing together;
+// each ray still visits exactly the nodes, in exactly the order, of the sequential algorithm.
 __device__ __forceinline__ bool trace_ray(const PairNode* __restrict__ pairs, const PrimRecord* __restrict__ prims,
                                           const ChildRec& root, const RayQ& r, float tmin, float tmax,
                                           bool any_hit, TraceResult& res, uint32_t& node_visits) {
@@ -133,36 +140,9 @@ __device__ __forceinline__ bool trace_ray(const PairNode* __restrict__ pairs, co
   float st_tn[kMaxStack];
   int sp = 0;
   uint32_t cur = root.link;
-  for (;;) {
-    if (cur & kLeafBit) {
-      uint32_t k = cur & ~kLeafBit;
-      for (;;) {
-        const float4* p = reinterpret_cast<const float4*>(prims + k);
-        const float4 A = __ldg(p);
-        const float4 B = __ldg(p + 1);
-        const uint32_t tag = __float_as_uint(A.w);
-        float t;
-        bool ok;
-        if (tag & kTagTriangle) {
-          const float4 C = __ldg(p + 2);
-          ok = hit_triangle(r, A, B, C, tmin, closest, t);
-        } else {
-          ok = hit_sphere(r, A, B, tmin, closest, t);
-        }
-        if (ok) {
-          closest = t;
-          found = true;
-          res.tag = tag;
-          res.rec = k;
-          if (any_hit) {
-            res.t = closest;
-            return true;
-          }
-        }
-        if (tag & kTagLast) break;
-        ++k;
-      }
-    } else {
+  while (cur != kNoNode) {
+    // Descend: interior nodes until a leaf is reached or the stack is exhausted.
+    while ((cur & kLeafBit) == 0u) {
       ++node_visits;
       const float4* q = reinterpret_cast<const float4*>(pairs + cur);
       const float4 a0 = __ldg(q), a1 = __ldg(q + 1), b0 = __ldg(q + 2), b1 = __ldg(q + 3);
@@ -176,21 +156,58 @@ __device__ __forceinline__ bool trace_ray(const PairNode* __restrict__ pairs, co
         st_tn[sp] = a_first ? tb : ta;
         ++sp;
         cur = a_first ? la : lb;
-        continue;
+      } else if (ha) {
+        cur = la;
+      } else if (hb) {
+        cur = lb;
+      } else {
+        cur = kNoNode;
+        while (sp > 0) {
+          --sp;
+          if (st_tn[sp] <= closest) {
+            cur = st_ref[sp];
+            break;
+          }
+        }
+        if (cur == kNoNode) break;
       }
-      if (ha) { cur = la; continue; }
-      if (hb) { cur = lb; continue; }
     }
-    bool popped = false;
+    if (cur == kNoNode) break;
+    // Leaf: primitives in leaf order.
+    uint32_t k = cur & ~kLeafBit;
+    for (;;) {
+      const float4* p = reinterpret_cast<const float4*>(prims + k);
+      const float4 A = __ldg(p);
+      const float4 B = __ldg(p + 1);
+      const uint32_t tag = __float_as_uint(A.w);
+      float t;
+      bool ok;
+      if (tag & kTagTriangle) {
+        const float4 C = __ldg(p + 2);
+        ok = hit_triangle(r, A, B, C, tmin, closest, t);
+      } else {
+        ok = hit_sphere(r, A, B, tmin, closest, t);
+      }
+      if (ok) {
+        closest = t;
+        found = true;
+        res.tag = tag;
+        res.rec = k;
+        if (any_hit) break;
+      }
+      if (tag & kTagLast) break;
+      ++k;
+    }
+    if (any_hit && found) break;
+    // Next stacked node that survives the re-test against the updated closest distance.
+    cur = kNoNode;
     while (sp > 0) {
       --sp;
       if (st_tn[sp] <= closest) {
         cur = st_ref[sp];
-        popped = true;
         break;
       }
     }
-    if (!popped) break;
   }
   res.t = closest;
   return found;

@@ -40,7 +40,15 @@ EXPORTED_SYMBOLS = (
     "tc_build_bvh_host",
     "tc_record_sizes",
     "tc_umma_selftest",
+    "tc_guide_set_params",
+    "tc_guide_get_params",
+    "tc_guide_infer",
+    "tc_guide_loss_grad",
+    "tc_guide_adam_step",
+    "tc_guide_train",
 )
+
+GUIDE_PARAMS = 15584
 
 
 class TcError(RuntimeError):
@@ -130,6 +138,12 @@ def load_library(path: os.PathLike | None = None) -> ctypes.CDLL:
     lib.tc_build_bvh_host.restype = ctypes.c_long
     lib.tc_record_sizes.argtypes = [ctypes.POINTER(u32), sz]
     lib.tc_umma_selftest.argtypes = [vp, vp, vp, i32, i32, i32, i32]
+    lib.tc_guide_set_params.argtypes = [vp, vp, vp]
+    lib.tc_guide_get_params.argtypes = [vp, vp]
+    lib.tc_guide_infer.argtypes = [vp, vp, sz, vp]
+    lib.tc_guide_loss_grad.argtypes = [vp, vp, sz, vp, vp]
+    lib.tc_guide_adam_step.argtypes = [vp, f32]
+    lib.tc_guide_train.argtypes = [vp, vp, sz, u32, u32, f32, ctypes.c_uint64, vp]
     for name in EXPORTED_SYMBOLS:
         if not hasattr(lib, name):
             raise RuntimeError(f"{p} does not export {name}")

@@ -166,6 +166,46 @@ class GpuRenderer:
         self._check(self._lib.tc_trace_closest_device_async(self._ctx, rays_ptr, n, tmin, prim_ptr, t_ptr,
                                                             stream or None))
 
+    # ---------------------------------------------------------------- path-guiding network
+    def guide_set_params(self, params: np.ndarray, bounds) -> None:
+        """FP32 weights (TC_GUIDE_PARAMS) and encoding frame (cx, cy, cz, scale); resets Adam."""
+        p = np.ascontiguousarray(params, np.float32).reshape(-1)
+        if p.size != native.GUIDE_PARAMS:
+            raise ValueError(f"expected {native.GUIDE_PARAMS} parameters, got {p.size}")
+        b = np.ascontiguousarray(bounds, np.float32).reshape(4)
+        self._check(self._lib.tc_guide_set_params(self._ctx, p.ctypes.data, b.ctypes.data))
+
+    def guide_get_params(self) -> np.ndarray:
+        out = np.empty(native.GUIDE_PARAMS, np.float32)
+        self._check(self._lib.tc_guide_get_params(self._ctx, out.ctypes.data))
+        return out
+
+    def guide_infer(self, points: np.ndarray, normals: np.ndarray) -> np.ndarray:
+        """Decoded mixtures (n, 40): 8 x (mu.xyz, kappa) then 8 weights."""
+        q = np.ascontiguousarray(np.concatenate([points, normals], axis=1), np.float32)
+        out = np.empty((q.shape[0], 40), np.float32)
+        self._check(self._lib.tc_guide_infer(self._ctx, q.ctypes.data, q.shape[0], out.ctypes.data))
+        return out
+
+    def guide_loss_grad(self, samples: np.ndarray):
+        """Mean weighted NLL and its gradient for samples (n, 10): position, normal, direction, weight."""
+        s = np.ascontiguousarray(samples, np.float32).reshape(-1, 10)
+        grad = np.empty(native.GUIDE_PARAMS, np.float32)
+        loss = ctypes.c_float()
+        self._check(self._lib.tc_guide_loss_grad(self._ctx, s.ctypes.data, s.shape[0], grad.ctypes.data,
+                                                 ctypes.byref(loss)))
+        return grad, float(loss.value)
+
+    def guide_adam_step(self, lr: float = 1e-2) -> None:
+        self._check(self._lib.tc_guide_adam_step(self._ctx, lr))
+
+    def guide_train(self, samples: np.ndarray, steps: int, batch: int, lr: float = 1e-2, seed: int = 0) -> np.ndarray:
+        s = np.ascontiguousarray(samples, np.float32).reshape(-1, 10)
+        losses = np.empty(max(steps, 1), np.float32)
+        self._check(self._lib.tc_guide_train(self._ctx, s.ctypes.data, s.shape[0], steps, batch, lr, seed,
+                                             losses.ctypes.data))
+        return losses[:steps]
+
     def stats(self) -> dict:
         s = native.Stats()
         self._check(self._lib.tc_get_stats(self._ctx, ctypes.byref(s)))
