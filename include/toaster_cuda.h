@@ -138,8 +138,10 @@ typedef struct tc_render_options {
   uint32_t block_size;       /* threads per block for the path kernel; 0 = tuned default */
   uint32_t samples_per_item; /* samples one lane traces for a pixel before taking new work; 0 = default */
   uint32_t keep_moments;     /* 1: also accumulate per-pixel sums of squared samples (FP64) */
-  uint32_t guiding;          /* 1: learned path guiding (requires tc_guiding_* setup) */
-  uint32_t _reserved[4];
+  uint32_t guiding;          /* 1: learned path guiding at diffuse vertices (needs tc_guide_set_params) */
+  uint32_t guide_record;     /* 1: record (position, normal, direction, incident radiance) training
+                                samples at every diffuse scatter of this batch (plain sampling) */
+  uint32_t _reserved[3];
 } tc_render_options;
 
 /* Counters of the most recent tc_render / tc_trace_* call. */
@@ -187,6 +189,23 @@ int tc_render(tc_context* ctx, const tc_gpu_render_params* params, const tc_rend
  * float4 linear-HDR averages into rgba (n_floats >= 4*width*height). */
 int tc_readback(tc_context* ctx, float* rgba, size_t n_floats);
 
+/* Same traversal and estimator as tc_render, for callers that cannot allocate device memory at
+ * render time: code running inside CUDA stream capture, hosts whose device memory is owned by
+ * their own pool or framework allocator, and embedders with a fixed memory budget. No reference
+ * counterpart (toaster-gpu allocates all its buffers through wgpu).
+ * It allocates nothing. The scene comes from an earlier tc_upload_scene; the caller supplies the
+ * FP64 per-pixel sums: `sums` is device memory of at least 3*width*height doubles (n_doubles).
+ * accumulated_samples == 0 clears it first, otherwise the batch is added to it. The image is
+ * sums / (total samples), which the caller tracks. The kernel's scratch (work counter and
+ * counters) is a 256-byte static device array holding at most 32 words; this call uses 4, at any
+ * image size. It is shared by every call: calls whose work overlaps on the GPU race, so
+ * serialise them (one stream, or wait between calls). The first call on a device looks up that
+ * array's address (cudaGetSymbolAddress), so make it before any stream capture. The work is
+ * enqueued on `stream` (NULL = the context's stream) and not synchronised. Rejects frames above
+ * 2^31 pixels and sums buffers smaller than 3*width*height doubles. */
+int tc_render_no_alloc(tc_context* ctx, const tc_gpu_render_params* params, double* sums, size_t n_doubles,
+                       void* stream);
+
 /* Per-pixel FP64 running sums (3 per pixel) and, when keep_moments was set, sums of squared
  * sample values (3 per pixel). Either pointer may be NULL. *samples receives the count. */
 int tc_readback_sums(tc_context* ctx, double* sum, double* sum_sq, size_t n_doubles, uint32_t* samples);
@@ -228,6 +247,14 @@ int tc_guide_adam_step(tc_context* ctx, float lr);
  * seeded random order. losses (optional) receives one value per step. */
 int tc_guide_train(tc_context* ctx, const float* samples, size_t n, uint32_t steps, uint32_t batch, float lr,
                    uint64_t seed, float* losses);
+
+/* Builds training samples from the diffuse scatters recorded by the last tc_render with
+ * guide_record = 1 (weight = luminance of the radiance that arrived along each scattered
+ * direction, normalised by its mean and clamped at 50x the mean) and runs `steps` Adam steps on
+ * batches of `batch` samples drawn at random. losses (optional) receives one value per step and
+ * n_samples (optional) the number of samples. */
+int tc_guide_train_recorded(tc_context* ctx, uint32_t steps, uint32_t batch, float lr, uint64_t seed, float* losses,
+                            uint32_t* n_samples);
 
 /* Tensor-core self-test (no reference counterpart): one 128 x n tile D = A * B^T with bf16 A
  * (128 x k, row-major) and B (n x k, row-major) staged in shared memory as K-major

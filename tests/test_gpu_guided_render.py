@@ -1,0 +1,76 @@
+"""Guided rendering (needs a B200): unbiased against plain sampling, trainable from recorded samples."""
+
+import math
+
+import numpy as np
+import pytest
+
+from oracle import guide_net as gn
+from toaster_b200 import configs, guiding_eval
+from toaster_b200.scene import scene_to_gpu
+
+pytestmark = pytest.mark.gpu
+
+
+def test_initial_params_match_the_reference_init():
+    assert np.array_equal(guiding_eval.initial_params(3), gn.init_params(3))
+
+
+def blocks(x, b):
+    h, w = x.shape
+    return x[: h // b * b, : w // b * b].reshape(h // b, b, w // b, b).sum(axis=(1, 3))
+
+
+def render_moments(r, spp, **kw):
+    r.render(samples=spp, keep_moments=True, **kw)
+    s, q, n = r.readback_sums(moments=True)
+    w = np.array([0.2126, 0.7152, 0.0722])
+    m = s / n
+    v = np.maximum(q / n - m * m, 0.0) * n / (n - 1)
+    return m @ w, v @ (w**2), n
+
+
+@pytest.mark.parametrize("make", [lambda: configs.mixed(width=64, height=36, samples=64),
+                                  lambda: configs.room_with_window(width=64, height=36, samples=64, clutter=1024)],
+                         ids=["mixed", "room"])
+def test_guided_sampling_is_unbiased(renderer, make):
+    # Untrained (random) network: the one-sample MIS of BSDF and guide sampling must still give
+    # the plain estimator's expectation.
+    scene = make()
+    renderer.upload(scene_to_gpu(scene))
+    renderer.guide_set_params(guiding_eval.initial_params(7), configs.scene_bounds(scene))
+    pl, pv, n = render_moments(renderer, 2048, frame_index=3)
+    gl, gv, m = render_moments(renderer, 2048, frame_index=4, guiding=True)
+    d = blocks(gl - pl, 2) / 4
+    var = (blocks(pv, 2) / n + blocks(gv, 2) / m) / 16
+    nz = var > 0
+    z = d[nz] / np.sqrt(var[nz])
+    assert np.mean(np.abs(z) > 3) <= 0.06, np.mean(np.abs(z) > 3)
+    assert abs(np.median(z)) <= 0.35
+    se = math.sqrt((pv.sum() / n + gv.sum() / m)) / pv.size
+    assert abs(gl.mean() - pl.mean()) <= 6 * se, (gl.mean(), pl.mean(), se)
+
+
+def test_record_train_and_render_guided(renderer):
+    scene = configs.room_with_window(width=96, height=54, samples=16, clutter=2048)
+    renderer.upload(scene_to_gpu(scene))
+    renderer.guide_set_params(guiding_eval.initial_params(1), configs.scene_bounds(scene))
+    renderer.render(samples=16, frame_index=0, guide_record=True)
+    losses, n = renderer.guide_train_recorded(steps=100, batch=4096, lr=1e-2, seed=5)
+    assert n > 10_000
+    assert np.all(np.isfinite(losses))
+    assert losses[-10:].mean() < losses[:5].mean()
+    renderer.render(samples=16, frame_index=1, accumulate=True, guiding=True)
+    assert renderer.accumulated == 32
+    img = renderer.readback()
+    assert np.all(np.isfinite(img))
+    st = renderer.stats()
+    assert st["paths"] == 96 * 54 * 16
+
+
+def test_guiding_reduces_error_at_equal_time(native_lib):
+    scene = configs.room_with_window(width=64, height=36, clutter=2048)
+    out = guiding_eval.equal_time_comparison(scene, ref_spp=16384, plain_spp=256, batch=16, train_steps=200,
+                                             train_batch=8192, seed=2)
+    assert out["guided_rmse_at_plain_time"] is not None
+    assert out["guided_rmse_at_plain_time"] < out["plain_rmse"], out

@@ -254,3 +254,68 @@ def large_mesh(seed: int = 7, grid: int = 1024, width: int = 1920, height: int =
         triangles=tris, triangle_materials=np.zeros(tris.shape[0], np.uint32),
         environment=environment if environment is not None else sky_environment(),
     )
+
+
+def _quad(a, b, c, d):
+    """Two triangles of the quad a-b-c-d (counter-clockwise)."""
+    return [[a, b, c], [a, c, d]]
+
+
+def room_with_window(seed: int = 0, width: int = 1280, height: int = 720, samples: int = 16, max_bounces: int = 8,
+                     clutter: int = 8192, environment: EnvironmentMap | None = None) -> Scene:
+    """Hard-lighting interior: a closed 4 x 3 x 4 room (x, z in [-2, 2], y in [0, 3]) whose only
+    opening is a 0.4 x 0.4 window in the +z wall (x in [0.3, 0.7], y in [1.6, 2.0]); it is lit only
+    by the mixed-scene sky and sun through that window. Walls 0.7, floor 0.5, ceiling 0.8 diffuse.
+    ``clutter`` seeded triangles (centre uniform in [-1.8, 1.8] x [0.1, 2.5] x [-1.8, 1.6], edges as in
+    random_triangles) are 70% diffuse (albedo U[0.2, 0.8]^3) and 30% metal (albedo U[0.5, 0.95]^3,
+    roughness U[0, 0.5]). The camera stands near the -z wall looking toward the window wall."""
+    rng = np.random.default_rng(seed + 5000)
+    x0, x1, y0, y1, z0, z1 = -2.0, 2.0, 0.0, 3.0, -2.0, 2.0
+    wx0, wx1, wy0, wy1 = 0.3, 0.7, 1.6, 2.0
+    shell = []
+    shell += _quad((x0, y0, z0), (x1, y0, z0), (x1, y0, z1), (x0, y0, z1))  # floor
+    shell += _quad((x0, y1, z0), (x0, y1, z1), (x1, y1, z1), (x1, y1, z0))  # ceiling
+    shell += _quad((x0, y0, z0), (x0, y1, z0), (x1, y1, z0), (x1, y0, z0))  # -z wall
+    shell += _quad((x0, y0, z0), (x0, y0, z1), (x0, y1, z1), (x0, y1, z0))  # -x wall
+    shell += _quad((x1, y0, z0), (x1, y1, z0), (x1, y1, z1), (x1, y0, z1))  # +x wall
+    # +z wall with the window cut out: below, above, left and right of the opening.
+    shell += _quad((x0, y0, z1), (x1, y0, z1), (x1, wy0, z1), (x0, wy0, z1))
+    shell += _quad((x0, wy1, z1), (x1, wy1, z1), (x1, y1, z1), (x0, y1, z1))
+    shell += _quad((x0, wy0, z1), (wx0, wy0, z1), (wx0, wy1, z1), (x0, wy1, z1))
+    shell += _quad((wx1, wy0, z1), (x1, wy0, z1), (x1, wy1, z1), (wx1, wy1, z1))
+    shell = np.array(shell, np.float32)
+    shell_mat = np.array([0, 0, 1, 1] + [2] * 14, np.uint32)  # floor, ceiling, walls
+    mats = [Material.diffuse((0.5, 0.5, 0.5), "floor"), Material.diffuse((0.8, 0.8, 0.8), "ceiling"),
+            Material.diffuse((0.7, 0.7, 0.7), "walls")]
+    tris = random_triangles(clutter, seed + 1)
+    lo = np.array([-1.8, 0.1, -1.8]); hi = np.array([1.8, 2.5, 1.6])
+    centre = tris.mean(axis=1, keepdims=True)
+    tris = (tris - centre + (lo + (centre + 1.0) / 2.0 * (hi - lo))).astype(np.float32)
+    kinds = rng.uniform(0, 1, clutter)
+    clutter_mat = []
+    for i in range(clutter):
+        if kinds[i] < 0.7:
+            mats.append(Material.diffuse(rng.uniform(0.2, 0.8, 3), f"c{i}"))
+        else:
+            mats.append(Material.metal(rng.uniform(0.5, 0.95, 3), rng.uniform(0.0, 0.5), f"c{i}"))
+        clutter_mat.append(len(mats) - 1)
+    return Scene(
+        camera_position=(-1.0, 1.5, -1.8), camera_look_at=(0.5, 1.2, 1.0), fov_degrees=60.0,
+        width=width, height=height, samples=samples, max_bounces=max_bounces, background=gt.ENVIRONMENT,
+        materials=mats, triangles=np.concatenate([shell, tris]),
+        triangle_materials=np.concatenate([shell_mat, np.array(clutter_mat, np.uint32)]),
+        environment=environment if environment is not None else sky_environment(),
+    )
+
+
+def scene_bounds(scene: Scene):
+    """(centre xyz, scale) mapping the scene's bounding box into [-1, 1] (guiding encoding frame)."""
+    pts = [scene.triangles.reshape(-1, 3)] if scene.triangle_count else []
+    if scene.sphere_count:
+        r = scene.sphere_radii[:, None]
+        pts += [scene.sphere_centers - r, scene.sphere_centers + r]
+    allp = np.concatenate(pts).astype(np.float64)
+    lo, hi = allp.min(0), allp.max(0)
+    centre = (lo + hi) / 2
+    half = max(float((hi - lo).max()) / 2, 1e-6)
+    return (float(centre[0]), float(centre[1]), float(centre[2]), 1.0 / half)

@@ -88,6 +88,12 @@ struct tc_context {
   bool has_guide = false;
   tcb::GuideDevice guide;
   DevBuf g_params, g_m, g_v, g_grad, g_images, g_biases, g_status, g_in, g_out;
+  // Guided wavefront buffers (two state buffers, queries, decoded mixtures, round counters).
+  DevBuf w_state_a, w_state_b, w_query, w_mix, w_counts;
+  // Recorded training data of the last guide_record batch.
+  DevBuf rec_records, rec_count, rec_path_rad, rec_samples, rec_wsum;
+  uint32_t rec_capacity = 0;
+  bool has_records = false;
 
   tc_stats stats{};
 };
@@ -487,7 +493,6 @@ int tc_render(tc_context* ctx, const tc_gpu_render_params* p, const tc_render_op
   tc_render_options o{};
   if (opt) o = *opt;
   const bool moments = o.keep_moments != 0;
-  if (o.guiding) return fail(ctx, TC_ERR_STATE, "guided rendering needs a trained guiding network");
   const uint32_t npix = p->width * p->height;
   cudaStream_t st = ctx->stream;
   TC_CUDA(ctx, cudaEventRecord(ctx->ev_begin, st));
@@ -524,7 +529,7 @@ int tc_render(tc_context* ctx, const tc_gpu_render_params* p, const tc_render_op
   L.max_bounces = p->max_bounces;
   L.frame_index = p->frame_index;
   L.sample_base = ctx->accumulated;
-  L.samples_per_item = std::min<uint32_t>(o.samples_per_item ? o.samples_per_item : 4u, p->samples);
+  L.samples_per_item = std::min<uint32_t>(o.samples_per_item ? o.samples_per_item : 1u, p->samples);
   L.items_per_pixel = (p->samples + L.samples_per_item - 1) / L.samples_per_item;
   L.total_items = uint64_t(npix) * L.items_per_pixel;
   L.accum = ctx->accum.as<double>();
@@ -536,17 +541,81 @@ int tc_render(tc_context* ctx, const tc_gpu_render_params* p, const tc_render_op
   const int block = o.block_size ? int(o.block_size) : 128;
   if (block % 32 != 0 || block < 32 || block > 256)
     return fail(ctx, TC_ERR_INVALID, "block_size must be a multiple of 32 in [32, 256]");
-  int per_sm = tcb::render_max_blocks_per_sm(block, moments);
+  if (o.guiding && o.guide_record) return fail(ctx, TC_ERR_INVALID, "guiding and guide_record are exclusive");
+  if (o.guiding && !ctx->has_guide) return fail(ctx, TC_ERR_STATE, "guided rendering needs tc_guide_set_params first");
+  const int mode = o.guiding ? tcb::kModeGuided : (o.guide_record ? tcb::kModeRecord : tcb::kModePlain);
+  int per_sm = tcb::render_max_blocks_per_sm(block, moments, mode);
   if (per_sm <= 0) return fail(ctx, TC_ERR_CUDA, "render kernel cannot be resident with this block size");
   const int grid = per_sm * ctx->sm_count;
+  if (mode == tcb::kModeRecord) {
+    // One record per diffuse scatter (capped) and the final radiance of every path of the batch.
+    const uint64_t paths = uint64_t(npix) * p->samples;
+    if (paths > (1ull << 31)) return fail(ctx, TC_ERR_INVALID, "too many paths to record in one batch");
+    ctx->rec_capacity = uint32_t(std::min<uint64_t>(2 * paths, uint64_t(1) << 23));
+    TC_CUDA(ctx, ctx->rec_records.reserve(sizeof(float4) * 4 * size_t(ctx->rec_capacity)));
+    TC_CUDA(ctx, ctx->rec_count.reserve(sizeof(uint32_t)));
+    TC_CUDA(ctx, ctx->rec_path_rad.reserve(sizeof(float4) * size_t(paths)));
+    TC_CUDA(ctx, cudaMemsetAsync(ctx->rec_count.ptr, 0, sizeof(uint32_t), st));
+    L.g.records = ctx->rec_records.as<float4>();
+    L.g.record_count = ctx->rec_count.as<uint32_t>();
+    L.g.record_capacity = ctx->rec_capacity;
+    L.g.path_radiance = ctx->rec_path_rad.as<float4>();
+  }
   TC_CUDA(ctx, cudaEventRecord(ctx->ev_kernel0, st));
-  TC_CUDA(ctx, tcb::launch_render(L, block, grid, moments, st));
+  if (mode != tcb::kModeGuided) {
+    TC_CUDA(ctx, tcb::launch_render(L, block, grid, moments, st, mode));
+  } else {
+    // Wavefront: waves of whole samples per pixel; within a wave, rounds of (path kernel ->
+    // suspended diffuse vertices -> tensor-core inference of their mixtures -> resume). Counts
+    // stay on the device, so the rounds need no host synchronisation.
+    const uint32_t kWaveCap = 1u << 21;
+    const uint32_t wave_spp = std::max<uint32_t>(1u, std::min<uint32_t>(p->samples, kWaveCap / npix));
+    const uint32_t cap = wave_spp * npix;
+    const uint32_t rounds = p->max_bounces > 1 ? p->max_bounces - 1 : 0;
+    TC_CUDA(ctx, ctx->w_state_a.reserve(sizeof(float4) * 6 * size_t(cap)));
+    TC_CUDA(ctx, ctx->w_state_b.reserve(sizeof(float4) * 6 * size_t(cap)));
+    TC_CUDA(ctx, ctx->w_query.reserve(sizeof(float4) * 2 * size_t(cap)));
+    TC_CUDA(ctx, ctx->w_mix.reserve(sizeof(float4) * tcb::kGuideDecodedF4 * size_t(cap)));
+    TC_CUDA(ctx, ctx->w_counts.reserve(sizeof(uint32_t) * (rounds + 2)));
+    float4* state_in = ctx->w_state_a.as<float4>();
+    float4* state_out = ctx->w_state_b.as<float4>();
+    uint32_t* counts = ctx->w_counts.as<uint32_t>();
+    for (uint32_t first = 0; first < p->samples; first += wave_spp) {
+      const uint32_t ws = std::min(wave_spp, p->samples - first);
+      TC_CUDA(ctx, cudaMemsetAsync(counts, 0, sizeof(uint32_t) * (rounds + 2), st));
+      tcb::RenderLaunch R = L;
+      R.total_items = uint64_t(npix) * ws;
+      R.g.capacity = cap;
+      R.g.out_query = ctx->w_query.as<float4>();
+      R.g.wave_first_sample = ctx->accumulated + first;
+      R.g.wave_spp = ws;
+      R.g.resume = 0;
+      R.g.out_state = state_out;
+      R.g.out_count = counts;
+      TC_CUDA(ctx, cudaMemsetAsync(ctx->work_counter.ptr, 0, sizeof(unsigned long long), st));
+      TC_CUDA(ctx, tcb::launch_render(R, block, grid, moments, st, mode));
+      for (uint32_t r = 0; r < rounds; ++r) {
+        std::swap(state_in, state_out);
+        TC_CUDA(ctx, tcb::guide_launch_infer(ctx->guide, ctx->w_query.as<float4>(), cap, ctx->w_mix.as<float4>(),
+                                             ctx->sm_count, st, counts + r));
+        R.g.resume = 1;
+        R.g.in_state = state_in;
+        R.g.in_count = counts + r;
+        R.g.in_mix = ctx->w_mix.as<float4>();
+        R.g.out_state = state_out;
+        R.g.out_count = counts + r + 1;
+        TC_CUDA(ctx, cudaMemsetAsync(ctx->work_counter.ptr, 0, sizeof(unsigned long long), st));
+        TC_CUDA(ctx, tcb::launch_render(R, block, grid, moments, st, mode));
+      }
+    }
+  }
   TC_CUDA(ctx, cudaEventRecord(ctx->ev_kernel1, st));
   unsigned long long counters[4] = {0, 0, 0, 0};
   TC_CUDA(ctx, cudaMemcpyAsync(counters, ctx->counters.ptr, sizeof(counters), cudaMemcpyDeviceToHost, st));
   TC_CUDA(ctx, cudaEventRecord(ctx->ev_end, st));
   TC_CUDA(ctx, cudaStreamSynchronize(st));
   ctx->accumulated += p->samples;
+  if (mode == tcb::kModeRecord) ctx->has_records = true;
   ctx->stats.paths = counters[0];
   ctx->stats.extension_rays = counters[1];
   ctx->stats.shadow_rays = counters[2];
@@ -556,6 +625,46 @@ int tc_render(tc_context* ctx, const tc_gpu_render_params* p, const tc_render_op
   if (counters[0] != uint64_t(npix) * p->samples)
     return fail(ctx, TC_ERR_DEVICE_STATUS, "path kernel completed " + std::to_string(counters[0]) + " of " +
                                                 std::to_string(uint64_t(npix) * p->samples) + " paths");
+  return TC_OK;
+}
+
+int tc_render_no_alloc(tc_context* ctx, const tc_gpu_render_params* p, double* sums, size_t n_doubles, void* stream) {
+  if (!ctx) return fail(nullptr, TC_ERR_INVALID, "context is null");
+  if (!p || !sums) return fail(ctx, TC_ERR_INVALID, "render params or sums buffer is null");
+  if (!ctx->has_scene) return fail(ctx, TC_ERR_STATE, "tc_render_no_alloc before tc_upload_scene");
+  if (p->width == 0 || p->height == 0) return fail(ctx, TC_ERR_INVALID, "render dimensions must be nonzero");
+  if (p->samples == 0) return fail(ctx, TC_ERR_INVALID, "sample batch must be greater than zero");
+  const uint64_t npix = uint64_t(p->width) * p->height;
+  if (npix > (1ull << 31)) return fail(ctx, TC_ERR_INVALID, "image is too large: at most 2^31 pixels");
+  if (n_doubles < 3 * npix)
+    return fail(ctx, TC_ERR_INVALID, "sums buffer holds " + std::to_string(n_doubles) + " doubles; " +
+                                         std::to_string(3 * npix) + " (3 per pixel) are needed");
+  TC_CUDA(ctx, cudaSetDevice(ctx->device));
+  unsigned long long* scratch = nullptr;
+  TC_CUDA(ctx, tcb::render_static_scratch(ctx->device, &scratch));
+  static_assert(tcb::kStaticScratchWords >= 4, "the render scratch needs 4 words");
+  cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : ctx->stream;
+  if (p->accumulated_samples == 0) TC_CUDA(ctx, cudaMemsetAsync(sums, 0, sizeof(double) * 3 * npix, st));
+  TC_CUDA(ctx, cudaMemsetAsync(scratch, 0, 4 * sizeof(unsigned long long), st));
+  tcb::RenderLaunch L{};
+  L.scene = ctx->scene;
+  L.width = p->width;
+  L.height = p->height;
+  L.samples = p->samples;
+  L.max_bounces = p->max_bounces;
+  L.frame_index = p->frame_index;
+  L.sample_base = p->accumulated_samples;
+  L.samples_per_item = 1u;
+  L.items_per_pixel = (p->samples + L.samples_per_item - 1) / L.samples_per_item;
+  L.total_items = npix * L.items_per_pixel;
+  L.accum = sums;
+  L.accum_sq = nullptr;
+  L.work_counter = scratch;
+  L.counters = scratch + 1;
+  const int block = 128;
+  const int per_sm = tcb::render_max_blocks_per_sm(block, false);
+  if (per_sm <= 0) return fail(ctx, TC_ERR_CUDA, "render kernel cannot be resident with this block size");
+  TC_CUDA(ctx, tcb::launch_render(L, block, per_sm * ctx->sm_count, false, st));
   return TC_OK;
 }
 
@@ -811,6 +920,55 @@ int tc_guide_train(tc_context* ctx, const float* samples, size_t n, uint32_t ste
   cudaEventElapsedTime(&ctx->stats.kernel_ms, ctx->ev_kernel0, ctx->ev_kernel1);
   if (rc != TC_OK) return rc;
   if (losses) std::memcpy(losses, step_loss.data(), sizeof(float) * steps);
+  return TC_OK;
+}
+
+int tc_guide_train_recorded(tc_context* ctx, uint32_t steps, uint32_t batch, float lr, uint64_t seed, float* losses,
+                            uint32_t* n_samples) {
+  if (!ctx) return fail(nullptr, TC_ERR_INVALID, "context is null");
+  if (!ctx->has_guide) return fail(ctx, TC_ERR_STATE, "guiding parameters were never set");
+  if (!ctx->has_records) return fail(ctx, TC_ERR_STATE, "no batch was rendered with guide_record = 1");
+  if (batch == 0) return fail(ctx, TC_ERR_INVALID, "batch must be positive");
+  TC_CUDA(ctx, cudaSetDevice(ctx->device));
+  cudaStream_t st = ctx->stream;
+  TC_CUDA(ctx, ctx->rec_samples.reserve(sizeof(float4) * 3 * size_t(ctx->rec_capacity)));
+  TC_CUDA(ctx, ctx->rec_wsum.reserve(sizeof(float)));
+  TC_CUDA(ctx, cudaMemsetAsync(ctx->rec_wsum.ptr, 0, sizeof(float), st));
+  TC_CUDA(ctx, cudaEventRecord(ctx->ev_kernel0, st));
+  TC_CUDA(ctx, tcb::launch_guide_samples(ctx->rec_records.as<float4>(), ctx->rec_count.as<uint32_t>(), ctx->rec_capacity,
+                                         ctx->rec_path_rad.as<float4>(), ctx->rec_samples.as<float4>(),
+                                         ctx->rec_wsum.as<float>(), st));
+  uint32_t count = 0;
+  float wsum = 0.0f;
+  TC_CUDA(ctx, cudaMemcpyAsync(&count, ctx->rec_count.ptr, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+  TC_CUDA(ctx, cudaMemcpyAsync(&wsum, ctx->rec_wsum.ptr, sizeof(float), cudaMemcpyDeviceToHost, st));
+  TC_CUDA(ctx, cudaStreamSynchronize(st));
+  count = std::min(count, ctx->rec_capacity);
+  if (n_samples) *n_samples = count;
+  if (count == 0 || !(wsum > 0.0f)) return fail(ctx, TC_ERR_STATE, "the recorded batch carries no radiance to learn from");
+  const float mean = wsum / float(count);
+  const uint32_t b = std::min(batch, count);
+  TC_CUDA(ctx, ctx->g_out.reserve(sizeof(float) * std::max<uint32_t>(steps, 1)));
+  uint64_t x = seed;
+  for (uint32_t s = 0; s < steps; ++s) {
+    x += 0x9E3779B97F4A7C15ull;
+    uint64_t z = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    const uint32_t gather = uint32_t(z ^ (z >> 31)) | 1u;
+    TC_CUDA(ctx, tcb::guide_launch_loss_grad(ctx->guide, ctx->rec_samples.as<float4>(), b, 1.0f / float(b),
+                                             ctx->sm_count, st, 1.0f / mean, 50.0f, gather, count));
+    TC_CUDA(ctx, cudaMemcpyAsync(ctx->g_out.as<float>() + s, ctx->guide.grad + tcb::kGuideParams, sizeof(float),
+                                 cudaMemcpyDeviceToDevice, st));
+    TC_CUDA(ctx, cudaMemsetAsync(ctx->guide.grad + tcb::kGuideParams, 0, sizeof(float), st));
+    TC_CUDA(ctx, tcb::guide_launch_adam(ctx->guide, lr, st));
+  }
+  TC_CUDA(ctx, cudaEventRecord(ctx->ev_kernel1, st));
+  std::vector<float> step_loss(steps);
+  if (steps) TC_CUDA(ctx, cudaMemcpyAsync(step_loss.data(), ctx->g_out.ptr, sizeof(float) * steps, cudaMemcpyDeviceToHost, st));
+  int rc = guide_check_status(ctx);
+  cudaEventElapsedTime(&ctx->stats.kernel_ms, ctx->ev_kernel0, ctx->ev_kernel1);
+  if (rc != TC_OK) return rc;
+  if (losses && steps) std::memcpy(losses, step_loss.data(), sizeof(float) * steps);
   return TC_OK;
 }
 

@@ -35,6 +35,31 @@ struct DevScene {
   float cam_origin[3], cam_lower_left[3], cam_horizontal[3], cam_vertical[3];
 };
 
+// Training-data recording and guided wavefront rounds (render modes kRecord / kGuided).
+struct GuideLaunch {
+  // Recording: one 4-float4 record per diffuse scatter (position + path id, normal + T'.x,
+  // direction + T'.y, radiance so far + T'.z) and the final radiance of every path.
+  float4* records;
+  uint32_t* record_count;
+  uint32_t record_capacity;
+  float4* path_radiance;
+  // Guided rounds: paths suspended at a diffuse vertex (6 float4 each) with their decoded
+  // mixtures (10 float4 each); this round's suspensions go to out_state / out_query.
+  const float4* in_state;
+  const uint32_t* in_count;
+  const float4* in_mix;
+  float4* out_state;
+  float4* out_query;
+  uint32_t* out_count;
+  uint32_t capacity;
+  uint32_t resume;         // 0: start the wave's camera paths, 1: resume in_state
+  uint32_t wave_first_sample;
+  uint32_t wave_spp;
+};
+
+// Path kernel modes.
+enum RenderMode : int { kModePlain = 0, kModeRecord = 1, kModeGuided = 2 };
+
 struct RenderLaunch {
   DevScene scene;
   uint32_t width, height, samples, max_bounces;
@@ -47,13 +72,24 @@ struct RenderLaunch {
   double* accum_sq;            // 3 doubles per pixel or null
   unsigned long long* work_counter;
   unsigned long long* counters;  // [0] paths, [1] extension rays, [2] shadow rays
+  GuideLaunch g;
 };
 
 // Launchers implemented in kernels.cu. All enqueue on `stream` and return the launch error.
 cudaError_t launch_trace_closest(const DevScene& s, const float* rays, uint64_t n, float tmin, uint32_t* prim,
                                  float* t, cudaStream_t stream);
-cudaError_t launch_render(const RenderLaunch& r, int block_size, int grid_size, bool moments, cudaStream_t stream);
-int render_max_blocks_per_sm(int block_size, bool moments);
+cudaError_t launch_render(const RenderLaunch& r, int block_size, int grid_size, bool moments, cudaStream_t stream,
+                          int mode = kModePlain);
+int render_max_blocks_per_sm(int block_size, bool moments, int mode = kModePlain);
+// Training samples (3 float4 each: position + weight, normal, direction) from recorded diffuse
+// scatters: weight = luminance of the radiance that arrived along the scattered direction.
+cudaError_t launch_guide_samples(const float4* records, const uint32_t* record_count, uint32_t capacity,
+                                 const float4* path_radiance, float4* samples, float* weight_sum,
+                                 cudaStream_t stream);
+// Device address of the library's static render scratch (kStaticScratchWords 64-bit words) on
+// `device`, which must be the current device; looked up once per device.
+constexpr int kStaticScratchWords = 32;
+cudaError_t render_static_scratch(int device, unsigned long long** out);
 cudaError_t launch_resolve(const double* accum, uint32_t pixels, double inv_samples, float4* out,
                            cudaStream_t stream);
 // Environment importance tables from RGB texels; `row_sums` is FP64 scratch of H entries.

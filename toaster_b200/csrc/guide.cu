@@ -192,7 +192,8 @@ constexpr int kInferSmem = int(kImgFwdBytes) + 128 * 80 * 2 + 224 * 4;
 __global__ void __launch_bounds__(128, 1) guide_infer_kernel(const float4* __restrict__ queries, uint32_t n,
                                                              const uint8_t* __restrict__ img,
                                                              const float* __restrict__ biases, GuideBounds bounds,
-                                                             float4* __restrict__ out, int* status) {
+                                                             float4* __restrict__ out, int* status,
+                                                             const uint32_t* __restrict__ n_dev) {
   extern __shared__ __align__(1024) uint8_t smem[];
   uint8_t* s_w = smem;
   uint8_t* s_a = smem + kImgFwdBytes;
@@ -210,6 +211,7 @@ __global__ void __launch_bounds__(128, 1) guide_infer_kernel(const float4* __res
   const uint32_t lane_tmem = tmem + (uint32_t(warp * 32) << 16);
   uint32_t phase = 0;
   bool ok = true;
+  if (n_dev) n = min(*n_dev, n);
   const uint32_t tiles = (n + 127) / 128;
   for (uint32_t t = blockIdx.x; t < tiles && ok; t += gridDim.x) {
     const uint32_t q = t * 128 + tid;
@@ -261,13 +263,14 @@ __global__ void __launch_bounds__(128, 1) guide_infer_kernel(const float4* __res
 }
 
 cudaError_t guide_launch_infer(const GuideDevice& g, const float4* queries, uint32_t n, float4* out, int sm_count,
-                               cudaStream_t stream) {
+                               cudaStream_t stream, const uint32_t* n_dev) {
   if (n == 0) return cudaSuccess;
   cudaError_t e = cudaFuncSetAttribute(guide_infer_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kInferSmem);
   if (e != cudaSuccess) return e;
   const uint32_t tiles = (n + 127) / 128;
   const int grid = int(tiles < uint32_t(4 * sm_count) ? tiles : uint32_t(4 * sm_count));
-  guide_infer_kernel<<<grid, 128, kInferSmem, stream>>>(queries, n, g.images, g.biases, g.bounds, out, g.status);
+  guide_infer_kernel<<<grid, 128, kInferSmem, stream>>>(queries, n, g.images, g.biases, g.bounds, out, g.status,
+                                                         n_dev);
   return cudaGetLastError();
 }
 
@@ -364,7 +367,9 @@ __device__ __forceinline__ void epilogue_backward(uint32_t lane_tmem, const uint
 __global__ void __launch_bounds__(128, 1) guide_train_kernel(const float4* __restrict__ samples, uint32_t n,
                                                              const uint8_t* __restrict__ img,
                                                              const float* __restrict__ biases, GuideBounds bounds,
-                                                             float inv_batch, float* __restrict__ grad, int* status) {
+                                                             float inv_batch, float* __restrict__ grad, int* status,
+                                                             float w_scale, float w_clamp, uint32_t gather_seed,
+                                                             uint32_t n_total) {
   extern __shared__ __align__(1024) uint8_t smem[];
   uint8_t* s_w = smem;
   uint8_t* s_x = smem + kTrainX;
@@ -407,9 +412,16 @@ __global__ void __launch_bounds__(128, 1) guide_train_kernel(const float4* __res
     const bool valid = q < n;
     float4 p = make_float4(0, 0, 0, 0), nn = p, om = p;
     if (valid) {
-      p = samples[3 * size_t(q)];
-      nn = samples[3 * size_t(q) + 1];
-      om = samples[3 * size_t(q) + 2];
+      uint32_t idx = q;
+      if (gather_seed) {  // hashed draw (SplitMix-style finaliser) from the whole sample set
+        uint32_t h = q * 0x9E3779B9u ^ gather_seed;
+        h ^= h >> 16; h *= 0x7FEB352Du; h ^= h >> 15; h *= 0x846CA68Bu; h ^= h >> 16;
+        idx = h % n_total;
+      }
+      p = samples[3 * size_t(idx)];
+      nn = samples[3 * size_t(idx) + 1];
+      om = samples[3 * size_t(idx) + 2];
+      p.w = fminf(p.w * w_scale, w_clamp);
     }
     encode_row(s_x, tid, valid, p.x, p.y, p.z, nn.x, nn.y, nn.z, bounds);
     // Forward.
@@ -538,14 +550,16 @@ __global__ void __launch_bounds__(128, 1) guide_train_kernel(const float4* __res
 }
 
 cudaError_t guide_launch_loss_grad(const GuideDevice& g, const float4* samples, uint32_t n, float inv_batch,
-                                   int sm_count, cudaStream_t stream) {
+                                   int sm_count, cudaStream_t stream, float w_scale, float w_clamp,
+                                   uint32_t gather_seed, uint32_t n_total) {
   if (n == 0) return cudaSuccess;
   cudaError_t e = cudaFuncSetAttribute(guide_train_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kTrainSmem);
   if (e != cudaSuccess) return e;
   const uint32_t tiles = (n + 127) / 128;
   const int grid = int(tiles < uint32_t(sm_count) ? tiles : uint32_t(sm_count));
   guide_train_kernel<<<grid, 128, kTrainSmem, stream>>>(samples, n, g.images, g.biases, g.bounds, inv_batch, g.grad,
-                                                         g.status);
+                                                         g.status, w_scale, w_clamp, gather_seed,
+                                                         n_total ? n_total : n);
   return cudaGetLastError();
 }
 

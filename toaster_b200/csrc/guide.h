@@ -54,15 +54,17 @@ struct GuideDevice {
 
 cudaError_t guide_refresh_images(const GuideDevice& g, cudaStream_t stream);
 // queries: 2 float4 per query (position, normal); out: kGuideDecodedF4 float4 per query.
+// When n_dev is non-null the query count is read from device memory (capped at n).
 cudaError_t guide_launch_infer(const GuideDevice& g, const float4* queries, uint32_t n, float4* out, int sm_count,
-                               cudaStream_t stream);
+                               cudaStream_t stream, const uint32_t* n_dev = nullptr);
 // samples: 3 float4 per sample (position + weight, normal, direction); gradient of the mean
 // weighted NLL accumulated into g.grad[0..kGuideParams), the loss into g.grad[kGuideParams].
+// Sample weights are scaled by w_scale and clamped at w_clamp. With gather_seed != 0 the n
+// samples of the batch are drawn (hashed indices) from the first n_total samples.
 cudaError_t guide_launch_loss_grad(const GuideDevice& g, const float4* samples, uint32_t n, float inv_batch,
-                                   int sm_count, cudaStream_t stream);
+                                   int sm_count, cudaStream_t stream, float w_scale = 1.0f,
+                                   float w_clamp = 3.0e38f, uint32_t gather_seed = 0, uint32_t n_total = 0);
 cudaError_t guide_launch_adam(GuideDevice& g, float lr, cudaStream_t stream);
-
-// Device-side mixture evaluation used by the path kernels (defined in guide_mixture.cuh).
 
 }  // namespace tcb
 

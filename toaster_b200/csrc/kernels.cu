@@ -15,6 +15,8 @@
 #include <math_constants.h>
 #include <stdint.h>
 
+#include <mutex>
+
 #include "device_scene.h"
 #include "traverse.cuh"
 
@@ -250,8 +252,64 @@ struct Lane {
   int depth;         // remaining depth (ray_color_inner's remaining_depth)
   bool include_emission;
   uint32_t pixel, item_samples, item_done, sample;
+  int mix_slot;      // guided mode: decoded mixture of the current diffuse vertex, or -1
   Pcg rng;
 };
+
+// ------------------------------------------------------------------------ guiding mixture
+// Decoded 8-lobe von Mises-Fisher mixture: mix[j] = (mu.xyz, kappa), mix[8..9] = weights.
+__device__ __forceinline__ float mix_pdf(const float4* __restrict__ mix, V3 w) {
+  const float4 w0 = __ldg(mix + 8), w1 = __ldg(mix + 9);
+  const float wt[8] = {w0.x, w0.y, w0.z, w0.w, w1.x, w1.y, w1.z, w1.w};
+  float p = 0.0f;
+#pragma unroll
+  for (int j = 0; j < 8; ++j) {
+    const float4 m = __ldg(mix + j);
+    const float c = m.x * w.x + m.y * w.y + m.z * w.z;
+    const float norm = m.w / (2.0f * kPiF * -expm1f(-2.0f * m.w));
+    p += wt[j] * norm * __expf(m.w * (c - 1.0f));
+  }
+  return p;
+}
+
+// Lobe chosen by its weight with u1; direction from the vMF inverse CDF (cosine to the mean
+// W = 1 + log(u2 + (1 - u2) e^{-2 kappa}) / kappa, azimuth 2 pi u3) in an orthonormal frame.
+__device__ __forceinline__ V3 mix_sample(const float4* __restrict__ mix, float u1, float u2, float u3) {
+  const float4 w0 = __ldg(mix + 8), w1 = __ldg(mix + 9);
+  const float wt[8] = {w0.x, w0.y, w0.z, w0.w, w1.x, w1.y, w1.z, w1.w};
+  int j = 7;
+  float acc = 0.0f;
+#pragma unroll
+  for (int k = 0; k < 7; ++k) {
+    acc += wt[k];
+    if (u1 < acc) { j = k; break; }
+  }
+  const float4 m = __ldg(mix + j);
+  const float kappa = m.w;
+  float W = 1.0f + __logf(u2 + (1.0f - u2) * __expf(-2.0f * kappa)) / kappa;
+  W = fminf(fmaxf(W, -1.0f), 1.0f);
+  const float r = sqrtf(fmaxf(0.0f, 1.0f - W * W));
+  float sp, cp;
+  sincospif(2.0f * u3, &sp, &cp);
+  // Branchless orthonormal basis (Duff et al. 2017) around the lobe axis.
+  const float sign = copysignf(1.0f, m.z);
+  const float a = -1.0f / (sign + m.z);
+  const float b = m.x * m.y * a;
+  const V3 t = mk(1.0f + sign * m.x * m.x * a, sign * b, -sign * m.x);
+  const V3 bb = mk(b, sign + m.y * m.y * a, -m.y);
+  return mk(m.x, m.y, m.z) * W + (t * cp + bb * sp) * r;
+}
+
+// One slot of a counter shared by the lanes that reach this call together (one atomic per warp).
+__device__ __forceinline__ uint32_t aggregated_increment(uint32_t* counter) {
+  const unsigned active = __activemask();
+  const int leader = __ffs(active) - 1;
+  const unsigned lane = threadIdx.x & 31u;
+  uint32_t base = 0;
+  if (int(lane) == leader) base = atomicAdd(counter, uint32_t(__popc(active)));
+  base = __shfl_sync(active, base, leader);
+  return base + uint32_t(__popc(active & ((1u << lane) - 1u)));
+}
 
 __device__ __forceinline__ void start_sample(const RenderLaunch& L, Lane& ln) {
   const DevScene& s = L.scene;
@@ -270,11 +328,16 @@ __device__ __forceinline__ void start_sample(const RenderLaunch& L, Lane& ln) {
   ln.depth = int(L.max_bounces);
   ln.include_emission = true;
   ln.bsdf_pdf = -1.0f;
+  ln.mix_slot = -1;
   ln.phase = kExtend;
 }
 
-template <bool kMoments>
+template <int kMode, bool kMoments>
 __device__ __forceinline__ void finish_sample(const RenderLaunch& L, Lane& ln, uint32_t& n_paths) {
+  if constexpr (kMode == kModeRecord) {
+    const uint32_t path = (ln.sample - L.sample_base) * (L.width * L.height) + ln.pixel;
+    L.g.path_radiance[path] = make_float4(ln.rad.x, ln.rad.y, ln.rad.z, 0.0f);
+  }
   ln.acc = ln.acc + ln.rad;
   if (kMoments) ln.acc2 = ln.acc2 + ln.rad * ln.rad;
   ++n_paths;
@@ -334,8 +397,11 @@ __device__ __forceinline__ bool prepare_light_shadow(const DevScene& s, Lane& ln
   return true;
 }
 
-// Environment-sampling shadow ray with the power heuristic (integrator.rs:208-244).
-__device__ __forceinline__ bool prepare_env_shadow(const DevScene& s, Lane& ln) {
+// Environment-sampling shadow ray with the power heuristic (integrator.rs:208-244). At a guided
+// vertex the competing technique is the 50/50 BSDF / guide mixture, so its pdf enters the weight.
+template <int kMode>
+__device__ __forceinline__ bool prepare_env_shadow(const RenderLaunch& L, Lane& ln) {
+  const DevScene& s = L.scene;
   if (s.background != 2u || !s.env_sampleable) return false;
   const float u1 = ln.rng.uniform(), u2 = ln.rng.uniform(), u3 = ln.rng.uniform();
   V3 dir, rad;
@@ -343,7 +409,11 @@ __device__ __forceinline__ bool prepare_env_shadow(const DevScene& s, Lane& ln) 
   if (!env_sample(s, u1, u2, u3, dir, rad, pdf)) return false;
   const float cs = fmaxf(dot(ln.hn, dir), 0.0f);
   if (cs <= 0.0f || pdf <= 0.0f) return false;
-  const float mis = power_heuristic(pdf, cs / kPiF);
+  float indirect_pdf = cs / kPiF;
+  if constexpr (kMode == kModeGuided) {
+    if (ln.mix_slot >= 0) indirect_pdf = 0.5f * indirect_pdf + 0.5f * mix_pdf(L.g.in_mix + 10 * size_t(ln.mix_slot), dir);
+  }
+  const float mis = power_heuristic(pdf, indirect_pdf);
   ln.pend = ln.thr * ln.alb * rad * (cs * mis / (kPiF * pdf));
   ln.ro = ln.hp + ln.hn * kRayEps;
   ln.rd = dir;
@@ -362,7 +432,46 @@ __device__ __forceinline__ V3 background(const DevScene& s, V3 d, float bsdf_pdf
   return r * w;
 }
 
-template <bool kMoments>
+// Writes a path suspended at a diffuse vertex (guided mode) and the query for its mixture.
+__device__ __forceinline__ void suspend_path(const RenderLaunch& L, const Lane& ln) {
+  const uint32_t slot = aggregated_increment(L.g.out_count);
+  if (slot >= L.g.capacity) return;  // cannot happen: capacity covers every path of the wave
+  float4* st = L.g.out_state + 6 * size_t(slot);
+  st[0] = make_float4(ln.hp.x, ln.hp.y, ln.hp.z, ln.hn.x);
+  st[1] = make_float4(ln.hn.y, ln.hn.z, ln.alb.x, ln.alb.y);
+  st[2] = make_float4(ln.alb.z, ln.thr.x, ln.thr.y, ln.thr.z);
+  st[3] = make_float4(ln.rad.x, ln.rad.y, ln.rad.z, __int_as_float(ln.depth));
+  st[4] = make_float4(__uint_as_float(ln.pixel), __uint_as_float(uint32_t(ln.rng.state)),
+                      __uint_as_float(uint32_t(ln.rng.state >> 32)), __uint_as_float(uint32_t(ln.rng.inc)));
+  st[5] = make_float4(__uint_as_float(uint32_t(ln.rng.inc >> 32)), 0.0f, 0.0f, 0.0f);
+  float4* q = L.g.out_query + 2 * size_t(slot);
+  q[0] = make_float4(ln.hp.x, ln.hp.y, ln.hp.z, 0.0f);
+  q[1] = make_float4(ln.hn.x, ln.hn.y, ln.hn.z, 0.0f);
+}
+
+__device__ __forceinline__ void resume_path(const RenderLaunch& L, Lane& ln, uint32_t slot) {
+  const float4* st = L.g.in_state + 6 * size_t(slot);
+  const float4 a = st[0], b = st[1], c = st[2], d = st[3], e = st[4], f = st[5];
+  ln.hp = mk(a.x, a.y, a.z);
+  ln.hn = mk(a.w, b.x, b.y);
+  ln.alb = mk(b.z, b.w, c.x);
+  ln.thr = mk(c.y, c.z, c.w);
+  ln.rad = mk(d.x, d.y, d.z);
+  ln.depth = __float_as_int(d.w);
+  ln.pixel = __float_as_uint(e.x);
+  ln.rng.state = uint64_t(__float_as_uint(e.y)) | (uint64_t(__float_as_uint(e.z)) << 32);
+  ln.rng.inc = uint64_t(__float_as_uint(e.w)) | (uint64_t(__float_as_uint(f.x)) << 32);
+  ln.include_emission = false;
+  ln.bsdf_pdf = -1.0f;
+  ln.mix_slot = int(slot);
+  ln.item_samples = 1;
+  ln.item_done = 0;
+  ln.acc = mk(0.f, 0.f, 0.f);
+  ln.acc2 = mk(0.f, 0.f, 0.f);
+  ln.phase = kShadowLight;
+}
+
+template <int kMode, bool kMoments>
 __device__ __forceinline__ void shade_hit(const RenderLaunch& L, Lane& ln, const TraceResult& tr, uint32_t& n_paths) {
   const DevScene& s = L.scene;
   const float4* p = reinterpret_cast<const float4*>(s.prims + tr.rec);
@@ -411,14 +520,22 @@ __device__ __forceinline__ void shade_hit(const RenderLaunch& L, Lane& ln, const
   const DevMaterial m = s.materials[mat];
   if (m.kind == kEmissive) {
     if (ln.include_emission) ln.rad = ln.rad + ln.thr * mk(m.emission[0], m.emission[1], m.emission[2]);
-    finish_sample<kMoments>(L, ln, n_paths);
+    finish_sample<kMode, kMoments>(L, ln, n_paths);
     return;
   }
   if (m.kind == kDiffuse) {
     ln.hp = hp;
     ln.hn = nrm;
     ln.alb = base_color(s, m, tu, tv);
+    ln.mix_slot = -1;
     ln.phase = kShadowLight;
+    if constexpr (kMode == kModeGuided) {
+      // A vertex that will scatter waits for the network's mixture; the last vertex only does NEE.
+      if (ln.depth > 1) {
+        suspend_path(L, ln);
+        ln.phase = kIdle;
+      }
+    }
     return;
   }
   if (m.kind == kMetal) {
@@ -426,7 +543,7 @@ __device__ __forceinline__ void shade_hit(const RenderLaunch& L, Lane& ln, const
     const V3 ball = uniform_ball(ln.rng.uniform(), ln.rng.uniform(), ln.rng.uniform());
     const V3 dir = refl + ball * m.roughness;
     if (dot(dir, nrm) <= 0.0f) {
-      finish_sample<kMoments>(L, ln, n_paths);
+      finish_sample<kMode, kMoments>(L, ln, n_paths);
       return;
     }
     ln.ro = hp;
@@ -450,16 +567,21 @@ __device__ __forceinline__ void shade_hit(const RenderLaunch& L, Lane& ln, const
   ln.phase = kExtend;
 }
 
-template <bool kMoments>
+template <int kMode, bool kMoments>
 __global__ void __launch_bounds__(256) render_kernel(const RenderLaunch L) {
   const DevScene& s = L.scene;
   const unsigned lane = threadIdx.x & 31u;
   const uint32_t npix = L.width * L.height;
   Lane ln;
   ln.phase = kIdle;
+  ln.mix_slot = -1;
   ln.acc = ln.acc2 = mk(0.f, 0.f, 0.f);
   bool finished = false;
   uint32_t n_paths = 0, n_ext = 0, n_shadow = 0, node_visits = 0;
+  uint64_t total_items = L.total_items;
+  if constexpr (kMode == kModeGuided) {
+    if (L.g.resume) total_items = *L.g.in_count < L.g.capacity ? *L.g.in_count : L.g.capacity;
+  }
 
   for (;;) {
     // Refill idle lanes: one atomic per warp for all of them.
@@ -472,8 +594,20 @@ __global__ void __launch_bounds__(256) render_kernel(const RenderLaunch L) {
       base = __shfl_sync(0xffffffffu, base, leader);
       if (want) {
         const uint64_t item = base + __popc(want_mask & ((1u << lane) - 1u));
-        if (item >= L.total_items) {
+        if (item >= total_items) {
           finished = true;
+        } else if (kMode == kModeGuided && L.g.resume) {
+          resume_path(L, ln, uint32_t(item));
+        } else if (kMode == kModeGuided) {
+          // One path per item: pixel-major within each sample of the wave.
+          const uint32_t k = uint32_t(item / npix);
+          ln.pixel = uint32_t(item - uint64_t(k) * npix);
+          ln.item_samples = 1;
+          ln.item_done = 0;
+          ln.sample = L.g.wave_first_sample + k;
+          ln.acc = mk(0.f, 0.f, 0.f);
+          if (kMoments) ln.acc2 = mk(0.f, 0.f, 0.f);
+          start_sample(L, ln);
         } else {
           const uint32_t chunk = uint32_t(item / npix);
           ln.pixel = uint32_t(item - uint64_t(chunk) * npix);
@@ -496,7 +630,7 @@ __global__ void __launch_bounds__(256) render_kernel(const RenderLaunch L) {
       switch (ln.phase) {
         case kExtend:
           if (ln.depth <= 0) {
-            finish_sample<kMoments>(L, ln, n_paths);
+            finish_sample<kMode, kMoments>(L, ln, n_paths);
           } else {
             have = true;
             any_hit = false;
@@ -508,18 +642,61 @@ __global__ void __launch_bounds__(256) render_kernel(const RenderLaunch L) {
           else ln.phase = kShadowEnv;
           break;
         case kShadowEnv:
-          if (prepare_env_shadow(s, ln)) { have = true; any_hit = true; }
+          if (prepare_env_shadow<kMode>(L, ln)) { have = true; any_hit = true; }
           else ln.phase = kScatter;
           break;
         default: {  // kScatter: cosine-weighted diffuse bounce (integrator.rs:277-289)
           ln.depth -= 1;
           if (ln.depth <= 0) {
-            finish_sample<kMoments>(L, ln, n_paths);
+            finish_sample<kMode, kMoments>(L, ln, n_paths);
             break;
+          }
+          if constexpr (kMode == kModeGuided) {
+            if (ln.mix_slot >= 0) {
+              // One-sample MIS of BSDF and guide sampling (the balance heuristic = the 50/50
+              // mixture pdf), so the estimator stays unbiased whatever the network predicts.
+              const float4* mix = L.g.in_mix + 10 * size_t(ln.mix_slot);
+              const float ut = ln.rng.uniform();
+              V3 dir;
+              if (ut < 0.5f) {
+                dir = ln.hn + uniform_sphere(ln.rng.uniform(), ln.rng.uniform());
+                if (dot(dir, dir) < 1e-8f) dir = ln.hn;
+                dir = normalize(dir);
+              } else {
+                const float a = ln.rng.uniform(), b = ln.rng.uniform(), c = ln.rng.uniform();
+                dir = mix_sample(mix, a, b, c);
+              }
+              const float cs = dot(ln.hn, dir);
+              ln.mix_slot = -1;
+              if (!(cs > 0.0f)) {
+                finish_sample<kMode, kMoments>(L, ln, n_paths);
+                break;
+              }
+              const float p = 0.5f * cs / kPiF + 0.5f * mix_pdf(mix, dir);
+              ln.ro = ln.hp;
+              ln.rd = dir;
+              ln.thr = ln.thr * ln.alb * (cs / (kPiF * p));
+              ln.include_emission = false;
+              ln.bsdf_pdf = p;
+              ln.phase = kExtend;
+              break;
+            }
           }
           V3 dir = ln.hn + uniform_sphere(ln.rng.uniform(), ln.rng.uniform());
           if (dot(dir, dir) < 1e-8f) dir = ln.hn;
           dir = normalize(dir);
+          if constexpr (kMode == kModeRecord) {
+            const uint32_t slot = aggregated_increment(L.g.record_count);
+            if (slot < L.g.record_capacity) {
+              const uint32_t path = (ln.sample - L.sample_base) * npix + ln.pixel;
+              const V3 t = ln.thr * ln.alb;
+              float4* r = L.g.records + 4 * size_t(slot);
+              r[0] = make_float4(ln.hp.x, ln.hp.y, ln.hp.z, __uint_as_float(path));
+              r[1] = make_float4(ln.hn.x, ln.hn.y, ln.hn.z, t.x);
+              r[2] = make_float4(dir.x, dir.y, dir.z, t.y);
+              r[3] = make_float4(ln.rad.x, ln.rad.y, ln.rad.z, t.z);
+            }
+          }
           ln.ro = ln.hp;
           ln.rd = dir;
           ln.thr = ln.thr * ln.alb;
@@ -548,9 +725,9 @@ __global__ void __launch_bounds__(256) render_kernel(const RenderLaunch L) {
         ++n_ext;
         if (!hit) {
           ln.rad = ln.rad + ln.thr * background(s, ln.rd, ln.bsdf_pdf);
-          finish_sample<kMoments>(L, ln, n_paths);
+          finish_sample<kMode, kMoments>(L, ln, n_paths);
         } else {
-          shade_hit<kMoments>(L, ln, tr, n_paths);
+          shade_hit<kMode, kMoments>(L, ln, tr, n_paths);
         }
       }
     }
@@ -567,18 +744,97 @@ __global__ void __launch_bounds__(256) render_kernel(const RenderLaunch L) {
   }
 }
 
-cudaError_t launch_render(const RenderLaunch& r, int block_size, int grid_size, bool moments, cudaStream_t stream) {
-  if (moments) render_kernel<true><<<grid_size, block_size, 0, stream>>>(r);
-  else render_kernel<false><<<grid_size, block_size, 0, stream>>>(r);
+template <int kMode>
+static cudaError_t launch_mode(const RenderLaunch& r, int block_size, int grid_size, bool moments, cudaStream_t stream) {
+  if (moments) render_kernel<kMode, true><<<grid_size, block_size, 0, stream>>>(r);
+  else render_kernel<kMode, false><<<grid_size, block_size, 0, stream>>>(r);
   return cudaGetLastError();
 }
 
-int render_max_blocks_per_sm(int block_size, bool moments) {
+cudaError_t launch_render(const RenderLaunch& r, int block_size, int grid_size, bool moments, cudaStream_t stream,
+                          int mode) {
+  if (mode == kModeRecord) return launch_mode<kModeRecord>(r, block_size, grid_size, moments, stream);
+  if (mode == kModeGuided) return launch_mode<kModeGuided>(r, block_size, grid_size, moments, stream);
+  return launch_mode<kModePlain>(r, block_size, grid_size, moments, stream);
+}
+
+template <int kMode>
+static int blocks_for(int block_size, bool moments) {
   int blocks = 0;
   cudaError_t e = moments
-      ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, render_kernel<true>, block_size, 0)
-      : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, render_kernel<false>, block_size, 0);
+      ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, render_kernel<kMode, true>, block_size, 0)
+      : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, render_kernel<kMode, false>, block_size, 0);
   return e == cudaSuccess ? blocks : 0;
+}
+
+int render_max_blocks_per_sm(int block_size, bool moments, int mode) {
+  if (mode == kModeRecord) return blocks_for<kModeRecord>(block_size, moments);
+  if (mode == kModeGuided) return blocks_for<kModeGuided>(block_size, moments);
+  return blocks_for<kModePlain>(block_size, moments);
+}
+
+// ------------------------------------------------------------------------ training samples
+__global__ void guide_samples_kernel(const float4* __restrict__ rec, const uint32_t* __restrict__ count,
+                                     uint32_t capacity, const float4* __restrict__ path_rad,
+                                     float4* __restrict__ out, float* __restrict__ weight_sum) {
+  const uint32_t n = min(*count, capacity);
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  float w = 0.0f;
+  if (i < n) {
+    const float4 a = rec[4 * size_t(i)], b = rec[4 * size_t(i) + 1], c = rec[4 * size_t(i) + 2],
+                 d = rec[4 * size_t(i) + 3];
+    const float4 end = path_rad[__float_as_uint(a.w)];
+    // Radiance that arrived along the scattered direction: what the path gathered after this
+    // vertex, divided by the throughput it had just after scattering.
+    const float lx = b.w > 0.0f ? fmaxf(end.x - d.x, 0.0f) / b.w : 0.0f;
+    const float ly = c.w > 0.0f ? fmaxf(end.y - d.y, 0.0f) / c.w : 0.0f;
+    const float lz = d.w > 0.0f ? fmaxf(end.z - d.z, 0.0f) / d.w : 0.0f;
+    w = 0.2126f * lx + 0.7152f * ly + 0.0722f * lz;
+    if (!isfinite(w)) w = 0.0f;
+    out[3 * size_t(i)] = make_float4(a.x, a.y, a.z, w);
+    out[3 * size_t(i) + 1] = make_float4(b.x, b.y, b.z, 0.0f);
+    out[3 * size_t(i) + 2] = make_float4(c.x, c.y, c.z, 0.0f);
+  }
+  for (int o = 16; o > 0; o >>= 1) w += __shfl_down_sync(0xffffffffu, w, o);
+  if ((threadIdx.x & 31u) == 0 && w != 0.0f) atomicAdd(weight_sum, w);
+}
+
+cudaError_t launch_guide_samples(const float4* records, const uint32_t* record_count, uint32_t capacity,
+                                 const float4* path_radiance, float4* samples, float* weight_sum,
+                                 cudaStream_t stream) {
+  if (capacity == 0) return cudaSuccess;
+  guide_samples_kernel<<<(capacity + 255) / 256, 256, 0, stream>>>(records, record_count, capacity, path_radiance,
+                                                                   samples, weight_sum);
+  return cudaGetLastError();
+}
+
+// ------------------------------------------------------------------------ scratch without allocation
+// Scratch of tc_render_no_alloc: [0] the work-queue counter, [1..3] the path, extension-ray and
+// shadow-ray counters. Every GPU that loads the library holds these 256 bytes until exit; all
+// calls share them, so the entry point clears them at the start of each call, and calls whose
+// kernels overlap on the GPU race on them.
+static __device__ __align__(256) unsigned long long g_render_scratch[kStaticScratchWords];
+
+cudaError_t render_static_scratch(int device, unsigned long long** out) {
+  // The symbol's device address is looked up once per device, with that device current (host
+  // code must never hand the array's name itself to a kernel: it is only a host-side stand-in).
+  constexpr int kMaxDevices = 64;
+  static std::mutex lock;
+  static unsigned long long* cache[kMaxDevices] = {};
+  if (device < 0 || device >= kMaxDevices) return cudaErrorInvalidDevice;
+  std::lock_guard<std::mutex> guard(lock);
+  if (!cache[device]) {
+    int current = 0;
+    cudaError_t e = cudaGetDevice(&current);
+    if (e != cudaSuccess) return e;
+    if (current != device) return cudaErrorInvalidDevice;
+    void* ptr = nullptr;
+    e = cudaGetSymbolAddress(&ptr, g_render_scratch);
+    if (e != cudaSuccess) return e;
+    cache[device] = static_cast<unsigned long long*>(ptr);
+  }
+  *out = cache[device];
+  return cudaSuccess;
 }
 
 // ------------------------------------------------------------------------ resolve

@@ -1,0 +1,161 @@
+"""Equal-time comparison of guided and plain path tracing.
+
+    python -m toaster_b200.guiding_eval [--width W --height H --ref-spp N --plain-spp 256]
+
+Protocol:
+- A converged reference is rendered with plain sampling and FP64 accumulation.
+- Plain sampling accumulates batches of `batch` spp up to `plain_spp`. After each batch the GPU time
+  so far and the RGB RMSE against the reference are recorded.
+- Guided sampling starts with `record_spp` plain spp that also record training samples at every
+  diffuse scatter (these samples stay in the image). It then trains the network on the GPU with
+  Adam, and accumulates guided batches. Training time counts toward the guided timeline.
+- The result is the guided time needed to reach the plain method's RMSE at `plain_spp`, as a
+  fraction of the plain time.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import time
+
+import numpy as np
+
+from . import configs
+from .renderer import GpuRenderer
+from .scene import Scene, scene_to_gpu
+
+def initial_params(seed: int = 0) -> np.ndarray:
+    """He-uniform hidden layers, a 10x smaller output layer, zero biases, zero padded inputs."""
+    rng = np.random.default_rng(seed)
+    shapes = [(64, 80), (64,), (64, 64), (64,), (64, 64), (64,), (32, 64), (32,)]
+    out = []
+    for k, shape in enumerate(shapes):
+        if len(shape) == 1:
+            out.append(np.zeros(shape, np.float32))
+            continue
+        fan_in = 75 if k == 0 else shape[1]
+        bound = np.sqrt(6.0 / fan_in) * (0.1 if k == 6 else 1.0)
+        w = rng.uniform(-bound, bound, shape).astype(np.float32)
+        if k == 0:
+            w[:, 75:] = 0.0
+        out.append(w)
+    return np.concatenate([a.reshape(-1) for a in out])
+
+
+def _image(r: GpuRenderer) -> np.ndarray:
+    s, _, n = r.readback_sums()
+    return s / n
+
+
+def reference_image(scene: Scene, spp: int, batch: int = 256, device: int = 0) -> np.ndarray:
+    with GpuRenderer(device) as r:
+        r.upload(scene_to_gpu(scene))
+        done = 0
+        while done < spp:
+            n = min(batch, spp - done)
+            r.render(samples=n, frame_index=1_000_000 + done, accumulate=done > 0)
+            done += n
+        return _image(r)
+
+
+def rmse(a: np.ndarray, b: np.ndarray) -> float:
+    return float(np.sqrt(np.mean((a - b) ** 2)))
+
+
+def timeline_plain(scene: Scene, reference: np.ndarray, total_spp: int, batch: int, device: int = 0):
+    points = []
+    with GpuRenderer(device) as r:
+        r.upload(scene_to_gpu(scene))
+        t = 0.0
+        done = 0
+        while done < total_spp:
+            n = min(batch, total_spp - done)
+            r.render(samples=n, frame_index=done, accumulate=done > 0)
+            t += r.stats()["total_ms"] * 1e-3
+            done += n
+            points.append((t, done, rmse(_image(r), reference)))
+    return points
+
+
+def timeline_guided(scene: Scene, reference: np.ndarray, total_spp: int, batch: int, record_spp: int,
+                    train_steps: int, train_batch: int, lr: float = 1e-2, seed: int = 0, device: int = 0):
+    points = []
+    info = {}
+    with GpuRenderer(device) as r:
+        r.upload(scene_to_gpu(scene))
+        r.guide_set_params(initial_params(seed), configs.scene_bounds(scene))
+        r.render(samples=record_spp, frame_index=0, guide_record=True)
+        t = r.stats()["total_ms"] * 1e-3
+        points.append((t, record_spp, rmse(_image(r), reference)))
+        t0 = time.perf_counter()
+        losses, n = r.guide_train_recorded(train_steps, train_batch, lr, seed)
+        train_s = r.stats()["kernel_ms"] * 1e-3
+        info.update(train_seconds=train_s, train_host_seconds=time.perf_counter() - t0, samples=n,
+                    loss_first=float(losses[:5].mean()), loss_last=float(losses[-5:].mean()))
+        t += train_s
+        done = record_spp
+        while done < total_spp:
+            m = min(batch, total_spp - done)
+            r.render(samples=m, frame_index=done, accumulate=True, guiding=True)
+            t += r.stats()["total_ms"] * 1e-3
+            done += m
+            points.append((t, done, rmse(_image(r), reference)))
+    return points, info
+
+
+def time_to_reach(points, target: float):
+    """Earliest (interpolated in log RMSE between batches) time at which RMSE <= target, or None."""
+    prev = None
+    for t, spp, e in points:
+        if e <= target:
+            if prev is None or prev[2] <= e:
+                return t
+            t0, _, e0 = prev
+            f = (np.log(e0) - np.log(target)) / (np.log(e0) - np.log(e))
+            return t0 + f * (t - t0)
+        prev = (t, spp, e)
+    return None
+
+
+def equal_time_comparison(scene: Scene, ref_spp: int, plain_spp: int = 256, batch: int = 16, record_spp: int = 16,
+                          guided_spp: int | None = None, train_steps: int = 300, train_batch: int = 8192,
+                          seed: int = 0, device: int = 0) -> dict:
+    reference = reference_image(scene, ref_spp, device=device)
+    plain = timeline_plain(scene, reference, plain_spp, batch, device)
+    guided, info = timeline_guided(scene, reference, guided_spp or plain_spp, batch, record_spp, train_steps,
+                                   train_batch, seed=seed, device=device)
+    t_plain, _, e_plain = plain[-1]
+    t_guided = time_to_reach(guided, e_plain)
+    e_guided_at_equal_time = None
+    for t, _, e in guided:
+        if t <= t_plain:
+            e_guided_at_equal_time = e
+    return {
+        "width": scene.width, "height": scene.height, "max_bounces": scene.max_bounces, "reference_spp": ref_spp,
+        "plain_spp": plain_spp, "plain_seconds": t_plain, "plain_rmse": e_plain,
+        "guided_seconds_to_plain_rmse": t_guided,
+        "time_fraction": None if t_guided is None else t_guided / t_plain,
+        "guided_rmse_at_plain_time": e_guided_at_equal_time,
+        "plain_timeline": plain, "guided_timeline": guided, **info,
+    }
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--width", type=int, default=320)
+    ap.add_argument("--height", type=int, default=180)
+    ap.add_argument("--ref-spp", type=int, default=65536)
+    ap.add_argument("--plain-spp", type=int, default=256)
+    ap.add_argument("--guided-spp", type=int, default=0)
+    ap.add_argument("--train-steps", type=int, default=300)
+    ap.add_argument("--seed", type=int, default=0)
+    args = ap.parse_args()
+    scene = configs.room_with_window(width=args.width, height=args.height)
+    out = equal_time_comparison(scene, args.ref_spp, args.plain_spp, guided_spp=args.guided_spp or None,
+                                train_steps=args.train_steps, seed=args.seed)
+    print(json.dumps(out))
+
+
+if __name__ == "__main__":
+    main()

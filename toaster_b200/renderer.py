@@ -111,7 +111,8 @@ class GpuRenderer:
 
     def render(self, samples: Optional[int] = None, max_bounces: Optional[int] = None, width: Optional[int] = None,
                height: Optional[int] = None, frame_index: int = 0, accumulate: bool = False,
-               keep_moments: bool = False, block_size: int = 0, samples_per_item: int = 0) -> None:
+               keep_moments: bool = False, block_size: int = 0, samples_per_item: int = 0, guiding: bool = False,
+               guide_record: bool = False) -> None:
         """Traces ``samples`` paths per pixel; ``accumulate`` adds them to the previous batches."""
         if self._params is None:
             raise RuntimeError("render before upload")
@@ -130,6 +131,8 @@ class GpuRenderer:
         opts.block_size = block_size
         opts.samples_per_item = samples_per_item
         opts.keep_moments = 1 if keep_moments else 0
+        opts.guiding = 1 if guiding else 0
+        opts.guide_record = 1 if guide_record else 0
         self._check(self._lib.tc_render(self._ctx, p.ctypes.data, ctypes.byref(opts)))
         self.width, self.height = int(p["width"][0]), int(p["height"][0])
         self.accumulated = (self.accumulated if accumulate else 0) + int(p["samples"][0])
@@ -205,6 +208,14 @@ class GpuRenderer:
         self._check(self._lib.tc_guide_train(self._ctx, s.ctypes.data, s.shape[0], steps, batch, lr, seed,
                                              losses.ctypes.data))
         return losses[:steps]
+
+    def guide_train_recorded(self, steps: int, batch: int, lr: float = 1e-2, seed: int = 0):
+        """Adam steps on the samples recorded by the last render(guide_record=True)."""
+        losses = np.empty(max(steps, 1), np.float32)
+        n = ctypes.c_uint32()
+        self._check(self._lib.tc_guide_train_recorded(self._ctx, steps, batch, lr, seed, losses.ctypes.data,
+                                                      ctypes.byref(n)))
+        return losses[:steps], int(n.value)
 
     def stats(self) -> dict:
         s = native.Stats()
