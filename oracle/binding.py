@@ -75,6 +75,7 @@ def _load():
         lib.orc_num_threads.restype = i32
         lib.orc_aabb_intersects.argtypes = [vp, vp, vp, vp, f32, f32]
         lib.orc_aabb_intersects.restype = i32
+        lib.orc_display_rgba8.argtypes = [vp, u64, f32, vp]
         _lib = lib
     return _lib
 
@@ -296,3 +297,12 @@ def aabb_intersects(mn, mx, origin, inv, tmin, tmax):
     args = [_c(mn), _c(mx), _c(origin), _c(inv)]
     return bool(lib.orc_aabb_intersects(args[0].ctypes.data, args[1].ctypes.data, args[2].ctypes.data,
                                         args[3].ctypes.data, tmin, tmax))
+
+
+def display_rgba8(rgba, exposure_stops=0.0):
+    """Linear-HDR float4 pixels -> display RGBA8 (color.rs:42-74, image_output.rs:57-88)."""
+    lib = _load()
+    px = _c(rgba).reshape(-1, 4)
+    out = np.zeros((px.shape[0], 4), np.uint8)
+    lib.orc_display_rgba8(px.ctypes.data, px.shape[0], exposure_stops, out.ctypes.data)
+    return out

@@ -1107,6 +1107,31 @@ int orc_env_direction_to_uv(void* e, const float* d, float* out) {
   return env->direction_to_uv(v3(d[0], d[1], d[2]), out[0], out[1], out[2]) ? 1 : 0;
 }
 
+// crates/toaster-core/src/color.rs:24-74 and crates/toaster-gpu/src/image_output.rs:57-88: exposure,
+// ACES fitted tone map, clamp, sRGB transfer, round to bytes; alpha clamped and rounded.
+static float aces_channel(float c) {
+  if (std::isnan(c)) return 0.0f;
+  if (!std::isfinite(c)) return c > 0.0f ? 1.0f : 0.0f;
+  c = std::fmax(c, 0.0f);
+  return (c * (2.51f * c + 0.03f)) / (c * (2.43f * c + 0.59f) + 0.14f);
+}
+static float linear_to_srgb(float c) {
+  return c <= 0.0031308f ? 12.92f * c : 1.055f * std::pow(c, 1.0f / 2.4f) - 0.055f;
+}
+static uint8_t channel_to_u8(float c) { return uint8_t(std::round(std::fmin(std::fmax(c, 0.0f), 1.0f) * 255.0f)); }
+
+void orc_display_rgba8(const float* rgba, uint64_t n, float exposure_stops, uint8_t* out) {
+  const float scale = std::exp2(exposure_stops);
+  for (uint64_t i = 0; i < n; ++i) {
+    for (int c = 0; c < 3; ++c) {
+      float t = aces_channel(rgba[4 * i + c] * scale);
+      t = std::fmin(std::fmax(t, 0.0f), 1.0f);
+      out[4 * i + c] = channel_to_u8(linear_to_srgb(t));
+    }
+    out[4 * i + 3] = channel_to_u8(rgba[4 * i + 3]);
+  }
+}
+
 int orc_num_threads() {
 #ifdef _OPENMP
   return omp_get_max_threads();

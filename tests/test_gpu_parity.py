@@ -236,3 +236,13 @@ def test_tcgen05_tile_matches_fp32_matmul(native_lib, a_mn, b_mn, n, k):
     d = native.umma_selftest(a, b, a_mn, b_mn)
     ref = from_bf16_bits(a).astype(np.float64) @ from_bf16_bits(b).astype(np.float64).T
     assert np.allclose(d, ref, rtol=1e-3, atol=1e-3), np.abs(d - ref).max()
+
+
+def test_closest_hit_large_mesh_2_20_rays(renderer):
+    # Config 3 geometry: 1024 x 1024 fBm heightfield (2,093,058 triangles) + 512 spheres; the
+    # hierarchy (2^20 - 1 nodes) lives in HBM.
+    scene = configs.large_mesh()
+    rays = configs.parity_rays(scene, 1 << 20, seed=9)
+    gp, gtt, op, ot = check_hits(renderer, scene, rays)
+    assert np.array_equal(gtt.view(np.uint32), ot.view(np.uint32))
+    assert np.mean(op != MISS) > 0.3

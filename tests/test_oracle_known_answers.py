@@ -465,3 +465,21 @@ def test_rejects_invalid_environment_dimensions_pixels_and_controls():  # enviro
 def test_gpu_types_match_wgsl_layout_sizes():
     for name, (dtype, size) in gt.RECORD_SIZES.items():
         assert dtype.itemsize == size, name
+
+
+# ------------------------------------------------------------------ color.rs / image_output.rs
+def test_converts_float_pixels_to_rgba_once():  # image_output.rs:96-103
+    px = np.array([[-1.0, 0.5, 2.0, 1.0], [0.0, 0.25, 0.75, 0.0]], np.float32)
+    assert ob.display_rgba8(px).reshape(-1).tolist() == [0, 206, 245, 255, 0, 165, 223, 0]
+
+
+def test_display_conversion_handles_nonfinite_radiance():  # color.rs:104-113
+    px = np.array([[np.nan, -np.inf, np.inf, 1.0]], np.float32)
+    assert ob.display_rgba8(px)[0, :3].tolist() == [0, 0, 255]
+
+
+def test_exposure_scales_by_powers_of_two():  # color.rs:88-93
+    px = np.array([[0.125, 0.5, 2.0, 1.0]], np.float32)
+    scale = lambda k: px * np.float32([k, k, k, 1.0])  # noqa: E731 - alpha is not exposed
+    assert np.array_equal(ob.display_rgba8(px, 2.0), ob.display_rgba8(scale(4.0)))
+    assert np.array_equal(ob.display_rgba8(px, -1.0), ob.display_rgba8(scale(0.5)))
