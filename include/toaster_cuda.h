@@ -189,6 +189,24 @@ int tc_render(tc_context* ctx, const tc_gpu_render_params* params, const tc_rend
  * float4 linear-HDR averages into rgba (n_floats >= 4*width*height). */
 int tc_readback(tc_context* ctx, float* rgba, size_t n_floats);
 
+/* Same traversal and estimator as tc_render, for callers that cannot allocate device memory at
+ * render time: hosts whose device memory belongs to their own pool or framework allocator (a
+ * cudaMalloc beside it is invisible to that allocator's accounting and can fail once the pool
+ * has reserved the rest of HBM), and embedders running under a fixed device-memory budget that
+ * must be known before the first frame. No reference counterpart (toaster-gpu allocates all its
+ * buffers through wgpu).
+ * It allocates nothing. The scene comes from an earlier tc_upload_scene; the caller supplies the
+ * FP64 per-pixel sums: `sums` is device memory of at least 3*width*height doubles (n_doubles).
+ * accumulated_samples == 0 clears it first, otherwise the batch is added to it. The image is
+ * sums / (total samples), which the caller tracks. The kernel's scratch (work counter and
+ * counters) is a 256-byte static device array holding at most 32 words; this call uses 4, at any
+ * image size. It is shared by every call: calls whose work overlaps on the GPU race, so
+ * serialise them (one stream, or wait between calls). The first call on a device looks up that
+ * array's address once (cudaGetSymbolAddress). The work is enqueued on `stream` (NULL = the
+ * context's stream) and not synchronised. Rejects frames above 2^31 pixels and sums buffers
+ * smaller than 3*width*height doubles. */
+int tc_render_no_alloc(tc_context* ctx, const tc_gpu_render_params* params, double* sums, size_t n_doubles,
+                       void* stream);
 
 /* Per-pixel FP64 running sums (3 per pixel) and, when keep_moments was set, sums of squared
  * sample values (3 per pixel). Either pointer may be NULL. *samples receives the count. */

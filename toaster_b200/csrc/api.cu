@@ -628,6 +628,46 @@ int tc_render(tc_context* ctx, const tc_gpu_render_params* p, const tc_render_op
   return TC_OK;
 }
 
+int tc_render_no_alloc(tc_context* ctx, const tc_gpu_render_params* p, double* sums, size_t n_doubles, void* stream) {
+  if (!ctx) return fail(nullptr, TC_ERR_INVALID, "context is null");
+  if (!p || !sums) return fail(ctx, TC_ERR_INVALID, "render params or sums buffer is null");
+  if (!ctx->has_scene) return fail(ctx, TC_ERR_STATE, "tc_render_no_alloc before tc_upload_scene");
+  if (p->width == 0 || p->height == 0) return fail(ctx, TC_ERR_INVALID, "render dimensions must be nonzero");
+  if (p->samples == 0) return fail(ctx, TC_ERR_INVALID, "sample batch must be greater than zero");
+  const uint64_t npix = uint64_t(p->width) * p->height;
+  if (npix > (1ull << 31)) return fail(ctx, TC_ERR_INVALID, "image is too large: at most 2^31 pixels");
+  if (n_doubles < 3 * npix)
+    return fail(ctx, TC_ERR_INVALID, "sums buffer holds " + std::to_string(n_doubles) + " doubles; " +
+                                         std::to_string(3 * npix) + " (3 per pixel) are needed");
+  TC_CUDA(ctx, cudaSetDevice(ctx->device));
+  unsigned long long* scratch = nullptr;
+  TC_CUDA(ctx, tcb::render_static_scratch(ctx->device, &scratch));
+  static_assert(tcb::kStaticScratchWords >= 4, "the render scratch needs 4 words");
+  cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : ctx->stream;
+  if (p->accumulated_samples == 0) TC_CUDA(ctx, cudaMemsetAsync(sums, 0, sizeof(double) * 3 * npix, st));
+  TC_CUDA(ctx, cudaMemsetAsync(scratch, 0, 4 * sizeof(unsigned long long), st));
+  tcb::RenderLaunch L{};
+  L.scene = ctx->scene;
+  L.width = p->width;
+  L.height = p->height;
+  L.samples = p->samples;
+  L.max_bounces = p->max_bounces;
+  L.frame_index = p->frame_index;
+  L.sample_base = p->accumulated_samples;
+  L.samples_per_item = 1u;
+  L.items_per_pixel = (p->samples + L.samples_per_item - 1) / L.samples_per_item;
+  L.total_items = npix * L.items_per_pixel;
+  L.accum = sums;
+  L.accum_sq = nullptr;
+  L.work_counter = scratch;
+  L.counters = scratch + 1;
+  const int block = 128;
+  const int per_sm = tcb::render_max_blocks_per_sm(block, false);
+  if (per_sm <= 0) return fail(ctx, TC_ERR_CUDA, "render kernel cannot be resident with this block size");
+  TC_CUDA(ctx, tcb::launch_render(L, block, per_sm * ctx->sm_count, false, st));
+  return TC_OK;
+}
+
 int tc_readback(tc_context* ctx, float* rgba, size_t n_floats) {
   if (!ctx) return fail(nullptr, TC_ERR_INVALID, "context is null");
   if (!rgba) return fail(ctx, TC_ERR_INVALID, "output buffer is null");

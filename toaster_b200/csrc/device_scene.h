@@ -86,6 +86,10 @@ int render_max_blocks_per_sm(int block_size, bool moments, int mode = kModePlain
 cudaError_t launch_guide_samples(const float4* records, const uint32_t* record_count, uint32_t capacity,
                                  const float4* path_radiance, float4* samples, float* weight_sum,
                                  cudaStream_t stream);
+// Device address of the library's static render scratch (kStaticScratchWords 64-bit words) on
+// `device`, which must be the current device; looked up once per device.
+constexpr int kStaticScratchWords = 32;
+cudaError_t render_static_scratch(int device, unsigned long long** out);
 cudaError_t launch_resolve(const double* accum, uint32_t pixels, double inv_samples, float4* out,
                            cudaStream_t stream);
 // Environment importance tables from RGB texels; `row_sums` is FP64 scratch of H entries.

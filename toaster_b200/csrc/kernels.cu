@@ -15,6 +15,8 @@
 #include <math_constants.h>
 #include <stdint.h>
 
+#include <mutex>
+
 #include "device_scene.h"
 #include "traverse.cuh"
 
@@ -804,6 +806,35 @@ cudaError_t launch_guide_samples(const float4* records, const uint32_t* record_c
   guide_samples_kernel<<<(capacity + 255) / 256, 256, 0, stream>>>(records, record_count, capacity, path_radiance,
                                                                    samples, weight_sum);
   return cudaGetLastError();
+}
+
+// ------------------------------------------------------------------------ scratch without allocation
+// Scratch of tc_render_no_alloc: [0] the work-queue counter, [1..3] the path, extension-ray and
+// shadow-ray counters. Every GPU that loads the library holds these 256 bytes until exit; all
+// calls share them, so the entry point clears them at the start of each call, and calls whose
+// kernels overlap on the GPU race on them.
+static __device__ __align__(256) unsigned long long g_render_scratch[kStaticScratchWords];
+
+cudaError_t render_static_scratch(int device, unsigned long long** out) {
+  // The symbol's device address is looked up once per device, with that device current (host
+  // code must never hand the array's name itself to a kernel: it is only a host-side stand-in).
+  constexpr int kMaxDevices = 64;
+  static std::mutex lock;
+  static unsigned long long* cache[kMaxDevices] = {};
+  if (device < 0 || device >= kMaxDevices) return cudaErrorInvalidDevice;
+  std::lock_guard<std::mutex> guard(lock);
+  if (!cache[device]) {
+    int current = 0;
+    cudaError_t e = cudaGetDevice(&current);
+    if (e != cudaSuccess) return e;
+    if (current != device) return cudaErrorInvalidDevice;
+    void* ptr = nullptr;
+    e = cudaGetSymbolAddress(&ptr, g_render_scratch);
+    if (e != cudaSuccess) return e;
+    cache[device] = static_cast<unsigned long long*>(ptr);
+  }
+  *out = cache[device];
+  return cudaSuccess;
 }
 
 // ------------------------------------------------------------------------ resolve

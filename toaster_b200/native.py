@@ -46,6 +46,7 @@ EXPORTED_SYMBOLS = (
     "tc_guide_loss_grad",
     "tc_guide_adam_step",
     "tc_guide_train",
+    "tc_render_no_alloc",
     "tc_guide_train_recorded",
 )
 
@@ -145,6 +146,7 @@ def load_library(path: os.PathLike | None = None) -> ctypes.CDLL:
     lib.tc_guide_infer.argtypes = [vp, vp, sz, vp]
     lib.tc_guide_loss_grad.argtypes = [vp, vp, sz, vp, vp]
     lib.tc_guide_adam_step.argtypes = [vp, f32]
+    lib.tc_render_no_alloc.argtypes = [vp, vp, vp, sz, vp]
     lib.tc_guide_train_recorded.argtypes = [vp, u32, u32, f32, ctypes.c_uint64, vp, ctypes.POINTER(u32)]
     lib.tc_guide_train.argtypes = [vp, vp, sz, u32, u32, f32, ctypes.c_uint64, vp]
     for name in EXPORTED_SYMBOLS:
