@@ -179,15 +179,57 @@ int tc_upload_scene(tc_context* ctx, const tc_scene_data* scene);
 /* Replaces the camera write_buffer (path_tracer.rs:680-684). */
 int tc_set_camera(tc_context* ctx, const tc_gpu_camera* camera);
 
+/* What one scene evaluation changed; mirrors toaster_scene::SceneChanges
+ * (crates/toaster-scene/src/evaluation.rs:9-18). Nonzero = changed. */
+typedef struct tc_scene_changes {
+  uint32_t camera;             /* camera basis or position */
+  uint32_t spheres;            /* at least one sphere moved or resized */
+  uint32_t triangles;          /* at least one triangle or its attributes changed */
+  uint32_t emissive_geometry;  /* a moved primitive is emissive: the light records change */
+} tc_scene_changes;
+
+/* Per-frame update of an uploaded scene (the evaluated frame of path_tracer.rs:611-721). Instead
+ * of the reference's host rebuild + full re-upload, the changed geometry is copied to the device
+ * and the hierarchy is refit there: primitive records are rewritten and every box is recomputed
+ * bottom-up with the topology of the last tc_upload_scene. Intersections stay exact; only the
+ * tree's quality drifts under large motion (call tc_upload_scene to rebuild). `scene` holds the
+ * whole evaluated frame in the reference records; its counts must equal the uploaded scene's
+ * (path_tracer.rs:639-653). Materials are not re-read. Lights are re-packed when
+ * emissive_geometry is set, the camera when camera is set. Synchronous. */
+int tc_update_geometry(tc_context* ctx, const tc_scene_data* scene, const tc_scene_changes* changes);
+
 /* Replaces dispatch_compute_2d (crates/toaster-gpu/src/dispatch.rs:28-60): traces
  * params->samples paths per pixel. params->accumulated_samples == 0 starts a new image;
  * otherwise it must equal the samples already accumulated (progressive mode,
  * path_tracer.rs:900-923). options may be NULL. */
 int tc_render(tc_context* ctx, const tc_gpu_render_params* params, const tc_render_options* options);
 
+/* One persistent launch over n independent frames of possibly different scenes and sizes:
+ * contexts[i] holds scene i (from tc_upload_scene) and renders params[i] under the same
+ * progressive contract as tc_render. Work items of all frames share one queue, so small frames
+ * fill the GPU together instead of one launch (and one tail) each. No reference counterpart: the
+ * reference renders scenes one dispatch at a time (dispatch.rs:28-60). All contexts must be on
+ * one device and distinct; the launch runs on contexts[0]'s stream after the others' pending
+ * work, and tc_get_stats(contexts[0]) reports the whole batch. Plain sampling only (options may
+ * set block_size and samples_per_item). Synchronous. */
+int tc_render_batch(tc_context* const* contexts, const tc_gpu_render_params* params, size_t n,
+                    const tc_render_options* options);
+
 /* Replaces readback_pixels (crates/toaster-gpu/src/readback.rs:8-25): writes width*height
  * float4 linear-HDR averages into rgba (n_floats >= 4*width*height). */
 int tc_readback(tc_context* ctx, float* rgba, size_t n_floats);
+
+/* Display conversion on the device, then readback of 4 bytes per pixel: exposure (2^stops),
+ * ACES fitted tone map, clamp, sRGB transfer and rounding to RGBA8 (alpha 255), row-major,
+ * y down. Replaces readback_pixels + pixels_to_rgba_image (crates/toaster-gpu/src/
+ * image_output.rs:57-88 over crates/toaster-core/src/color.rs:24-74), which convert on the
+ * host after copying 16 bytes per pixel. n_bytes >= 4*width*height. */
+int tc_readback_rgba8(tc_context* ctx, float exposure_stops, uint8_t* rgba, size_t n_bytes);
+
+/* The same conversion into caller-owned device memory (d_rgba, n_bytes >= 4*width*height),
+ * enqueued on `stream` (NULL = the context's stream) without synchronising, for sinks that
+ * consume frames on the device. No reference counterpart. */
+int tc_display_rgba8_async(tc_context* ctx, float exposure_stops, void* d_rgba, size_t n_bytes, void* stream);
 
 /* Same traversal and estimator as tc_render, for callers that cannot allocate device memory at
  * render time: hosts whose device memory belongs to their own pool or framework allocator (a
@@ -257,6 +299,13 @@ int tc_guide_train(tc_context* ctx, const float* samples, size_t n, uint32_t ste
  * n_samples (optional) the number of samples. */
 int tc_guide_train_recorded(tc_context* ctx, uint32_t steps, uint32_t batch, float lr, uint64_t seed, float* losses,
                             uint32_t* n_samples);
+
+/* The training samples derived from the last guide_record batch, as tc_guide_train_recorded
+ * sees them: 12 floats each (position + weight, normal + 0, direction + 0), weight = luminance of
+ * the radiance that arrived along the recorded direction. Writes min(count, n_floats / 12)
+ * samples; *count receives the number recorded. out may be NULL to query the count. No
+ * reference counterpart (inspection of the guiding data). */
+int tc_guide_recorded_samples(tc_context* ctx, float* out, size_t n_floats, uint32_t* count);
 
 /* Tensor-core self-test (no reference counterpart): one 128 x n tile D = A * B^T with bf16 A
  * (128 x k, row-major) and B (n x k, row-major) staged in shared memory as K-major

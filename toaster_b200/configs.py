@@ -262,13 +262,15 @@ def _quad(a, b, c, d):
 
 
 def room_with_window(seed: int = 0, width: int = 1280, height: int = 720, samples: int = 16, max_bounces: int = 8,
-                     clutter: int = 8192, environment: EnvironmentMap | None = None) -> Scene:
+                     clutter: int = 8192, environment: EnvironmentMap | None = None,
+                     metal_fraction: float = 0.3) -> Scene:
     """Hard-lighting interior: a closed 4 x 3 x 4 room (x, z in [-2, 2], y in [0, 3]) whose only
     opening is a 0.4 x 0.4 window in the +z wall (x in [0.3, 0.7], y in [1.6, 2.0]); it is lit only
     by the mixed-scene sky and sun through that window. Walls 0.7, floor 0.5, ceiling 0.8 diffuse.
     ``clutter`` seeded triangles (centre uniform in [-1.8, 1.8] x [0.1, 2.5] x [-1.8, 1.6], edges as in
     random_triangles) are 70% diffuse (albedo U[0.2, 0.8]^3) and 30% metal (albedo U[0.5, 0.95]^3,
-    roughness U[0, 0.5]). The camera stands near the -z wall looking toward the window wall."""
+    roughness U[0, 0.5]); ``metal_fraction`` changes that split. The camera stands near the -z wall
+    looking toward the window wall."""
     rng = np.random.default_rng(seed + 5000)
     x0, x1, y0, y1, z0, z1 = -2.0, 2.0, 0.0, 3.0, -2.0, 2.0
     wx0, wx1, wy0, wy1 = 0.3, 0.7, 1.6, 2.0
@@ -294,7 +296,7 @@ def room_with_window(seed: int = 0, width: int = 1280, height: int = 720, sample
     kinds = rng.uniform(0, 1, clutter)
     clutter_mat = []
     for i in range(clutter):
-        if kinds[i] < 0.7:
+        if kinds[i] >= metal_fraction:
             mats.append(Material.diffuse(rng.uniform(0.2, 0.8, 3), f"c{i}"))
         else:
             mats.append(Material.metal(rng.uniform(0.5, 0.95, 3), rng.uniform(0.0, 0.5), f"c{i}"))

@@ -15,8 +15,10 @@
 #include "../../include/toaster_cuda.h"
 #include "bvh_build.h"
 #include "device_scene.h"
+#include "display.h"
 #include "guide.h"
 #include "layout.h"
+#include "refit.h"
 
 static_assert(sizeof(tc_gpu_render_params) == 96, "GpuRenderParams is 96 bytes");
 static_assert(sizeof(tc_gpu_camera) == 64, "GpuCamera is 64 bytes");
@@ -75,6 +77,14 @@ struct tc_context {
   DevBuf env_rgb, env_marginal, env_conditional, env_pdf, env_row_sums, env_total;
   uint32_t sphere_count = 0, triangle_count = 0, material_count = 0, light_count = 0, bvh_prims = 0;
   uint32_t bvh_depth = 0;
+  bool any_attr = false;
+  // Geometry refit (tc_update_geometry): the root record, the scene-order geometry the prim
+  // records are rewritten from, and pair-node indices grouped by depth.
+  DevBuf root_buf, raw_spheres, raw_triangles, refit_nodes;
+  std::vector<uint32_t> refit_levels;
+  bool raw_spheres_valid = false, raw_triangles_valid = false;
+  // Display conversion output (packed RGBA8) and the job table of batched launches.
+  DevBuf display, batch_jobs;
 
   // Accumulation state (progressive contract of path_tracer.rs:900-923)
   uint32_t width = 0, height = 0, accumulated = 0;
@@ -156,6 +166,120 @@ void build_alias(const std::vector<double>& w, std::vector<float>& prob, std::ve
 }
 
 bool finite3(const float* v) { return std::isfinite(v[0]) && std::isfinite(v[1]) && std::isfinite(v[2]); }
+
+// Per-primitive checks shared by uploads and geometry updates (scene_upload.rs:84-98 plus
+// finiteness, which the device layout needs).
+int validate_geometry(tc_context* ctx, const tc_scene_data* sd, uint32_t n_mat) {
+  for (size_t i = 0; i < sd->sphere_count; ++i) {
+    const tc_gpu_sphere& s = sd->spheres[i];
+    if (s.material_index >= n_mat) return fail(ctx, TC_ERR_INVALID, "sphere " + std::to_string(i) + " references an unknown material");
+    if (!std::isfinite(s.center_radius[3]) || !(s.center_radius[3] > 0.0f) || !finite3(s.center_radius))
+      return fail(ctx, TC_ERR_INVALID, "sphere " + std::to_string(i) + " must have a finite center and positive radius");
+  }
+  for (size_t i = 0; i < sd->triangle_count; ++i) {
+    const tc_gpu_triangle& t = sd->triangles[i];
+    if (t.material_index >= n_mat) return fail(ctx, TC_ERR_INVALID, "triangle " + std::to_string(i) + " references an unknown material");
+    if (!finite3(t.v0) || !finite3(t.v1) || !finite3(t.v2))
+      return fail(ctx, TC_ERR_INVALID, "triangle " + std::to_string(i) + " vertices must be finite");
+  }
+  return TC_OK;
+}
+
+// Device light records with a Walker alias table over the GpuLight weights (the light
+// distribution of light.rs:57-113). Validates kinds, areas and material references.
+int pack_lights(tc_context* ctx, const tc_scene_data* sd, uint32_t n_mat, std::vector<tcb::DevLight>& lights) {
+  lights.assign(sd->light_count, tcb::DevLight{});
+  if (sd->light_count) {
+    if (!sd->lights) return fail(ctx, TC_ERR_INVALID, "light pointer is null for a nonzero count");
+    std::vector<double> w(sd->light_count);
+    double total = 0.0;
+    for (size_t i = 0; i < sd->light_count; ++i) {
+      w[i] = std::max(0.0, double(sd->lights[i].area_weight_cumulative[1]));
+      total += w[i];
+    }
+    if (!(total > 0.0)) return fail(ctx, TC_ERR_INVALID, "lights have no positive weight");
+    std::vector<float> prob;
+    std::vector<uint32_t> alias;
+    build_alias(w, prob, alias);
+    for (size_t i = 0; i < sd->light_count; ++i) {
+      const tc_gpu_light& l = sd->lights[i];
+      if (l.material_index >= n_mat) return fail(ctx, TC_ERR_INVALID, "light " + std::to_string(i) + " references an unknown material");
+      const tc_gpu_material& m = sd->materials[l.material_index];
+      tcb::DevLight d{};
+      d.kind = l.kind;
+      const float area = l.area_weight_cumulative[0];
+      if (!(area > 0.0f)) return fail(ctx, TC_ERR_INVALID, "light " + std::to_string(i) + " has no area");
+      d.pdf_area = float((w[i] / total) / double(area));
+      for (int c = 0; c < 3; ++c) d.emission[c] = m.albedo[c] * m.params[2];
+      if (l.kind == 0) {
+        float e1[3], e2[3];
+        for (int c = 0; c < 3; ++c) {
+          d.p0[c] = l.v0[c];
+          e1[c] = l.v1[c] - l.v0[c];
+          e2[c] = l.v2[c] - l.v0[c];
+          d.e1[c] = e1[c];
+          d.e2[c] = e2[c];
+        }
+        const float nx = e1[1] * e2[2] - e2[1] * e1[2], ny = e1[2] * e2[0] - e2[2] * e1[0],
+                    nz = e1[0] * e2[1] - e2[0] * e1[1];
+        const float inv = 1.0f / std::sqrt(nx * nx + ny * ny + nz * nz);
+        d.normal[0] = nx * inv;
+        d.normal[1] = ny * inv;
+        d.normal[2] = nz * inv;
+      } else if (l.kind == 1) {
+        for (int c = 0; c < 3; ++c) d.p0[c] = l.center_radius[c];
+        d.radius = l.center_radius[3];
+      } else {
+        return fail(ctx, TC_ERR_INVALID, "light " + std::to_string(i) + " kind must be 0 (triangle) or 1 (sphere)");
+      }
+      d.alias_prob = prob[i];
+      d.alias = alias[i];
+      lights[i] = d;
+    }
+  }
+  return TC_OK;
+}
+
+// Progressive contract of path_tracer.rs:900-923: accumulated_samples == 0 starts a new image
+// (buffers sized and cleared on `st`), otherwise it must equal the samples already held.
+int prepare_accumulation(tc_context* ctx, const tc_gpu_render_params* p, bool moments, cudaStream_t st) {
+  const uint32_t npix = p->width * p->height;
+  if (p->accumulated_samples == 0) {
+    if (ctx->width != p->width || ctx->height != p->height || !ctx->accum.ptr) {
+      TC_CUDA(ctx, ctx->accum.reserve(sizeof(double) * 3 * npix));
+      TC_CUDA(ctx, ctx->image.reserve(sizeof(float4) * npix));
+    }
+    if (moments) TC_CUDA(ctx, ctx->accum_sq.reserve(sizeof(double) * 3 * npix));
+    TC_CUDA(ctx, cudaMemsetAsync(ctx->accum.ptr, 0, sizeof(double) * 3 * npix, st));
+    if (moments) TC_CUDA(ctx, cudaMemsetAsync(ctx->accum_sq.ptr, 0, sizeof(double) * 3 * npix, st));
+    ctx->width = p->width;
+    ctx->height = p->height;
+    ctx->accumulated = 0;
+    ctx->has_moments = moments;
+  } else {
+    if (p->width != ctx->width || p->height != ctx->height)
+      return fail(ctx, TC_ERR_STATE, "progressive batch changes the image size");
+    if (p->accumulated_samples != ctx->accumulated)
+      return fail(ctx, TC_ERR_STATE, "accumulated_samples " + std::to_string(p->accumulated_samples) +
+                                          " does not match the " + std::to_string(ctx->accumulated) +
+                                          " samples held by the context");
+    if (moments && !ctx->has_moments)
+      return fail(ctx, TC_ERR_STATE, "keep_moments must be set from the first batch of an accumulation");
+  }
+  if (uint64_t(ctx->accumulated) + p->samples > 0xFFFFFFFFull)
+    return fail(ctx, TC_ERR_INVALID, "progressive accumulated sample count overflowed");
+  return TC_OK;
+}
+
+// Checks shared by every render entry point.
+int check_render_params(tc_context* ctx, const tc_gpu_render_params* p) {
+  if (!p) return fail(ctx, TC_ERR_INVALID, "render params are null");
+  if (!ctx->has_scene) return fail(ctx, TC_ERR_STATE, "render before tc_upload_scene");
+  if (p->width == 0 || p->height == 0) return fail(ctx, TC_ERR_INVALID, "render dimensions must be nonzero");
+  if (p->samples == 0) return fail(ctx, TC_ERR_INVALID, "sample batch must be greater than zero");
+  if (uint64_t(p->width) * p->height > (1ull << 31)) return fail(ctx, TC_ERR_INVALID, "image is too large");
+  return TC_OK;
+}
 
 }  // namespace
 
@@ -256,18 +380,7 @@ int tc_upload_scene(tc_context* ctx, const tc_scene_data* sd) {
   if (sd->sphere_count + sd->triangle_count > tcb::kMaxPrimitives)
     return fail(ctx, TC_ERR_INVALID, "too many primitives for GPU");
   const uint32_t n_mat = uint32_t(sd->material_count);
-  for (size_t i = 0; i < sd->sphere_count; ++i) {
-    const tc_gpu_sphere& s = sd->spheres[i];
-    if (s.material_index >= n_mat) return fail(ctx, TC_ERR_INVALID, "sphere " + std::to_string(i) + " references an unknown material");
-    if (!std::isfinite(s.center_radius[3]) || !(s.center_radius[3] > 0.0f) || !finite3(s.center_radius))
-      return fail(ctx, TC_ERR_INVALID, "sphere " + std::to_string(i) + " must have a finite center and positive radius");
-  }
-  for (size_t i = 0; i < sd->triangle_count; ++i) {
-    const tc_gpu_triangle& t = sd->triangles[i];
-    if (t.material_index >= n_mat) return fail(ctx, TC_ERR_INVALID, "triangle " + std::to_string(i) + " references an unknown material");
-    if (!finite3(t.v0) || !finite3(t.v1) || !finite3(t.v2))
-      return fail(ctx, TC_ERR_INVALID, "triangle " + std::to_string(i) + " vertices must be finite");
-  }
+  if (int rc = validate_geometry(ctx, sd, n_mat)) return rc;
   const uint32_t bg = sd->params.background_kind;
   if (bg > 2u) return fail(ctx, TC_ERR_INVALID, "background kind must be 0 (sky), 1 (black) or 2 (environment)");
   const uint32_t ew = sd->params.environment_width, eh = sd->params.environment_height;
@@ -350,55 +463,8 @@ int tc_upload_scene(tc_context* ctx, const tc_scene_data* sd) {
     return fail(ctx, TC_ERR_INVALID, err);
 
   // Lights: alias table over the GpuLight weights (light.rs:57-113 distribution).
-  std::vector<tcb::DevLight> lights(sd->light_count);
-  if (sd->light_count) {
-    if (!sd->lights) return fail(ctx, TC_ERR_INVALID, "light pointer is null for a nonzero count");
-    std::vector<double> w(sd->light_count);
-    double total = 0.0;
-    for (size_t i = 0; i < sd->light_count; ++i) {
-      w[i] = std::max(0.0, double(sd->lights[i].area_weight_cumulative[1]));
-      total += w[i];
-    }
-    if (!(total > 0.0)) return fail(ctx, TC_ERR_INVALID, "lights have no positive weight");
-    std::vector<float> prob;
-    std::vector<uint32_t> alias;
-    build_alias(w, prob, alias);
-    for (size_t i = 0; i < sd->light_count; ++i) {
-      const tc_gpu_light& l = sd->lights[i];
-      if (l.material_index >= n_mat) return fail(ctx, TC_ERR_INVALID, "light " + std::to_string(i) + " references an unknown material");
-      const tc_gpu_material& m = sd->materials[l.material_index];
-      tcb::DevLight d{};
-      d.kind = l.kind;
-      const float area = l.area_weight_cumulative[0];
-      if (!(area > 0.0f)) return fail(ctx, TC_ERR_INVALID, "light " + std::to_string(i) + " has no area");
-      d.pdf_area = float((w[i] / total) / double(area));
-      for (int c = 0; c < 3; ++c) d.emission[c] = m.albedo[c] * m.params[2];
-      if (l.kind == 0) {
-        float e1[3], e2[3];
-        for (int c = 0; c < 3; ++c) {
-          d.p0[c] = l.v0[c];
-          e1[c] = l.v1[c] - l.v0[c];
-          e2[c] = l.v2[c] - l.v0[c];
-          d.e1[c] = e1[c];
-          d.e2[c] = e2[c];
-        }
-        const float nx = e1[1] * e2[2] - e2[1] * e1[2], ny = e1[2] * e2[0] - e2[2] * e1[0],
-                    nz = e1[0] * e2[1] - e2[0] * e1[1];
-        const float inv = 1.0f / std::sqrt(nx * nx + ny * ny + nz * nz);
-        d.normal[0] = nx * inv;
-        d.normal[1] = ny * inv;
-        d.normal[2] = nz * inv;
-      } else if (l.kind == 1) {
-        for (int c = 0; c < 3; ++c) d.p0[c] = l.center_radius[c];
-        d.radius = l.center_radius[3];
-      } else {
-        return fail(ctx, TC_ERR_INVALID, "light " + std::to_string(i) + " kind must be 0 (triangle) or 1 (sphere)");
-      }
-      d.alias_prob = prob[i];
-      d.alias = alias[i];
-      lights[i] = d;
-    }
-  }
+  std::vector<tcb::DevLight> lights;
+  if (int rc = pack_lights(ctx, sd, n_mat, lights)) return rc;
 
   // Upload.
   cudaStream_t st = ctx->stream;
@@ -408,6 +474,25 @@ int tc_upload_scene(tc_context* ctx, const tc_scene_data* sd) {
   TC_CUDA(ctx, upload(ctx->lights, lights.data(), lights.size(), st));
   bool any_attr = false;
   for (uint32_t f : tri_flags) any_attr |= f != 0u;
+  TC_CUDA(ctx, upload(ctx->root_buf, &dh.root, 1, st));
+  {
+    // Pair nodes grouped by depth, root first, for the bottom-up refit.
+    std::vector<uint32_t> order, offsets{0u};
+    if (!(dh.root.link & tcb::kLeafBit)) {
+      order.push_back(dh.root.link);
+      size_t begin = 0;
+      while (begin < order.size()) {
+        const size_t end = order.size();
+        offsets.push_back(uint32_t(end));
+        for (size_t i = begin; i < end; ++i)
+          for (const tcb::ChildRec& c : dh.pairs[order[i]].child)
+            if (!(c.link & tcb::kLeafBit)) order.push_back(c.link);
+        begin = end;
+      }
+    }
+    TC_CUDA(ctx, upload(ctx->refit_nodes, order.data(), order.size(), st));
+    ctx->refit_levels = std::move(offsets);
+  }
   if (any_attr) TC_CUDA(ctx, upload(ctx->attributes, sd->triangle_attributes, sd->triangle_count, st));
   if (sd->texture_pixels && sd->texture_pixel_count)
     TC_CUDA(ctx, upload(ctx->texels, sd->texture_pixels, sd->texture_pixel_count, st));
@@ -416,7 +501,7 @@ int tc_upload_scene(tc_context* ctx, const tc_scene_data* sd) {
   s = tcb::DevScene{};
   s.pairs = ctx->pairs.as<tcb::PairNode>();
   s.prims = ctx->prims.as<tcb::PrimRecord>();
-  s.root = dh.root;
+  s.root = ctx->root_buf.as<tcb::ChildRec>();
   s.materials = ctx->materials.as<tcb::DevMaterial>();
   s.material_count = n_mat;
   s.lights = sd->light_count ? ctx->lights.as<tcb::DevLight>() : nullptr;
@@ -466,6 +551,62 @@ int tc_upload_scene(tc_context* ctx, const tc_scene_data* sd) {
   ctx->bvh_prims = uint32_t(flat.prims.size());
   ctx->bvh_depth = dh.depth;
   ctx->stats.bvh_depth = dh.depth;
+  ctx->any_attr = any_attr;
+  ctx->raw_spheres_valid = ctx->raw_triangles_valid = false;
+  return TC_OK;
+}
+
+int tc_update_geometry(tc_context* ctx, const tc_scene_data* sd, const tc_scene_changes* changes) {
+  if (!ctx) return fail(nullptr, TC_ERR_INVALID, "context is null");
+  if (!sd || !changes) return fail(ctx, TC_ERR_INVALID, "scene or change set is null");
+  if (!ctx->has_scene) return fail(ctx, TC_ERR_STATE, "tc_update_geometry before tc_upload_scene");
+  // Counts are fixed for a render session (path_tracer.rs:639-653).
+  if (sd->sphere_count != ctx->sphere_count || sd->triangle_count != ctx->triangle_count ||
+      sd->material_count != ctx->material_count || sd->light_count != ctx->light_count ||
+      (sd->triangle_attributes && sd->triangle_attribute_count != sd->triangle_count))
+    return fail(ctx, TC_ERR_INVALID,
+                "evaluated scenes must preserve GPU geometry, material, light, and BVH primitive counts");
+  if (!sd->materials) return fail(ctx, TC_ERR_INVALID, "GPU renderer requires at least one material");
+  if ((sd->sphere_count && !sd->spheres) || (sd->triangle_count && !sd->triangles))
+    return fail(ctx, TC_ERR_INVALID, "geometry pointer is null for a nonzero count");
+  const bool geometry = changes->spheres || changes->triangles;
+  if (geometry)
+    if (int rc = validate_geometry(ctx, sd, ctx->material_count)) return rc;
+  std::vector<tcb::DevLight> lights;
+  if (changes->emissive_geometry)
+    if (int rc = pack_lights(ctx, sd, ctx->material_count, lights)) return rc;
+  TC_CUDA(ctx, cudaSetDevice(ctx->device));
+  cudaStream_t st = ctx->stream;
+  if (geometry) {
+    if (ctx->sphere_count && (changes->spheres || !ctx->raw_spheres_valid)) {
+      TC_CUDA(ctx, upload(ctx->raw_spheres, sd->spheres, sd->sphere_count, st));
+      ctx->raw_spheres_valid = true;
+    }
+    if (ctx->triangle_count && (changes->triangles || !ctx->raw_triangles_valid)) {
+      TC_CUDA(ctx, upload(ctx->raw_triangles, sd->triangles, sd->triangle_count, st));
+      ctx->raw_triangles_valid = true;
+    }
+    if (changes->triangles && ctx->any_attr && sd->triangle_attributes)
+      TC_CUDA(ctx, upload(ctx->attributes, sd->triangle_attributes, sd->triangle_count, st));
+    tcb::RefitPlan plan;
+    plan.nodes = ctx->refit_nodes.as<uint32_t>();
+    plan.level_offsets = ctx->refit_levels;
+    TC_CUDA(ctx, tcb::launch_refit(plan, ctx->pairs.as<tcb::PairNode>(), ctx->root_buf.as<tcb::ChildRec>(),
+                                   ctx->prims.as<tcb::PrimRecord>(), ctx->bvh_prims,
+                                   ctx->raw_spheres.as<tc_gpu_sphere>(), ctx->raw_triangles.as<tc_gpu_triangle>(), st));
+  }
+  if (changes->emissive_geometry && !lights.empty())
+    TC_CUDA(ctx, upload(ctx->lights, lights.data(), lights.size(), st));
+  if (changes->camera) {
+    tcb::DevScene& s = ctx->scene;
+    for (int c = 0; c < 3; ++c) {
+      s.cam_origin[c] = sd->camera.origin[c];
+      s.cam_lower_left[c] = sd->camera.lower_left_corner[c];
+      s.cam_horizontal[c] = sd->camera.horizontal[c];
+      s.cam_vertical[c] = sd->camera.vertical[c];
+    }
+  }
+  TC_CUDA(ctx, cudaStreamSynchronize(st));
   return TC_OK;
 }
 
@@ -484,11 +625,7 @@ int tc_set_camera(tc_context* ctx, const tc_gpu_camera* cam) {
 
 int tc_render(tc_context* ctx, const tc_gpu_render_params* p, const tc_render_options* opt) {
   if (!ctx) return fail(nullptr, TC_ERR_INVALID, "context is null");
-  if (!p) return fail(ctx, TC_ERR_INVALID, "render params are null");
-  if (!ctx->has_scene) return fail(ctx, TC_ERR_STATE, "tc_render before tc_upload_scene");
-  if (p->width == 0 || p->height == 0) return fail(ctx, TC_ERR_INVALID, "render dimensions must be nonzero");
-  if (p->samples == 0) return fail(ctx, TC_ERR_INVALID, "sample batch must be greater than zero");
-  if (uint64_t(p->width) * p->height > (1ull << 31)) return fail(ctx, TC_ERR_INVALID, "image is too large");
+  if (int rc = check_render_params(ctx, p)) return rc;
   TC_CUDA(ctx, cudaSetDevice(ctx->device));
   tc_render_options o{};
   if (opt) o = *opt;
@@ -496,44 +633,21 @@ int tc_render(tc_context* ctx, const tc_gpu_render_params* p, const tc_render_op
   const uint32_t npix = p->width * p->height;
   cudaStream_t st = ctx->stream;
   TC_CUDA(ctx, cudaEventRecord(ctx->ev_begin, st));
-  if (p->accumulated_samples == 0) {
-    if (ctx->width != p->width || ctx->height != p->height || !ctx->accum.ptr) {
-      TC_CUDA(ctx, ctx->accum.reserve(sizeof(double) * 3 * npix));
-      TC_CUDA(ctx, ctx->image.reserve(sizeof(float4) * npix));
-    }
-    if (moments) TC_CUDA(ctx, ctx->accum_sq.reserve(sizeof(double) * 3 * npix));
-    TC_CUDA(ctx, cudaMemsetAsync(ctx->accum.ptr, 0, sizeof(double) * 3 * npix, st));
-    if (moments) TC_CUDA(ctx, cudaMemsetAsync(ctx->accum_sq.ptr, 0, sizeof(double) * 3 * npix, st));
-    ctx->width = p->width;
-    ctx->height = p->height;
-    ctx->accumulated = 0;
-    ctx->has_moments = moments;
-  } else {
-    if (p->width != ctx->width || p->height != ctx->height)
-      return fail(ctx, TC_ERR_STATE, "progressive batch changes the image size");
-    if (p->accumulated_samples != ctx->accumulated)
-      return fail(ctx, TC_ERR_STATE, "accumulated_samples " + std::to_string(p->accumulated_samples) +
-                                          " does not match the " + std::to_string(ctx->accumulated) +
-                                          " samples held by the context");
-    if (moments && !ctx->has_moments)
-      return fail(ctx, TC_ERR_STATE, "keep_moments must be set from the first batch of an accumulation");
-  }
-  if (uint64_t(ctx->accumulated) + p->samples > 0xFFFFFFFFull)
-    return fail(ctx, TC_ERR_INVALID, "progressive accumulated sample count overflowed");
+  if (int rc = prepare_accumulation(ctx, p, moments, st)) return rc;
 
   tcb::RenderLaunch L{};
-  L.scene = ctx->scene;
-  L.width = p->width;
-  L.height = p->height;
-  L.samples = p->samples;
-  L.max_bounces = p->max_bounces;
-  L.frame_index = p->frame_index;
-  L.sample_base = ctx->accumulated;
-  L.samples_per_item = std::min<uint32_t>(o.samples_per_item ? o.samples_per_item : 1u, p->samples);
-  L.items_per_pixel = (p->samples + L.samples_per_item - 1) / L.samples_per_item;
-  L.total_items = uint64_t(npix) * L.items_per_pixel;
-  L.accum = ctx->accum.as<double>();
-  L.accum_sq = moments ? ctx->accum_sq.as<double>() : nullptr;
+  L.f.scene = ctx->scene;
+  L.f.width = p->width;
+  L.f.height = p->height;
+  L.f.samples = p->samples;
+  L.f.max_bounces = p->max_bounces;
+  L.f.frame_index = p->frame_index;
+  L.f.sample_base = ctx->accumulated;
+  L.f.samples_per_item = std::min<uint32_t>(o.samples_per_item ? o.samples_per_item : 1u, p->samples);
+  L.f.items_per_pixel = (p->samples + L.f.samples_per_item - 1) / L.f.samples_per_item;
+  L.total_items = uint64_t(npix) * L.f.items_per_pixel;
+  L.f.accum = ctx->accum.as<double>();
+  L.f.accum_sq = moments ? ctx->accum_sq.as<double>() : nullptr;
   L.work_counter = ctx->work_counter.as<unsigned long long>();
   L.counters = ctx->counters.as<unsigned long long>();
   TC_CUDA(ctx, cudaMemsetAsync(ctx->work_counter.ptr, 0, sizeof(unsigned long long), st));
@@ -628,6 +742,93 @@ int tc_render(tc_context* ctx, const tc_gpu_render_params* p, const tc_render_op
   return TC_OK;
 }
 
+int tc_render_batch(tc_context* const* contexts, const tc_gpu_render_params* params, size_t n,
+                    const tc_render_options* opt) {
+  if (!contexts || !params || n == 0) return fail(nullptr, TC_ERR_INVALID, "batch is empty or null");
+  tc_context* lead = contexts[0];
+  if (!lead) return fail(nullptr, TC_ERR_INVALID, "context 0 of the batch is null");
+  tc_render_options o{};
+  if (opt) o = *opt;
+  if (o.keep_moments || o.guiding || o.guide_record)
+    return fail(lead, TC_ERR_INVALID, "batched frames are plain renders (no moments, guiding or recording)");
+  const int block = o.block_size ? int(o.block_size) : 128;
+  if (block % 32 != 0 || block < 32 || block > 256)
+    return fail(lead, TC_ERR_INVALID, "block_size must be a multiple of 32 in [32, 256]");
+  for (size_t i = 0; i < n; ++i) {
+    tc_context* c = contexts[i];
+    if (!c) return fail(lead, TC_ERR_INVALID, "context " + std::to_string(i) + " of the batch is null");
+    if (c->device != lead->device) return fail(lead, TC_ERR_INVALID, "batched contexts must share one device");
+    for (size_t j = 0; j < i; ++j)
+      if (contexts[j] == c) return fail(lead, TC_ERR_INVALID, "a context appears twice in the batch");
+    if (int rc = check_render_params(c, &params[i])) {
+      lead->error = "frame " + std::to_string(i) + ": " + c->error;
+      return rc;
+    }
+  }
+  TC_CUDA(lead, cudaSetDevice(lead->device));
+  cudaStream_t st = lead->stream;
+  TC_CUDA(lead, cudaEventRecord(lead->ev_begin, st));
+  std::vector<tcb::FrameJob> jobs(n);
+  uint64_t items = 0, paths = 0;
+  for (size_t i = 0; i < n; ++i) {
+    tc_context* c = contexts[i];
+    const tc_gpu_render_params* p = &params[i];
+    if (c != lead) {  // the batch writes this context's buffers: order after its own stream
+      TC_CUDA(lead, cudaEventRecord(c->ev_begin, c->stream));
+      TC_CUDA(lead, cudaStreamWaitEvent(st, c->ev_begin, 0));
+    }
+    if (int rc = prepare_accumulation(c, p, false, st)) {
+      lead->error = "frame " + std::to_string(i) + ": " + c->error;
+      return rc;
+    }
+    tcb::FrameJob& J = jobs[i];
+    J = tcb::FrameJob{};
+    J.scene = c->scene;
+    J.accum = c->accum.as<double>();
+    J.accum_sq = nullptr;
+    J.item_begin = items;
+    J.width = p->width;
+    J.height = p->height;
+    J.samples = p->samples;
+    J.max_bounces = p->max_bounces;
+    J.frame_index = p->frame_index;
+    J.sample_base = c->accumulated;
+    J.samples_per_item = std::min<uint32_t>(o.samples_per_item ? o.samples_per_item : 1u, p->samples);
+    J.items_per_pixel = (p->samples + J.samples_per_item - 1) / J.samples_per_item;
+    items += uint64_t(p->width) * p->height * J.items_per_pixel;
+    paths += uint64_t(p->width) * p->height * p->samples;
+  }
+  TC_CUDA(lead, upload(lead->batch_jobs, jobs.data(), jobs.size(), st));
+  tcb::RenderLaunch L{};
+  L.jobs = lead->batch_jobs.as<tcb::FrameJob>();
+  L.job_count = uint32_t(n);
+  L.total_items = items;
+  L.work_counter = lead->work_counter.as<unsigned long long>();
+  L.counters = lead->counters.as<unsigned long long>();
+  TC_CUDA(lead, cudaMemsetAsync(lead->work_counter.ptr, 0, sizeof(unsigned long long), st));
+  TC_CUDA(lead, cudaMemsetAsync(lead->counters.ptr, 0, 4 * sizeof(unsigned long long), st));
+  const int per_sm = tcb::render_batch_max_blocks_per_sm(block);
+  if (per_sm <= 0) return fail(lead, TC_ERR_CUDA, "batched render kernel cannot be resident with this block size");
+  TC_CUDA(lead, cudaEventRecord(lead->ev_kernel0, st));
+  TC_CUDA(lead, tcb::launch_render_batch(L, block, per_sm * lead->sm_count, st));
+  TC_CUDA(lead, cudaEventRecord(lead->ev_kernel1, st));
+  unsigned long long counters[4] = {0, 0, 0, 0};
+  TC_CUDA(lead, cudaMemcpyAsync(counters, lead->counters.ptr, sizeof(counters), cudaMemcpyDeviceToHost, st));
+  TC_CUDA(lead, cudaEventRecord(lead->ev_end, st));
+  TC_CUDA(lead, cudaStreamSynchronize(st));
+  for (size_t i = 0; i < n; ++i) contexts[i]->accumulated += params[i].samples;
+  lead->stats.paths = counters[0];
+  lead->stats.extension_rays = counters[1];
+  lead->stats.shadow_rays = counters[2];
+  lead->stats.rays = counters[1] + counters[2];
+  cudaEventElapsedTime(&lead->stats.kernel_ms, lead->ev_kernel0, lead->ev_kernel1);
+  cudaEventElapsedTime(&lead->stats.total_ms, lead->ev_begin, lead->ev_end);
+  if (counters[0] != paths)
+    return fail(lead, TC_ERR_DEVICE_STATUS, "batched path kernel completed " + std::to_string(counters[0]) + " of " +
+                                                std::to_string(paths) + " paths");
+  return TC_OK;
+}
+
 int tc_render_no_alloc(tc_context* ctx, const tc_gpu_render_params* p, double* sums, size_t n_doubles, void* stream) {
   if (!ctx) return fail(nullptr, TC_ERR_INVALID, "context is null");
   if (!p || !sums) return fail(ctx, TC_ERR_INVALID, "render params or sums buffer is null");
@@ -647,18 +848,18 @@ int tc_render_no_alloc(tc_context* ctx, const tc_gpu_render_params* p, double* s
   if (p->accumulated_samples == 0) TC_CUDA(ctx, cudaMemsetAsync(sums, 0, sizeof(double) * 3 * npix, st));
   TC_CUDA(ctx, cudaMemsetAsync(scratch, 0, 4 * sizeof(unsigned long long), st));
   tcb::RenderLaunch L{};
-  L.scene = ctx->scene;
-  L.width = p->width;
-  L.height = p->height;
-  L.samples = p->samples;
-  L.max_bounces = p->max_bounces;
-  L.frame_index = p->frame_index;
-  L.sample_base = p->accumulated_samples;
-  L.samples_per_item = 1u;
-  L.items_per_pixel = (p->samples + L.samples_per_item - 1) / L.samples_per_item;
-  L.total_items = npix * L.items_per_pixel;
-  L.accum = sums;
-  L.accum_sq = nullptr;
+  L.f.scene = ctx->scene;
+  L.f.width = p->width;
+  L.f.height = p->height;
+  L.f.samples = p->samples;
+  L.f.max_bounces = p->max_bounces;
+  L.f.frame_index = p->frame_index;
+  L.f.sample_base = p->accumulated_samples;
+  L.f.samples_per_item = 1u;
+  L.f.items_per_pixel = (p->samples + L.f.samples_per_item - 1) / L.f.samples_per_item;
+  L.total_items = npix * L.f.items_per_pixel;
+  L.f.accum = sums;
+  L.f.accum_sq = nullptr;
   L.work_counter = scratch;
   L.counters = scratch + 1;
   const int block = 128;
@@ -678,6 +879,34 @@ int tc_readback(tc_context* ctx, float* rgba, size_t n_floats) {
   TC_CUDA(ctx, tcb::launch_resolve(ctx->accum.as<double>(), uint32_t(npix), 1.0 / double(ctx->accumulated),
                                    ctx->image.as<float4>(), ctx->stream));
   TC_CUDA(ctx, cudaMemcpyAsync(rgba, ctx->image.ptr, sizeof(float4) * npix, cudaMemcpyDeviceToHost, ctx->stream));
+  TC_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return TC_OK;
+}
+
+int tc_display_rgba8_async(tc_context* ctx, float exposure_stops, void* d_rgba, size_t n_bytes, void* stream) {
+  if (!ctx) return fail(nullptr, TC_ERR_INVALID, "context is null");
+  if (!d_rgba) return fail(ctx, TC_ERR_INVALID, "output buffer is null");
+  if (ctx->accumulated == 0) return fail(ctx, TC_ERR_STATE, "display conversion before tc_render");
+  if (!std::isfinite(exposure_stops)) return fail(ctx, TC_ERR_INVALID, "exposure must be finite");
+  const size_t npix = size_t(ctx->width) * ctx->height;
+  if (n_bytes < 4 * npix) return fail(ctx, TC_ERR_INVALID, "output buffer holds fewer than 4*width*height bytes");
+  TC_CUDA(ctx, cudaSetDevice(ctx->device));
+  cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : ctx->stream;
+  TC_CUDA(ctx, tcb::launch_display_from_sums(ctx->accum.as<double>(), uint32_t(npix), 1.0 / double(ctx->accumulated),
+                                             exposure_stops, static_cast<uint32_t*>(d_rgba), st));
+  return TC_OK;
+}
+
+int tc_readback_rgba8(tc_context* ctx, float exposure_stops, uint8_t* rgba, size_t n_bytes) {
+  if (!ctx) return fail(nullptr, TC_ERR_INVALID, "context is null");
+  if (!rgba) return fail(ctx, TC_ERR_INVALID, "output buffer is null");
+  if (ctx->accumulated == 0) return fail(ctx, TC_ERR_STATE, "tc_readback_rgba8 before tc_render");
+  const size_t npix = size_t(ctx->width) * ctx->height;
+  if (n_bytes < 4 * npix) return fail(ctx, TC_ERR_INVALID, "output buffer holds fewer than 4*width*height bytes");
+  TC_CUDA(ctx, cudaSetDevice(ctx->device));
+  TC_CUDA(ctx, ctx->display.reserve(4 * npix));
+  if (int rc = tc_display_rgba8_async(ctx, exposure_stops, ctx->display.ptr, 4 * npix, nullptr)) return rc;
+  TC_CUDA(ctx, cudaMemcpyAsync(rgba, ctx->display.ptr, 4 * npix, cudaMemcpyDeviceToHost, ctx->stream));
   TC_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   return TC_OK;
 }
@@ -969,6 +1198,30 @@ int tc_guide_train_recorded(tc_context* ctx, uint32_t steps, uint32_t batch, flo
   cudaEventElapsedTime(&ctx->stats.kernel_ms, ctx->ev_kernel0, ctx->ev_kernel1);
   if (rc != TC_OK) return rc;
   if (losses && steps) std::memcpy(losses, step_loss.data(), sizeof(float) * steps);
+  return TC_OK;
+}
+
+int tc_guide_recorded_samples(tc_context* ctx, float* out, size_t n_floats, uint32_t* count) {
+  if (!ctx) return fail(nullptr, TC_ERR_INVALID, "context is null");
+  if (!ctx->has_records) return fail(ctx, TC_ERR_STATE, "no batch was rendered with guide_record = 1");
+  TC_CUDA(ctx, cudaSetDevice(ctx->device));
+  cudaStream_t st = ctx->stream;
+  TC_CUDA(ctx, ctx->rec_samples.reserve(sizeof(float4) * 3 * size_t(ctx->rec_capacity)));
+  TC_CUDA(ctx, ctx->rec_wsum.reserve(sizeof(float)));
+  TC_CUDA(ctx, cudaMemsetAsync(ctx->rec_wsum.ptr, 0, sizeof(float), st));
+  TC_CUDA(ctx, tcb::launch_guide_samples(ctx->rec_records.as<float4>(), ctx->rec_count.as<uint32_t>(), ctx->rec_capacity,
+                                         ctx->rec_path_rad.as<float4>(), ctx->rec_samples.as<float4>(),
+                                         ctx->rec_wsum.as<float>(), st));
+  uint32_t n = 0;
+  TC_CUDA(ctx, cudaMemcpyAsync(&n, ctx->rec_count.ptr, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+  TC_CUDA(ctx, cudaStreamSynchronize(st));
+  n = std::min(n, ctx->rec_capacity);
+  if (count) *count = n;
+  if (out) {
+    const size_t m = std::min<size_t>(n_floats / 12, n);
+    TC_CUDA(ctx, cudaMemcpyAsync(out, ctx->rec_samples.ptr, sizeof(float4) * 3 * m, cudaMemcpyDeviceToHost, st));
+    TC_CUDA(ctx, cudaStreamSynchronize(st));
+  }
   return TC_OK;
 }
 

@@ -13,7 +13,7 @@ namespace tcb {
 struct DevScene {
   const PairNode* pairs;
   const PrimRecord* prims;
-  ChildRec root;
+  const ChildRec* root;  // device memory: the root's bounds and link
   const DevMaterial* materials;
   uint32_t material_count;
   uint32_t light_count;
@@ -60,16 +60,25 @@ struct GuideLaunch {
 // Path kernel modes.
 enum RenderMode : int { kModePlain = 0, kModeRecord = 1, kModeGuided = 2 };
 
-struct RenderLaunch {
+// One independent frame: its scene, image and sample range. A single-frame launch carries it
+// inline (RenderLaunch::f); a batched launch reads one per job from device memory.
+struct FrameJob {
   DevScene scene;
+  double* accum;               // 3 doubles per pixel (running sums)
+  double* accum_sq;            // 3 doubles per pixel or null
+  uint64_t item_begin;         // batched launches: first global work item of this frame
   uint32_t width, height, samples, max_bounces;
   uint32_t frame_index;
   uint32_t sample_base;        // samples already accumulated (decorrelates progressive batches)
   uint32_t samples_per_item;   // samples a lane traces for one pixel before fetching new work
   uint32_t items_per_pixel;
+};
+
+struct RenderLaunch {
+  FrameJob f;                  // the frame of a single-frame launch
+  const FrameJob* jobs;        // batched launch: job_count frames in device memory (else null)
+  uint32_t job_count;
   uint64_t total_items;
-  double* accum;               // 3 doubles per pixel (running sums)
-  double* accum_sq;            // 3 doubles per pixel or null
   unsigned long long* work_counter;
   unsigned long long* counters;  // [0] paths, [1] extension rays, [2] shadow rays
   GuideLaunch g;
@@ -81,6 +90,9 @@ cudaError_t launch_trace_closest(const DevScene& s, const float* rays, uint64_t 
 cudaError_t launch_render(const RenderLaunch& r, int block_size, int grid_size, bool moments, cudaStream_t stream,
                           int mode = kModePlain);
 int render_max_blocks_per_sm(int block_size, bool moments, int mode = kModePlain);
+// Batched plain launch over r.jobs (r.job_count frames, items concatenated in job order).
+cudaError_t launch_render_batch(const RenderLaunch& r, int block_size, int grid_size, cudaStream_t stream);
+int render_batch_max_blocks_per_sm(int block_size);
 // Training samples (3 float4 each: position + weight, normal, direction) from recorded diffuse
 // scatters: weight = luminance of the radiance that arrived along the scattered direction.
 cudaError_t launch_guide_samples(const float4* records, const uint32_t* record_count, uint32_t capacity,

@@ -334,10 +334,21 @@ constexpr int kTrainSmem = kTrainDB + 224 * 4;
 // TMEM columns.
 constexpr uint32_t kColFwd = 0, kColDH = 64, kColDW4 = 128, kColDW3 = 192, kColDW2 = 256, kColDW1 = 320;
 
+// Bias gradient of one tile: column sums of the 128-row K-major BF16 dZ tile (the values the
+// weight-gradient MMA consumes), added to db. Thread c < k sums column c, so no atomics are needed.
+__device__ __forceinline__ void tile_column_sums(const uint8_t* tile, int k, float* db, int tid) {
+  if (tid >= k) return;
+  float acc[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+#pragma unroll 8
+  for (int r = 0; r < 128; ++r)
+    acc[r & 3] += __bfloat162float(*reinterpret_cast<const __nv_bfloat16*>(tile + kmajor_offset(r, tid, k)));
+  db[tid] += (acc[0] + acc[1]) + (acc[2] + acc[3]);
+}
+
 // Activation-gradient epilogue: dh (64 accumulator columns) -> dz = dh * [h > 0] -> BF16 row of the
-// dZ tile (K = 64), and the bias gradient in shared memory.
+// dZ tile (K = 64).
 __device__ __forceinline__ void epilogue_backward(uint32_t lane_tmem, const uint8_t* h_tile, uint8_t* dz_tile,
-                                                  float* db, int row) {
+                                                  int row) {
 #pragma unroll
   for (int c = 0; c < 64; c += 16) {
     float v[16];
@@ -351,8 +362,6 @@ __device__ __forceinline__ void epilogue_backward(uint32_t lane_tmem, const uint
 #pragma unroll
       for (int j = 0; j < 8; ++j) {
         r[j] = __bfloat162float(hb[j]) > 0.0f ? v[8 * hh + j] : 0.0f;
-        r[j] = __bfloat162float(__float2bfloat16_rn(r[j]));
-        atomicAdd(&db[c + 8 * hh + j], r[j]);
       }
       uint4 o;
       o.x = pack_bf16x2(r[0], r[1]);
@@ -464,10 +473,7 @@ __global__ void __launch_bounds__(128, 1) guide_train_kernel(const float4* __res
       for (int g = 0; g < 4; ++g) {
         float r[8];
 #pragma unroll
-        for (int j = 0; j < 8; ++j) {
-          r[j] = __bfloat162float(__float2bfloat16_rn(dy[8 * g + j]));
-          atomicAdd(&s_db[192 + 8 * g + j], r[j]);
-        }
+        for (int j = 0; j < 8; ++j) r[j] = dy[8 * g + j];
         uint4 o;
         o.x = pack_bf16x2(r[0], r[1]);
         o.y = pack_bf16x2(r[2], r[3]);
@@ -476,6 +482,8 @@ __global__ void __launch_bounds__(128, 1) guide_train_kernel(const float4* __res
         *reinterpret_cast<uint4*>(s_dz + kmajor_offset(tid, 8 * g, 32)) = o;
       }
     }
+    __syncthreads();
+    tile_column_sums(s_dz, 32, s_db + 192, tid);
     // Backward: dH3 = dY W4 and dW4 += dY^T H3.
     sync_for_mma();
     if (tid == 0) {
@@ -484,7 +492,9 @@ __global__ void __launch_bounds__(128, 1) guide_train_kernel(const float4* __res
       umma::commit(&mbar);
     }
     if (!wait_mma()) break;
-    epilogue_backward(tmem + lane + kColDH, s_h[2], s_dz, s_db + 128, tid);
+    epilogue_backward(tmem + lane + kColDH, s_h[2], s_dz, tid);
+    __syncthreads();
+    tile_column_sums(s_dz, 64, s_db + 128, tid);
     // dH2 = dZ3 W3, dW3 += dZ3^T H2.
     sync_for_mma();
     if (tid == 0) {
@@ -493,7 +503,9 @@ __global__ void __launch_bounds__(128, 1) guide_train_kernel(const float4* __res
       umma::commit(&mbar);
     }
     if (!wait_mma()) break;
-    epilogue_backward(tmem + lane + kColDH, s_h[1], s_dz, s_db + 64, tid);
+    epilogue_backward(tmem + lane + kColDH, s_h[1], s_dz, tid);
+    __syncthreads();
+    tile_column_sums(s_dz, 64, s_db + 64, tid);
     // dH1 = dZ2 W2, dW2 += dZ2^T H1.
     sync_for_mma();
     if (tid == 0) {
@@ -502,7 +514,9 @@ __global__ void __launch_bounds__(128, 1) guide_train_kernel(const float4* __res
       umma::commit(&mbar);
     }
     if (!wait_mma()) break;
-    epilogue_backward(tmem + lane + kColDH, s_h[0], s_dz, s_db, tid);
+    epilogue_backward(tmem + lane + kColDH, s_h[0], s_dz, tid);
+    __syncthreads();
+    tile_column_sums(s_dz, 64, s_db, tid);
     // dW1 += dZ1^T X.
     sync_for_mma();
     if (tid == 0) {

@@ -215,13 +215,16 @@ __device__ __forceinline__ float power_heuristic(float a, float b) {
 // ------------------------------------------------------------------------ parity kernel
 __global__ void trace_closest_kernel(const DevScene s, const float* __restrict__ rays, uint64_t n, float tmin,
                                      uint32_t* __restrict__ prim, float* __restrict__ tout) {
+  __shared__ ChildRec root;
+  if (threadIdx.x == 0) root = *s.root;
+  __syncthreads();
   const uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const float* r = rays + 6 * i;
   const RayQ q = make_ray(r[0], r[1], r[2], r[3], r[4], r[5]);
   TraceResult tr;
   uint32_t visits = 0;
-  const bool hit = trace_ray(s.pairs, s.prims, s.root, q, tmin, CUDART_INF_F, false, tr, visits);
+  const bool hit = trace_ray(s.pairs, s.prims, root, q, tmin, CUDART_INF_F, false, tr, visits);
   prim[i] = hit ? (tr.tag & ~kTagLast) : 0xFFFFFFFFu;
   tout[i] = hit ? tr.t : CUDART_INF_F;
 }
@@ -253,8 +256,16 @@ struct Lane {
   bool include_emission;
   uint32_t pixel, item_samples, item_done, sample;
   int mix_slot;      // guided mode: decoded mixture of the current diffuse vertex, or -1
+  uint32_t job;      // batched launch: frame of the current work item
   Pcg rng;
 };
+
+// The frame a lane works on: the launch's own (single-frame) or its job's (batched).
+template <bool kBatch>
+__device__ __forceinline__ const FrameJob& frame_of(const RenderLaunch& L, const Lane& ln) {
+  if constexpr (kBatch) return L.jobs[ln.job];
+  else return L.f;
+}
 
 // ------------------------------------------------------------------------ guiding mixture
 // Decoded 8-lobe von Mises-Fisher mixture: mix[j] = (mu.xyz, kappa), mix[8..9] = weights.
@@ -311,12 +322,12 @@ __device__ __forceinline__ uint32_t aggregated_increment(uint32_t* counter) {
   return base + uint32_t(__popc(active & ((1u << lane) - 1u)));
 }
 
-__device__ __forceinline__ void start_sample(const RenderLaunch& L, Lane& ln) {
-  const DevScene& s = L.scene;
-  ln.rng.seed(L.frame_index, ln.pixel, ln.sample);
-  const uint32_t x = ln.pixel % L.width, y = ln.pixel / L.width;
-  const float u = (float(x) + ln.rng.uniform()) / float(L.width);
-  const float v = 1.0f - (float(y) + ln.rng.uniform()) / float(L.height);
+__device__ __forceinline__ void start_sample(const FrameJob& J, Lane& ln) {
+  const DevScene& s = J.scene;
+  ln.rng.seed(J.frame_index, ln.pixel, ln.sample);
+  const uint32_t x = ln.pixel % J.width, y = ln.pixel / J.width;
+  const float u = (float(x) + ln.rng.uniform()) / float(J.width);
+  const float v = 1.0f - (float(y) + ln.rng.uniform()) / float(J.height);
   const V3 o = mk(s.cam_origin[0], s.cam_origin[1], s.cam_origin[2]);
   const V3 ll = mk(s.cam_lower_left[0], s.cam_lower_left[1], s.cam_lower_left[2]);
   const V3 h = mk(s.cam_horizontal[0], s.cam_horizontal[1], s.cam_horizontal[2]);
@@ -325,7 +336,7 @@ __device__ __forceinline__ void start_sample(const RenderLaunch& L, Lane& ln) {
   ln.rd = normalize(ll + u * h + v * vv - o);
   ln.thr = mk(1.f, 1.f, 1.f);
   ln.rad = mk(0.f, 0.f, 0.f);
-  ln.depth = int(L.max_bounces);
+  ln.depth = int(J.max_bounces);
   ln.include_emission = true;
   ln.bsdf_pdf = -1.0f;
   ln.mix_slot = -1;
@@ -333,9 +344,9 @@ __device__ __forceinline__ void start_sample(const RenderLaunch& L, Lane& ln) {
 }
 
 template <int kMode, bool kMoments>
-__device__ __forceinline__ void finish_sample(const RenderLaunch& L, Lane& ln, uint32_t& n_paths) {
+__device__ __forceinline__ void finish_sample(const RenderLaunch& L, const FrameJob& J, Lane& ln, uint32_t& n_paths) {
   if constexpr (kMode == kModeRecord) {
-    const uint32_t path = (ln.sample - L.sample_base) * (L.width * L.height) + ln.pixel;
+    const uint32_t path = (ln.sample - J.sample_base) * (J.width * J.height) + ln.pixel;
     L.g.path_radiance[path] = make_float4(ln.rad.x, ln.rad.y, ln.rad.z, 0.0f);
   }
   ln.acc = ln.acc + ln.rad;
@@ -344,19 +355,19 @@ __device__ __forceinline__ void finish_sample(const RenderLaunch& L, Lane& ln, u
   ++ln.item_done;
   ++ln.sample;
   if (ln.item_done >= ln.item_samples) {
-    double* a = L.accum + size_t(3) * ln.pixel;
+    double* a = J.accum + size_t(3) * ln.pixel;
     atomicAdd(a, double(ln.acc.x));
     atomicAdd(a + 1, double(ln.acc.y));
     atomicAdd(a + 2, double(ln.acc.z));
     if (kMoments) {
-      double* q = L.accum_sq + size_t(3) * ln.pixel;
+      double* q = J.accum_sq + size_t(3) * ln.pixel;
       atomicAdd(q, double(ln.acc2.x));
       atomicAdd(q + 1, double(ln.acc2.y));
       atomicAdd(q + 2, double(ln.acc2.z));
     }
     ln.phase = kIdle;
   } else {
-    start_sample(L, ln);
+    start_sample(J, ln);
   }
 }
 
@@ -400,8 +411,8 @@ __device__ __forceinline__ bool prepare_light_shadow(const DevScene& s, Lane& ln
 // Environment-sampling shadow ray with the power heuristic (integrator.rs:208-244). At a guided
 // vertex the competing technique is the 50/50 BSDF / guide mixture, so its pdf enters the weight.
 template <int kMode>
-__device__ __forceinline__ bool prepare_env_shadow(const RenderLaunch& L, Lane& ln) {
-  const DevScene& s = L.scene;
+__device__ __forceinline__ bool prepare_env_shadow(const RenderLaunch& L, const FrameJob& J, Lane& ln) {
+  const DevScene& s = J.scene;
   if (s.background != 2u || !s.env_sampleable) return false;
   const float u1 = ln.rng.uniform(), u2 = ln.rng.uniform(), u3 = ln.rng.uniform();
   V3 dir, rad;
@@ -472,8 +483,9 @@ __device__ __forceinline__ void resume_path(const RenderLaunch& L, Lane& ln, uin
 }
 
 template <int kMode, bool kMoments>
-__device__ __forceinline__ void shade_hit(const RenderLaunch& L, Lane& ln, const TraceResult& tr, uint32_t& n_paths) {
-  const DevScene& s = L.scene;
+__device__ __forceinline__ void shade_hit(const RenderLaunch& L, const FrameJob& J, Lane& ln, const TraceResult& tr,
+                                          uint32_t& n_paths) {
+  const DevScene& s = J.scene;
   const float4* p = reinterpret_cast<const float4*>(s.prims + tr.rec);
   const float4 A = __ldg(p), B = __ldg(p + 1);
   const V3 hp = ln.ro + ln.rd * tr.t;
@@ -520,7 +532,7 @@ __device__ __forceinline__ void shade_hit(const RenderLaunch& L, Lane& ln, const
   const DevMaterial m = s.materials[mat];
   if (m.kind == kEmissive) {
     if (ln.include_emission) ln.rad = ln.rad + ln.thr * mk(m.emission[0], m.emission[1], m.emission[2]);
-    finish_sample<kMode, kMoments>(L, ln, n_paths);
+    finish_sample<kMode, kMoments>(L, J, ln, n_paths);
     return;
   }
   if (m.kind == kDiffuse) {
@@ -543,7 +555,7 @@ __device__ __forceinline__ void shade_hit(const RenderLaunch& L, Lane& ln, const
     const V3 ball = uniform_ball(ln.rng.uniform(), ln.rng.uniform(), ln.rng.uniform());
     const V3 dir = refl + ball * m.roughness;
     if (dot(dir, nrm) <= 0.0f) {
-      finish_sample<kMode, kMoments>(L, ln, n_paths);
+      finish_sample<kMode, kMoments>(L, J, ln, n_paths);
       return;
     }
     ln.ro = hp;
@@ -567,14 +579,22 @@ __device__ __forceinline__ void shade_hit(const RenderLaunch& L, Lane& ln, const
   ln.phase = kExtend;
 }
 
-template <int kMode, bool kMoments>
+template <int kMode, bool kMoments, bool kBatch>
 __global__ void __launch_bounds__(256) render_kernel(const RenderLaunch L) {
-  const DevScene& s = L.scene;
+  static_assert(!kBatch || kMode == kModePlain, "batched launches trace plain paths");
+  // The root record lives in device memory (a geometry refit rewrites it between launches);
+  // single-frame launches stage it in shared memory once.
+  __shared__ ChildRec root;
+  if constexpr (!kBatch) {
+    if (threadIdx.x == 0) root = *L.f.scene.root;
+    __syncthreads();
+  }
   const unsigned lane = threadIdx.x & 31u;
-  const uint32_t npix = L.width * L.height;
+  const uint32_t npix = L.f.width * L.f.height;  // single-frame launches
   Lane ln;
   ln.phase = kIdle;
   ln.mix_slot = -1;
+  ln.job = 0;
   ln.acc = ln.acc2 = mk(0.f, 0.f, 0.f);
   bool finished = false;
   uint32_t n_paths = 0, n_ext = 0, n_shadow = 0, node_visits = 0;
@@ -607,21 +627,37 @@ __global__ void __launch_bounds__(256) render_kernel(const RenderLaunch L) {
           ln.sample = L.g.wave_first_sample + k;
           ln.acc = mk(0.f, 0.f, 0.f);
           if (kMoments) ln.acc2 = mk(0.f, 0.f, 0.f);
-          start_sample(L, ln);
+          start_sample(L.f, ln);
         } else {
-          const uint32_t chunk = uint32_t(item / npix);
-          ln.pixel = uint32_t(item - uint64_t(chunk) * npix);
-          const uint32_t first = chunk * L.samples_per_item;
-          ln.item_samples = min(L.samples_per_item, L.samples - first);
+          uint64_t local = item;
+          if constexpr (kBatch) {
+            // The job whose item range holds this item (item_begin ascends with the job index).
+            uint32_t lo = 0, hi = L.job_count - 1;
+            while (lo < hi) {
+              const uint32_t mid = (lo + hi + 1) >> 1;
+              if (L.jobs[mid].item_begin <= item) lo = mid;
+              else hi = mid - 1;
+            }
+            ln.job = lo;
+            local = item - L.jobs[lo].item_begin;
+          }
+          const FrameJob& J = frame_of<kBatch>(L, ln);
+          const uint32_t fpix = J.width * J.height;
+          const uint32_t chunk = uint32_t(local / fpix);
+          ln.pixel = uint32_t(local - uint64_t(chunk) * fpix);
+          const uint32_t first = chunk * J.samples_per_item;
+          ln.item_samples = min(J.samples_per_item, J.samples - first);
           ln.item_done = 0;
-          ln.sample = L.sample_base + first;
+          ln.sample = J.sample_base + first;
           ln.acc = mk(0.f, 0.f, 0.f);
           if (kMoments) ln.acc2 = mk(0.f, 0.f, 0.f);
-          start_sample(L, ln);
+          start_sample(J, ln);
         }
       }
     }
     if (__all_sync(0xffffffffu, finished)) break;
+    const FrameJob& J = frame_of<kBatch>(L, ln);
+    const DevScene& s = J.scene;
 
     // Advance the lane's state machine to its next ray.
     bool have = false;
@@ -630,7 +666,7 @@ __global__ void __launch_bounds__(256) render_kernel(const RenderLaunch L) {
       switch (ln.phase) {
         case kExtend:
           if (ln.depth <= 0) {
-            finish_sample<kMode, kMoments>(L, ln, n_paths);
+            finish_sample<kMode, kMoments>(L, J, ln, n_paths);
           } else {
             have = true;
             any_hit = false;
@@ -642,13 +678,13 @@ __global__ void __launch_bounds__(256) render_kernel(const RenderLaunch L) {
           else ln.phase = kShadowEnv;
           break;
         case kShadowEnv:
-          if (prepare_env_shadow<kMode>(L, ln)) { have = true; any_hit = true; }
+          if (prepare_env_shadow<kMode>(L, J, ln)) { have = true; any_hit = true; }
           else ln.phase = kScatter;
           break;
         default: {  // kScatter: cosine-weighted diffuse bounce (integrator.rs:277-289)
           ln.depth -= 1;
           if (ln.depth <= 0) {
-            finish_sample<kMode, kMoments>(L, ln, n_paths);
+            finish_sample<kMode, kMoments>(L, J, ln, n_paths);
             break;
           }
           if constexpr (kMode == kModeGuided) {
@@ -669,7 +705,7 @@ __global__ void __launch_bounds__(256) render_kernel(const RenderLaunch L) {
               const float cs = dot(ln.hn, dir);
               ln.mix_slot = -1;
               if (!(cs > 0.0f)) {
-                finish_sample<kMode, kMoments>(L, ln, n_paths);
+                finish_sample<kMode, kMoments>(L, J, ln, n_paths);
                 break;
               }
               const float p = 0.5f * cs / kPiF + 0.5f * mix_pdf(mix, dir);
@@ -688,7 +724,7 @@ __global__ void __launch_bounds__(256) render_kernel(const RenderLaunch L) {
           if constexpr (kMode == kModeRecord) {
             const uint32_t slot = aggregated_increment(L.g.record_count);
             if (slot < L.g.record_capacity) {
-              const uint32_t path = (ln.sample - L.sample_base) * npix + ln.pixel;
+              const uint32_t path = (ln.sample - J.sample_base) * npix + ln.pixel;
               const V3 t = ln.thr * ln.alb;
               float4* r = L.g.records + 4 * size_t(slot);
               r[0] = make_float4(ln.hp.x, ln.hp.y, ln.hp.z, __uint_as_float(path));
@@ -712,7 +748,12 @@ __global__ void __launch_bounds__(256) render_kernel(const RenderLaunch L) {
     bool hit = false;
     if (have) {
       const RayQ q = make_ray(ln.ro.x, ln.ro.y, ln.ro.z, ln.rd.x, ln.rd.y, ln.rd.z);
-      hit = trace_ray(s.pairs, s.prims, s.root, q, kRayEps, ln.tmax, any_hit, tr, node_visits);
+      if constexpr (kBatch) {
+        const ChildRec rt = *s.root;
+        hit = trace_ray(s.pairs, s.prims, rt, q, kRayEps, ln.tmax, any_hit, tr, node_visits);
+      } else {
+        hit = trace_ray(s.pairs, s.prims, root, q, kRayEps, ln.tmax, any_hit, tr, node_visits);
+      }
       if (ln.phase == kShadowLight) {
         ++n_shadow;
         if (!hit) ln.rad = ln.rad + ln.pend;
@@ -725,9 +766,9 @@ __global__ void __launch_bounds__(256) render_kernel(const RenderLaunch L) {
         ++n_ext;
         if (!hit) {
           ln.rad = ln.rad + ln.thr * background(s, ln.rd, ln.bsdf_pdf);
-          finish_sample<kMode, kMoments>(L, ln, n_paths);
+          finish_sample<kMode, kMoments>(L, J, ln, n_paths);
         } else {
-          shade_hit<kMode, kMoments>(L, ln, tr, n_paths);
+          shade_hit<kMode, kMoments>(L, J, ln, tr, n_paths);
         }
       }
     }
@@ -746,9 +787,22 @@ __global__ void __launch_bounds__(256) render_kernel(const RenderLaunch L) {
 
 template <int kMode>
 static cudaError_t launch_mode(const RenderLaunch& r, int block_size, int grid_size, bool moments, cudaStream_t stream) {
-  if (moments) render_kernel<kMode, true><<<grid_size, block_size, 0, stream>>>(r);
-  else render_kernel<kMode, false><<<grid_size, block_size, 0, stream>>>(r);
+  if (moments) render_kernel<kMode, true, false><<<grid_size, block_size, 0, stream>>>(r);
+  else render_kernel<kMode, false, false><<<grid_size, block_size, 0, stream>>>(r);
   return cudaGetLastError();
+}
+
+cudaError_t launch_render_batch(const RenderLaunch& r, int block_size, int grid_size, cudaStream_t stream) {
+  if (!r.jobs || r.job_count == 0) return cudaErrorInvalidValue;
+  render_kernel<kModePlain, false, true><<<grid_size, block_size, 0, stream>>>(r);
+  return cudaGetLastError();
+}
+
+int render_batch_max_blocks_per_sm(int block_size) {
+  int blocks = 0;
+  const cudaError_t e =
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, render_kernel<kModePlain, false, true>, block_size, 0);
+  return e == cudaSuccess ? blocks : 0;
 }
 
 cudaError_t launch_render(const RenderLaunch& r, int block_size, int grid_size, bool moments, cudaStream_t stream,
@@ -762,8 +816,8 @@ template <int kMode>
 static int blocks_for(int block_size, bool moments) {
   int blocks = 0;
   cudaError_t e = moments
-      ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, render_kernel<kMode, true>, block_size, 0)
-      : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, render_kernel<kMode, false>, block_size, 0);
+      ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, render_kernel<kMode, true, false>, block_size, 0)
+      : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, render_kernel<kMode, false, false>, block_size, 0);
   return e == cudaSuccess ? blocks : 0;
 }
 

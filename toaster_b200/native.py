@@ -48,6 +48,11 @@ EXPORTED_SYMBOLS = (
     "tc_guide_train",
     "tc_render_no_alloc",
     "tc_guide_train_recorded",
+    "tc_update_geometry",
+    "tc_readback_rgba8",
+    "tc_display_rgba8_async",
+    "tc_render_batch",
+    "tc_guide_recorded_samples",
 )
 
 GUIDE_PARAMS = 15584
@@ -59,6 +64,13 @@ class TcError(RuntimeError):
     def __init__(self, code: int, message: str):
         super().__init__(f"toaster_cuda error {code}: {message}")
         self.code = code
+
+
+class SceneChanges(ctypes.Structure):
+    """tc_scene_changes: toaster_scene::SceneChanges (evaluation.rs:9-18)."""
+
+    _fields_ = [("camera", ctypes.c_uint32), ("spheres", ctypes.c_uint32), ("triangles", ctypes.c_uint32),
+                ("emissive_geometry", ctypes.c_uint32)]
 
 
 class SceneData(ctypes.Structure):
@@ -149,6 +161,11 @@ def load_library(path: os.PathLike | None = None) -> ctypes.CDLL:
     lib.tc_render_no_alloc.argtypes = [vp, vp, vp, sz, vp]
     lib.tc_guide_train_recorded.argtypes = [vp, u32, u32, f32, ctypes.c_uint64, vp, ctypes.POINTER(u32)]
     lib.tc_guide_train.argtypes = [vp, vp, sz, u32, u32, f32, ctypes.c_uint64, vp]
+    lib.tc_update_geometry.argtypes = [vp, ctypes.POINTER(SceneData), ctypes.POINTER(SceneChanges)]
+    lib.tc_readback_rgba8.argtypes = [vp, f32, vp, sz]
+    lib.tc_display_rgba8_async.argtypes = [vp, f32, vp, sz, vp]
+    lib.tc_render_batch.argtypes = [ctypes.POINTER(vp), vp, sz, ctypes.POINTER(RenderOptions)]
+    lib.tc_guide_recorded_samples.argtypes = [vp, vp, sz, ctypes.POINTER(u32)]
     for name in EXPORTED_SYMBOLS:
         if not hasattr(lib, name):
             raise RuntimeError(f"{p} does not export {name}")

@@ -20,6 +20,38 @@ from . import native
 from .scene import Scene, SceneGpuData, scene_to_gpu
 
 
+def render_batch(renderers, samples=None, frame_index: int = 0, accumulate: bool = False, block_size: int = 0,
+                 samples_per_item: int = 0) -> dict:
+    """One persistent launch over the uploaded scenes of several renderers (same device).
+
+    ``samples`` may be one count or one per renderer. Returns the batch's stats (paths, rays,
+    kernel and total milliseconds)."""
+    if not renderers:
+        raise ValueError("empty batch")
+    lib = renderers[0]._lib
+    n = len(renderers)
+    spp = samples if isinstance(samples, (list, tuple)) else [samples] * n
+    params = np.zeros(n, gt.RENDER_PARAMS)
+    for i, r in enumerate(renderers):
+        if r._params is None:
+            raise RuntimeError("render before upload")
+        p = r._params.copy()
+        if spp[i] is not None:
+            p["samples"] = spp[i]
+        p["frame_index"] = frame_index
+        p["accumulated_samples"] = r.accumulated if accumulate else 0
+        params[i] = p[0] if p.shape else p
+    ctxs = (ctypes.c_void_p * n)(*[r._ctx for r in renderers])
+    opts = native.RenderOptions()
+    opts.block_size = block_size
+    opts.samples_per_item = samples_per_item
+    native.check(lib, renderers[0]._ctx, lib.tc_render_batch(ctxs, params.ctypes.data, n, ctypes.byref(opts)))
+    for i, r in enumerate(renderers):
+        r.width, r.height = int(params[i]["width"]), int(params[i]["height"])
+        r.accumulated = (r.accumulated if accumulate else 0) + int(params[i]["samples"])
+    return renderers[0].stats()
+
+
 def progressive_batch(requested_samples: int, accumulated_samples: int, target_samples: int) -> Optional[int]:
     """Next batch clamped to the remaining target, or None when complete (path_tracer.rs:900-923)."""
     if requested_samples <= 0:
@@ -71,8 +103,9 @@ class GpuRenderer:
     def _check(self, code: int) -> None:
         native.check(self._lib, self._ctx, code)
 
-    def upload(self, data: SceneGpuData) -> None:
-        """Copies packed scene records to the device and builds hierarchy and sampling tables."""
+    @staticmethod
+    def _scene_struct(data: SceneGpuData):
+        """tc_scene_data over the packed arrays; the arrays kept alive are returned beside it."""
         sd = native.SceneData()
         ctypes.memmove(sd.params, data.params.ctypes.data, 96)
         ctypes.memmove(sd.camera, data.camera.ctypes.data, 64)
@@ -97,9 +130,21 @@ class GpuRenderer:
             env = np.ascontiguousarray(data.environment_pixels, np.float32).reshape(-1, 4)
             keep.append(env)
             sd.environment_pixels, sd.environment_pixel_count = env.ctypes.data, env.shape[0]
+        return sd, keep
+
+    def upload(self, data: SceneGpuData) -> None:
+        """Copies packed scene records to the device and builds hierarchy and sampling tables."""
+        sd, keep = self._scene_struct(data)
         self._check(self._lib.tc_upload_scene(self._ctx, ctypes.byref(sd)))
         self._params = data.params.copy()
         self.accumulated = 0
+
+    def update_geometry(self, data: SceneGpuData, camera: bool = False, spheres: bool = True, triangles: bool = True,
+                        emissive_geometry: bool = False) -> None:
+        """Per-frame update: copies changed geometry and refits the hierarchy on the device."""
+        sd, keep = self._scene_struct(data)
+        ch = native.SceneChanges(int(camera), int(spheres), int(triangles), int(emissive_geometry))
+        self._check(self._lib.tc_update_geometry(self._ctx, ctypes.byref(sd), ctypes.byref(ch)))
 
     def set_stream(self, stream: int) -> None:
         """Enqueue on a caller-owned cudaStream_t (0 = the context's own stream)."""
@@ -143,6 +188,17 @@ class GpuRenderer:
             out = np.empty((self.height, self.width, 4), np.float32)
         self._check(self._lib.tc_readback(self._ctx, out.ctypes.data, out.size))
         return out
+
+    def readback_rgba8(self, exposure_stops: float = 0.0, out: Optional[np.ndarray] = None) -> np.ndarray:
+        """Display image (height, width, 4) uint8: exposure, ACES fitted, sRGB, converted on the device."""
+        if out is None:
+            out = np.empty((self.height, self.width, 4), np.uint8)
+        self._check(self._lib.tc_readback_rgba8(self._ctx, float(exposure_stops), out.ctypes.data, out.nbytes))
+        return out
+
+    def display_rgba8_device(self, exposure_stops: float, d_out: int, nbytes: int, stream: int = 0) -> None:
+        """Display conversion into caller-owned device memory, enqueued without synchronising."""
+        self._check(self._lib.tc_display_rgba8_async(self._ctx, float(exposure_stops), d_out, nbytes, stream or None))
 
     def readback_sums(self, moments: bool = False):
         """FP64 per-pixel sums (and sums of squares when kept) plus the sample count."""
@@ -216,6 +272,14 @@ class GpuRenderer:
         self._check(self._lib.tc_guide_train_recorded(self._ctx, steps, batch, lr, seed, losses.ctypes.data,
                                                       ctypes.byref(n)))
         return losses[:steps], int(n.value)
+
+    def guide_recorded_samples(self) -> np.ndarray:
+        """Training samples of the last guide_record batch: (n, 12) position + weight, normal, direction."""
+        count = ctypes.c_uint32()
+        self._check(self._lib.tc_guide_recorded_samples(self._ctx, None, 0, ctypes.byref(count)))
+        out = np.empty((count.value, 12), np.float32)
+        self._check(self._lib.tc_guide_recorded_samples(self._ctx, out.ctypes.data, out.size, ctypes.byref(count)))
+        return out
 
     def stats(self) -> dict:
         s = native.Stats()
