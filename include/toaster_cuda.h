@@ -294,17 +294,19 @@ int tc_guide_train(tc_context* ctx, const float* samples, size_t n, uint32_t ste
 
 /* Builds training samples from the diffuse scatters recorded by the last tc_render with
  * guide_record = 1 (weight = luminance of the radiance that arrived along each scattered
- * direction, normalised by its mean and clamped at 50x the mean) and runs `steps` Adam steps on
- * batches of `batch` samples drawn at random. losses (optional) receives one value per step and
- * n_samples (optional) the number of samples. */
+ * direction, normalised by its mean and clamped at 50x the mean; directions that carried no
+ * radiance are dropped, as they add nothing to the weighted likelihood) and runs `steps` Adam
+ * steps on batches of `batch` samples drawn at random. losses (optional) receives one value per
+ * step and n_samples (optional) the number of samples. */
 int tc_guide_train_recorded(tc_context* ctx, uint32_t steps, uint32_t batch, float lr, uint64_t seed, float* losses,
                             uint32_t* n_samples);
 
 /* The training samples derived from the last guide_record batch, as tc_guide_train_recorded
  * sees them: 12 floats each (position + weight, normal + 0, direction + 0), weight = luminance of
- * the radiance that arrived along the recorded direction. Writes min(count, n_floats / 12)
- * samples; *count receives the number recorded. out may be NULL to query the count. No
- * reference counterpart (inspection of the guiding data). */
+ * the radiance that arrived along the recorded direction. Only directions that carried radiance
+ * are kept (in an unspecified order). Writes min(count, n_floats / 12) samples; *count receives
+ * their number. out may be NULL to query the count. No reference counterpart (inspection of the
+ * guiding data). */
 int tc_guide_recorded_samples(tc_context* ctx, float* out, size_t n_floats, uint32_t* count);
 
 /* Tensor-core self-test (no reference counterpart): one 128 x n tile D = A * B^T with bf16 A

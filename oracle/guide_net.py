@@ -4,8 +4,8 @@ The reference renderer has no guiding; this restates, in plain NumPy, exactly wh
 kernels of toaster_b200/csrc/guide.cu compute, so that their forward outputs and gradients can
 be checked:
 
-  encoding   q = (p - centre) * scale; for axis i and frequency k in 0..11:
-             enc[24 i + 2 k] = sin(pi 2^k q_i), enc[24 i + 2 k + 1] = cos(pi 2^k q_i);
+  encoding   q = (p - centre) * scale; for axis i and frequency f_k = 2^(k/2), k in 0..11:
+             enc[24 i + 2 k] = sin(pi f_k q_i), enc[24 i + 2 k + 1] = cos(pi f_k q_i);
              enc[72:75] = normal; enc[75:80] = 0                               (80 inputs, bf16)
   network    h1 = relu(W1 x + b1), h2 = relu(W2 h1 + b2), h3 = relu(W3 h2 + b3), y = W4 h3 + b4
              with bf16 inputs/activations, FP32 accumulation and FP32 biases
@@ -26,6 +26,7 @@ SHAPES = [("W1", (N_HID, N_IN)), ("b1", (N_HID,)), ("W2", (N_HID, N_HID)), ("b2"
           ("W3", (N_HID, N_HID)), ("b3", (N_HID,)), ("W4", (N_OUT, N_HID)), ("b4", (N_OUT,))]
 N_PARAMS = sum(int(np.prod(s)) for _, s in SHAPES)
 KAPPA_LO, KAPPA_HI = -2.0, 7.0
+FREQS = np.float32(2.0) ** (np.arange(N_FREQ, dtype=np.float32) / np.float32(2.0))  # f32 values the kernels use
 
 
 def bf16(x):
@@ -70,7 +71,7 @@ def encode(points, normals, centre, scale):
     enc = np.zeros((n, N_IN), np.float64)
     for i in range(3):
         for k in range(N_FREQ):
-            ang = np.pi * (2.0 ** k) * q[:, i]
+            ang = np.pi * FREQS[k] * q[:, i]
             enc[:, 24 * i + 2 * k] = np.sin(ang)
             enc[:, 24 * i + 2 * k + 1] = np.cos(ang)
     enc[:, 72:75] = normals

@@ -665,7 +665,7 @@ int tc_render(tc_context* ctx, const tc_gpu_render_params* p, const tc_render_op
     // One record per diffuse scatter (capped) and the final radiance of every path of the batch.
     const uint64_t paths = uint64_t(npix) * p->samples;
     if (paths > (1ull << 31)) return fail(ctx, TC_ERR_INVALID, "too many paths to record in one batch");
-    ctx->rec_capacity = uint32_t(std::min<uint64_t>(2 * paths, uint64_t(1) << 23));
+    ctx->rec_capacity = uint32_t(std::min<uint64_t>(2 * paths, uint64_t(1) << 25));
     TC_CUDA(ctx, ctx->rec_records.reserve(sizeof(float4) * 4 * size_t(ctx->rec_capacity)));
     TC_CUDA(ctx, ctx->rec_count.reserve(sizeof(uint32_t)));
     TC_CUDA(ctx, ctx->rec_path_rad.reserve(sizeof(float4) * size_t(paths)));
@@ -1152,6 +1152,26 @@ int tc_guide_train(tc_context* ctx, const float* samples, size_t n, uint32_t ste
   return TC_OK;
 }
 
+// Positive-weight training samples of the last recorded batch into rec_samples; their number and
+// weight sum come back to the host.
+static int prepare_training_samples(tc_context* ctx, uint32_t* count, float* wsum) {
+  cudaStream_t st = ctx->stream;
+  TC_CUDA(ctx, ctx->rec_samples.reserve(sizeof(float4) * 3 * size_t(ctx->rec_capacity)));
+  TC_CUDA(ctx, ctx->rec_wsum.reserve(2 * sizeof(uint32_t)));
+  TC_CUDA(ctx, cudaMemsetAsync(ctx->rec_wsum.ptr, 0, 2 * sizeof(uint32_t), st));
+  float* d_wsum = ctx->rec_wsum.as<float>();
+  uint32_t* d_count = reinterpret_cast<uint32_t*>(d_wsum + 1);
+  TC_CUDA(ctx, tcb::launch_guide_samples(ctx->rec_records.as<float4>(), ctx->rec_count.as<uint32_t>(), ctx->rec_capacity,
+                                         ctx->rec_path_rad.as<float4>(), ctx->rec_samples.as<float4>(), d_count,
+                                         d_wsum, st));
+  uint32_t host[2] = {0, 0};
+  TC_CUDA(ctx, cudaMemcpyAsync(host, ctx->rec_wsum.ptr, sizeof(host), cudaMemcpyDeviceToHost, st));
+  TC_CUDA(ctx, cudaStreamSynchronize(st));
+  std::memcpy(wsum, &host[0], sizeof(float));
+  *count = std::min(host[1], ctx->rec_capacity);
+  return TC_OK;
+}
+
 int tc_guide_train_recorded(tc_context* ctx, uint32_t steps, uint32_t batch, float lr, uint64_t seed, float* losses,
                             uint32_t* n_samples) {
   if (!ctx) return fail(nullptr, TC_ERR_INVALID, "context is null");
@@ -1160,19 +1180,10 @@ int tc_guide_train_recorded(tc_context* ctx, uint32_t steps, uint32_t batch, flo
   if (batch == 0) return fail(ctx, TC_ERR_INVALID, "batch must be positive");
   TC_CUDA(ctx, cudaSetDevice(ctx->device));
   cudaStream_t st = ctx->stream;
-  TC_CUDA(ctx, ctx->rec_samples.reserve(sizeof(float4) * 3 * size_t(ctx->rec_capacity)));
-  TC_CUDA(ctx, ctx->rec_wsum.reserve(sizeof(float)));
-  TC_CUDA(ctx, cudaMemsetAsync(ctx->rec_wsum.ptr, 0, sizeof(float), st));
   TC_CUDA(ctx, cudaEventRecord(ctx->ev_kernel0, st));
-  TC_CUDA(ctx, tcb::launch_guide_samples(ctx->rec_records.as<float4>(), ctx->rec_count.as<uint32_t>(), ctx->rec_capacity,
-                                         ctx->rec_path_rad.as<float4>(), ctx->rec_samples.as<float4>(),
-                                         ctx->rec_wsum.as<float>(), st));
   uint32_t count = 0;
   float wsum = 0.0f;
-  TC_CUDA(ctx, cudaMemcpyAsync(&count, ctx->rec_count.ptr, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
-  TC_CUDA(ctx, cudaMemcpyAsync(&wsum, ctx->rec_wsum.ptr, sizeof(float), cudaMemcpyDeviceToHost, st));
-  TC_CUDA(ctx, cudaStreamSynchronize(st));
-  count = std::min(count, ctx->rec_capacity);
+  if (int rc = prepare_training_samples(ctx, &count, &wsum)) return rc;
   if (n_samples) *n_samples = count;
   if (count == 0 || !(wsum > 0.0f)) return fail(ctx, TC_ERR_STATE, "the recorded batch carries no radiance to learn from");
   const float mean = wsum / float(count);
@@ -1206,16 +1217,9 @@ int tc_guide_recorded_samples(tc_context* ctx, float* out, size_t n_floats, uint
   if (!ctx->has_records) return fail(ctx, TC_ERR_STATE, "no batch was rendered with guide_record = 1");
   TC_CUDA(ctx, cudaSetDevice(ctx->device));
   cudaStream_t st = ctx->stream;
-  TC_CUDA(ctx, ctx->rec_samples.reserve(sizeof(float4) * 3 * size_t(ctx->rec_capacity)));
-  TC_CUDA(ctx, ctx->rec_wsum.reserve(sizeof(float)));
-  TC_CUDA(ctx, cudaMemsetAsync(ctx->rec_wsum.ptr, 0, sizeof(float), st));
-  TC_CUDA(ctx, tcb::launch_guide_samples(ctx->rec_records.as<float4>(), ctx->rec_count.as<uint32_t>(), ctx->rec_capacity,
-                                         ctx->rec_path_rad.as<float4>(), ctx->rec_samples.as<float4>(),
-                                         ctx->rec_wsum.as<float>(), st));
   uint32_t n = 0;
-  TC_CUDA(ctx, cudaMemcpyAsync(&n, ctx->rec_count.ptr, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
-  TC_CUDA(ctx, cudaStreamSynchronize(st));
-  n = std::min(n, ctx->rec_capacity);
+  float wsum = 0.0f;
+  if (int rc = prepare_training_samples(ctx, &n, &wsum)) return rc;
   if (count) *count = n;
   if (out) {
     const size_t m = std::min<size_t>(n_floats / 12, n);

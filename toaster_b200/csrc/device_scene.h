@@ -94,10 +94,12 @@ int render_max_blocks_per_sm(int block_size, bool moments, int mode = kModePlain
 cudaError_t launch_render_batch(const RenderLaunch& r, int block_size, int grid_size, cudaStream_t stream);
 int render_batch_max_blocks_per_sm(int block_size);
 // Training samples (3 float4 each: position + weight, normal, direction) from recorded diffuse
-// scatters: weight = luminance of the radiance that arrived along the scattered direction.
+// scatters: weight = luminance of the radiance that arrived along the scattered direction. Only
+// positive-weight samples are written (compacted, order unspecified); *sample_count (zeroed by
+// the caller) receives their number and *weight_sum (zeroed) the sum of weights.
 cudaError_t launch_guide_samples(const float4* records, const uint32_t* record_count, uint32_t capacity,
-                                 const float4* path_radiance, float4* samples, float* weight_sum,
-                                 cudaStream_t stream);
+                                 const float4* path_radiance, float4* samples, uint32_t* sample_count,
+                                 float* weight_sum, cudaStream_t stream);
 // Device address of the library's static render scratch (kStaticScratchWords 64-bit words) on
 // `device`, which must be the current device; looked up once per device.
 constexpr int kStaticScratchWords = 32;

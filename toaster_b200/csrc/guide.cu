@@ -71,16 +71,19 @@ __device__ void encode_row(uint8_t* tile, int row, bool valid, float px, float p
   float e[kGuideIn];
   if (valid) {
     const float q[3] = {(px - b.cx) * b.scale, (py - b.cy) * b.scale, (pz - b.cz) * b.scale};
+    // Half-octave ladder 2^(k/2), k = 0..11 (1 to about 45 cycles per half scene width): the
+    // incident-light field varies at room scale, and finer features only add noise dimensions
+    // that a few hundred online steps cannot learn to ignore.
+    constexpr float kFreq[kGuideFreqs] = {1.0f, 1.41421356f, 2.0f, 2.82842712f, 4.0f, 5.65685425f,
+                                          8.0f, 11.3137085f, 16.0f, 22.6274170f, 32.0f, 45.2548340f};
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
-      float f = q[a];
 #pragma unroll
       for (int k = 0; k < kGuideFreqs; ++k) {
         float s, c;
-        sincospif(f, &s, &c);
+        sincospif(q[a] * kFreq[k], &s, &c);
         e[24 * a + 2 * k] = s;
         e[24 * a + 2 * k + 1] = c;
-        f *= 2.0f;
       }
     }
     e[72] = nx; e[73] = ny; e[74] = nz;

@@ -1,7 +1,7 @@
 // Path-guiding network: parameter packing, device state and kernel launchers (guide.cu).
 //
-// The network maps an 80-wide encoding of a surface point (12-frequency Fourier features of the
-// normalised position + the normal) through three 64-wide ReLU layers to 32 outputs that
+// The network maps an 80-wide encoding of a surface point (Fourier features of the normalised
+// position at 12 half-octave frequencies 2^(k/2) + the normal) through three 64-wide ReLU layers to 32 outputs that
 // parameterise an 8-lobe von Mises-Fisher mixture over outgoing directions.
 #ifndef TOASTER_B200_GUIDE_H
 #define TOASTER_B200_GUIDE_H

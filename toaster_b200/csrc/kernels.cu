@@ -828,15 +828,23 @@ int render_max_blocks_per_sm(int block_size, bool moments, int mode) {
 }
 
 // ------------------------------------------------------------------------ training samples
+// Training samples from the recorded scatters. Only scatters whose direction carried radiance
+// are kept (compacted through one atomic per warp): a zero weight adds nothing to the weighted
+// likelihood, and in dim interiors most recorded directions carry none, so uniform draws over
+// all records would leave almost every batch slot empty.
 __global__ void guide_samples_kernel(const float4* __restrict__ rec, const uint32_t* __restrict__ count,
                                      uint32_t capacity, const float4* __restrict__ path_rad,
-                                     float4* __restrict__ out, float* __restrict__ weight_sum) {
+                                     float4* __restrict__ out, uint32_t* __restrict__ out_count,
+                                     float* __restrict__ weight_sum) {
   const uint32_t n = min(*count, capacity);
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   float w = 0.0f;
+  float4 a = make_float4(0, 0, 0, 0), b = a, c = a;
   if (i < n) {
-    const float4 a = rec[4 * size_t(i)], b = rec[4 * size_t(i) + 1], c = rec[4 * size_t(i) + 2],
-                 d = rec[4 * size_t(i) + 3];
+    a = rec[4 * size_t(i)];
+    b = rec[4 * size_t(i) + 1];
+    c = rec[4 * size_t(i) + 2];
+    const float4 d = rec[4 * size_t(i) + 3];
     const float4 end = path_rad[__float_as_uint(a.w)];
     // Radiance that arrived along the scattered direction: what the path gathered after this
     // vertex, divided by the throughput it had just after scattering.
@@ -844,21 +852,33 @@ __global__ void guide_samples_kernel(const float4* __restrict__ rec, const uint3
     const float ly = c.w > 0.0f ? fmaxf(end.y - d.y, 0.0f) / c.w : 0.0f;
     const float lz = d.w > 0.0f ? fmaxf(end.z - d.z, 0.0f) / d.w : 0.0f;
     w = 0.2126f * lx + 0.7152f * ly + 0.0722f * lz;
-    if (!isfinite(w)) w = 0.0f;
-    out[3 * size_t(i)] = make_float4(a.x, a.y, a.z, w);
-    out[3 * size_t(i) + 1] = make_float4(b.x, b.y, b.z, 0.0f);
-    out[3 * size_t(i) + 2] = make_float4(c.x, c.y, c.z, 0.0f);
+    if (!(w > 0.0f) || !isfinite(w)) w = 0.0f;
+  }
+  const bool keep = w > 0.0f;
+  const unsigned mask = __ballot_sync(0xffffffffu, keep);
+  const unsigned lane = threadIdx.x & 31u;
+  uint32_t base = 0;
+  if (mask) {
+    const int leader = __ffs(mask) - 1;
+    if (int(lane) == leader) base = atomicAdd(out_count, uint32_t(__popc(mask)));
+    base = __shfl_sync(0xffffffffu, base, leader);
+  }
+  if (keep) {
+    const uint32_t slot = base + uint32_t(__popc(mask & ((1u << lane) - 1u)));
+    out[3 * size_t(slot)] = make_float4(a.x, a.y, a.z, w);
+    out[3 * size_t(slot) + 1] = make_float4(b.x, b.y, b.z, 0.0f);
+    out[3 * size_t(slot) + 2] = make_float4(c.x, c.y, c.z, 0.0f);
   }
   for (int o = 16; o > 0; o >>= 1) w += __shfl_down_sync(0xffffffffu, w, o);
-  if ((threadIdx.x & 31u) == 0 && w != 0.0f) atomicAdd(weight_sum, w);
+  if (lane == 0 && w != 0.0f) atomicAdd(weight_sum, w);
 }
 
 cudaError_t launch_guide_samples(const float4* records, const uint32_t* record_count, uint32_t capacity,
-                                 const float4* path_radiance, float4* samples, float* weight_sum,
-                                 cudaStream_t stream) {
+                                 const float4* path_radiance, float4* samples, uint32_t* sample_count,
+                                 float* weight_sum, cudaStream_t stream) {
   if (capacity == 0) return cudaSuccess;
   guide_samples_kernel<<<(capacity + 255) / 256, 256, 0, stream>>>(records, record_count, capacity, path_radiance,
-                                                                   samples, weight_sum);
+                                                                   samples, sample_count, weight_sum);
   return cudaGetLastError();
 }
 
