@@ -47,6 +47,11 @@ def parse_args():
     ap.add_argument("--cpu-seconds", type=float, default=10.0, help="target wall time of one CPU sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--spp", type=int, default=64, help="samples per pixel per frame (64 = the benchmark workload)")
+    ap.add_argument("--no-equal-time", action="store_true", help="skip the guided-vs-plain equal-time comparison")
+    ap.add_argument("--equal-time-ref-spp", type=int, default=4096,
+                    help="samples per pixel of the plain FP64 reference the equal-time RMSE is measured against")
+    ap.add_argument("--batch-eval", action="store_true",
+                    help="also run the batched-scenes and animated-frames evaluation (a few minutes)")
     return ap.parse_args()
 
 
@@ -334,6 +339,12 @@ def run_ours(args):
         }
         if roofline is not None:
             line["roofline"] = roofline
+        if world == 1 and not args.no_equal_time:
+            line["equal_time"] = equal_time_block(args.equal_time_ref_spp, local)
+        if world == 1 and args.batch_eval:
+            from toaster_b200 import batch_eval
+            line["batched"] = batch_eval.uneven()
+            line["animation"] = batch_eval.animation(frames=240)
         if cpu is not None:
             line["cpu_baseline"] = {
                 "value": cpu["mpaths_s"], "unit": UNIT, "cores": cpu["cores"], "kind": "port",
@@ -345,6 +356,28 @@ def run_ours(args):
     if world > 1:
         dist.destroy_process_group()
     return 0
+
+
+def equal_time_block(ref_spp: int, device: int) -> dict:
+    """Guided vs plain sampling at equal GPU time on the learned-guiding workload (window room,
+    8,192 clutter triangles with 30% metal, 1280x720, 8 bounces): plain accumulates 256 spp in
+    16-spp batches; guided records 16 spp, trains 600 Adam steps on the GPU and accumulates guided
+    batches. RMSE is against a plain FP64 reference of ``ref_spp`` samples per pixel; the trimmed
+    RMSE leaves out the 0.1% largest pixel errors."""
+    from toaster_b200 import configs, guiding_eval
+
+    scene = configs.room_with_window()
+    t0 = time.perf_counter()
+    out = guiding_eval.equal_time_comparison(scene, ref_spp=ref_spp, plain_spp=256, batch=16, record_spp=16,
+                                             train_steps=600, train_batch=8192, seed=0, device=device)
+    keep = ["plain_seconds", "plain_rmse", "guided_seconds_to_plain_rmse", "time_fraction",
+            "guided_rmse_at_plain_time", "plain_trimmed_rmse", "time_fraction_trimmed",
+            "guided_trimmed_rmse_at_plain_time", "train_seconds", "samples"]
+    block = {k: out[k] for k in keep}
+    block.update(workload="window room, 8,192 clutter triangles (30% metal), 1280x720, 8 bounces",
+                 reference_spp=ref_spp, plain_spp=256, record_spp=16, train_steps=600,
+                 wall_seconds=time.perf_counter() - t0)
+    return block
 
 
 def read_traffic(rays_per_launch):

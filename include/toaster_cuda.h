@@ -141,7 +141,14 @@ typedef struct tc_render_options {
   uint32_t guiding;          /* 1: learned path guiding at diffuse vertices (needs tc_guide_set_params) */
   uint32_t guide_record;     /* 1: record (position, normal, direction, incident radiance) training
                                 samples at every diffuse scatter of this batch (plain sampling) */
-  uint32_t _reserved[3];
+  uint32_t wave_paths;       /* guided wavefront width: paths in flight per wave; 0 = 2^23 */
+  uint32_t short_stack;      /* traversal stack entries per thread held in shared memory (0..16;
+                                deeper entries live in local memory); 0 = none */
+  uint32_t refill_lanes;     /* a warp pauses traversal to refill finished lanes once fewer than
+                                this many of its 32 lanes are still traversing (1..32; 1 = only
+                                when all have finished); 0 = default. refill_lanes > 1 or
+                                short_stack > 0 select the resumable traversal, for plain renders
+                                without moments; other launches ignore both */
 } tc_render_options;
 
 /* Counters of the most recent tc_render / tc_trace_* call. */
@@ -214,6 +221,42 @@ int tc_render(tc_context* ctx, const tc_gpu_render_params* params, const tc_rend
  * set block_size and samples_per_item). Synchronous. */
 int tc_render_batch(tc_context* const* contexts, const tc_gpu_render_params* params, size_t n,
                     const tc_render_options* options);
+
+/* Autotuner: a coordinate search over the launch shape on the uploaded scene at params' size,
+ * one knob at a time, each stage keeping the fastest value: block size {64, 128, 256}, refill
+ * lanes {1, 12, 20, 28}, shared-memory short-stack entries {0, 8, 16}, then samples per work item
+ * {1, 2, 4} or, when base->guiding is set, wavefront width {2^21, 2^22, 2^23} paths. Each shape
+ * runs once untimed and once timed (CUDA events) with probe_samples spp (0 = min(params->samples,
+ * 4)). Other fields of `base` are kept. The context's accumulated image is replaced by the last
+ * probe. No reference counterpart. */
+typedef struct tc_tune_result {
+  tc_render_options best;
+  float best_kernel_ms;       /* device time of the fastest probe */
+  float best_mpaths_per_s;    /* its throughput */
+  uint32_t candidates;        /* shapes timed */
+  uint32_t probe_samples;
+} tc_tune_result;
+int tc_autotune(tc_context* ctx, const tc_gpu_render_params* params, const tc_render_options* base,
+                uint32_t probe_samples, tc_tune_result* out);
+
+/* Animated frames through one captured CUDA graph (the frame loop of
+ * render_gpu_with_sink, path_tracer.rs:591-840, with its per-frame host rebuild replaced by a
+ * device refit). tc_animation_create renders `first_frame` once to size every buffer, then
+ * captures a frame's whole device work: the copy of the frame's geometry, camera and frame index
+ * from pinned staging, the hierarchy refit, the render of `params` (plain, or guided when
+ * options->guiding is set and the context holds trained guide weights), display conversion
+ * (exposure_stops) and the RGBA8 readback. update_lights != 0 also re-packs the light records
+ * every frame (moving emitters). tc_animation_frame copies one evaluated frame (same counts as
+ * the uploaded scene) into the staging, replays the graph and writes 4*width*height bytes to rgba
+ * (may be NULL). Each frame is independent (accumulated_samples = 0) and seeded by frame_index.
+ * The context must not be used by other calls while an animation replays on it. */
+typedef struct tc_animation tc_animation;
+int tc_animation_create(tc_context* ctx, const tc_scene_data* first_frame, const tc_gpu_render_params* params,
+                        const tc_render_options* options, float exposure_stops, uint32_t update_lights,
+                        tc_animation** out);
+int tc_animation_frame(tc_animation* anim, const tc_scene_data* frame, uint32_t frame_index, uint8_t* rgba,
+                       size_t n_bytes);
+int tc_animation_destroy(tc_animation* anim);
 
 /* Replaces readback_pixels (crates/toaster-gpu/src/readback.rs:8-25): writes width*height
  * float4 linear-HDR averages into rgba (n_floats >= 4*width*height). */

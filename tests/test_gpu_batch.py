@@ -56,3 +56,31 @@ def test_batch_rejects_duplicates_and_options(native_lib):
             render_batch([r, r])
     finally:
         r.close()
+
+
+def test_autotune_returns_a_working_shape(native_lib):
+    with GpuRenderer(0) as r:
+        r.upload(scene_to_gpu(configs.mixed(width=320, height=180, samples=4, max_bounces=4)))
+        best = r.autotune(probe_samples=2)
+        assert best["block_size"] in (64, 128, 256)
+        assert best["short_stack"] in (0, 8, 16)
+        assert best["refill_lanes"] in (1, 12, 20, 28)
+        assert best["samples_per_item"] in (1, 2, 4)
+        assert best["candidates"] >= 10 and best["mpaths_per_s"] > 0
+        r.render(block_size=best["block_size"], short_stack=best["short_stack"],
+                 refill_lanes=best["refill_lanes"], samples_per_item=best["samples_per_item"])
+        assert r.stats()["paths"] == 320 * 180 * 4
+
+
+@pytest.mark.parametrize("refill", [1, 12, 28, 32])
+@pytest.mark.parametrize("short_stack", [0, 16])
+def test_launch_shapes_trace_the_same_paths(renderer, refill, short_stack):
+    # Dynamic fetching and the shared short stack change when and where a lane's traversal runs,
+    # not what it computes: the image equals the default shape's up to FP64 summation order.
+    scene = configs.mixed(width=96, height=54, samples=8, max_bounces=6)
+    renderer.upload(scene_to_gpu(scene))
+    renderer.render(frame_index=5)
+    a = renderer.readback_sums()[0]
+    renderer.render(frame_index=5, refill_lanes=refill, short_stack=short_stack, block_size=256)
+    b = renderer.readback_sums()[0]
+    assert close(b, a) > 0.999

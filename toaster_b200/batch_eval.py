@@ -1,0 +1,151 @@
+"""Batched and animated rendering: throughput and per-frame latency against the plain unbatched path.
+
+    python -m toaster_b200.batch_eval [--frames 240] [--width 1280 --height 720] [--spp 32]
+
+Two workloads:
+- ``uneven``: 16 independent scenes (triangle counts log-uniform in [128, 262,144], resolutions
+  320x180 to 1280x720) rendered by one persistent launch (tc_render_batch) versus one tc_render
+  per scene. Reports aggregate Mpaths/s of both.
+- ``animation``: 240 frames of 64 spheres + 64 boxes on ballistic trajectories. The graph path
+  replays one captured CUDA graph per frame (pinned staging -> refit -> render -> device display
+  conversion -> RGBA8 readback), with plain sampling and again with guided sampling (network
+  trained on frame 0); the plain unbatched path does what the reference does per frame: a full
+  scene upload with a host hierarchy build, a plain render, a float4 readback and display
+  conversion on the host. Reports per-frame latency (p50 / p99, from the packed frame records to
+  RGBA8 bytes on the host) and aggregate Mpaths/s of each.
+Host packing of the evaluated frame (scene_to_gpu) is the same for every path and is reported
+separately; it is not part of any latency.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import time
+
+import numpy as np
+
+from . import configs, guiding_eval
+from .renderer import Animation, GpuRenderer, render_batch
+from .scene import scene_to_gpu
+
+
+def host_display_rgba8(hdr: np.ndarray, exposure_stops: float = 0.0) -> np.ndarray:
+    """Host display conversion as the reference does it after readback (color.rs:24-74):
+    exposure, ACES fitted, clamp, sRGB transfer, rounding."""
+    rgb = hdr[..., :3].astype(np.float32) * np.float32(2.0 ** exposure_stops)
+    rgb = np.nan_to_num(rgb, nan=0.0, posinf=1.0, neginf=0.0)
+    c = np.maximum(rgb, 0.0)
+    t = np.clip((c * (2.51 * c + 0.03)) / (c * (2.43 * c + 0.59) + 0.14), 0.0, 1.0)
+    s = np.where(t <= 0.0031308, 12.92 * t, 1.055 * np.power(t, 1.0 / 2.4) - 0.055)
+    out = np.empty(hdr.shape[:-1] + (4,), np.uint8)
+    out[..., :3] = np.round(np.clip(s, 0.0, 1.0) * 255.0)
+    out[..., 3] = np.round(np.clip(hdr[..., 3], 0.0, 1.0) * 255.0)
+    return out
+
+
+def uneven(count: int = 16, samples: int = 32, max_bounces: int = 8, repeats: int = 3, device: int = 0) -> dict:
+    scenes = configs.uneven_batch(count=count, samples=samples, max_bounces=max_bounces)
+    rs = [GpuRenderer(device) for _ in scenes]
+    try:
+        for r, s in zip(rs, scenes):
+            r.upload(scene_to_gpu(s))
+        paths = sum(s.width * s.height * s.samples for s in scenes)
+        render_batch(rs, frame_index=0)  # warm-up
+        batched = []
+        for k in range(repeats):
+            st = render_batch(rs, frame_index=1 + k)
+            batched.append(st["kernel_ms"])
+        for r in rs:
+            r.render(frame_index=0)
+        single = []
+        for k in range(repeats):
+            tot = 0.0
+            for r in rs:
+                r.render(frame_index=1 + k)
+                tot += r.stats()["kernel_ms"]
+            single.append(tot)
+        b, u = float(np.median(batched)), float(np.median(single))
+        return {"scenes": count, "triangles": [s.triangle_count for s in scenes],
+                "resolutions": [f"{s.width}x{s.height}" for s in scenes], "spp": samples, "max_bounces": max_bounces,
+                "paths": paths, "batched_ms": b, "unbatched_ms": u, "batched_mpaths_per_s": paths / (b * 1e3),
+                "unbatched_mpaths_per_s": paths / (u * 1e3), "speedup": u / b}
+    finally:
+        for r in rs:
+            r.close()
+
+
+def animation(frames: int = 240, width: int = 1280, height: int = 720, samples: int = 32, max_bounces: int = 8,
+              guiding: bool = True, train_steps: int = 400, device: int = 0) -> dict:
+    anim = configs.BallisticAnimation(width=width, height=height, samples=samples, max_bounces=max_bounces,
+                                      frames=frames)
+    pack_times = []
+
+    def packed(k):
+        t = time.perf_counter()
+        data = scene_to_gpu(anim.scene(k))
+        pack_times.append((time.perf_counter() - t) * 1e3)
+        return data
+
+    first = packed(0)
+    paths = width * height * samples
+    out = {"frames": frames, "width": width, "height": height, "spp": samples, "max_bounces": max_bounces,
+           "primitives": int(anim.n_spheres + 2 + 12 * anim.n_boxes)}
+    # Graph path: plain sampling, then guided sampling with the network trained on frame 0.
+    for guided in ([False, True] if guiding else [False]):
+        with GpuRenderer(device) as r:
+            r.upload(first)
+            train_ms = 0.0
+            if guided:
+                r.guide_set_params(guiding_eval.initial_params(0), configs.scene_bounds(anim.scene(0)))
+                r.render(samples=16, frame_index=0, guide_record=True)
+                r.guide_train_recorded(train_steps, 8192, 1e-2, 1)
+                train_ms = r.stats()["kernel_ms"]
+            lat = []
+            with Animation(r, first, guiding=guided, update_lights=True) as a:
+                img = np.empty((height, width, 4), np.uint8)
+                a.frame(first, 0, img)  # warm-up replay
+                for k in range(frames):
+                    data = packed(k)
+                    t = time.perf_counter()
+                    a.frame(data, k, img)
+                    lat.append((time.perf_counter() - t) * 1e3)
+            lat = np.array(lat)
+            out["graph_guided" if guided else "graph"] = {
+                "guided": guided, "train_ms": train_ms, "p50_ms": float(np.percentile(lat, 50)),
+                "p99_ms": float(np.percentile(lat, 99)), "mean_ms": float(lat.mean()),
+                "mpaths_per_s": paths * frames / (lat.sum() * 1e3)}
+    # Plain unbatched path (the reference's per-frame flow).
+    with GpuRenderer(device) as r:
+        lat = []
+        r.upload(first)
+        r.render(frame_index=0)
+        for k in range(frames):
+            data = packed(k)
+            t = time.perf_counter()
+            r.upload(data)
+            r.render(frame_index=k)
+            host_display_rgba8(r.readback())
+            lat.append((time.perf_counter() - t) * 1e3)
+        lat = np.array(lat)
+        out["plain_unbatched"] = {"p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+                                  "mean_ms": float(lat.mean()), "mpaths_per_s": paths * frames / (lat.sum() * 1e3)}
+    out["host_pack_ms_per_frame"] = float(np.mean(pack_times))
+    return out
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--frames", type=int, default=240)
+    ap.add_argument("--width", type=int, default=1280)
+    ap.add_argument("--height", type=int, default=720)
+    ap.add_argument("--spp", type=int, default=32)
+    ap.add_argument("--no-guiding", action="store_true")
+    args = ap.parse_args()
+    print(json.dumps({"uneven": uneven(samples=args.spp)}), flush=True)
+    print(json.dumps({"animation": animation(args.frames, args.width, args.height, args.spp,
+                                             guiding=not args.no_guiding)}), flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -20,7 +20,7 @@ import math
 import numpy as np
 
 from . import gpu_types as gt
-from .scene import EnvironmentMap, Material, Scene, triangle_is_valid
+from .scene import EnvironmentMap, Material, Scene, box_triangles, triangle_is_valid
 
 
 def _unit_vectors(rng: np.random.Generator, n: int) -> np.ndarray:
@@ -321,3 +321,97 @@ def scene_bounds(scene: Scene):
     centre = (lo + hi) / 2
     half = max(float((hi - lo).max()) / 2, 1e-6)
     return (float(centre[0]), float(centre[1]), float(centre[2]), 1.0 / half)
+
+
+class BallisticAnimation:
+    """240 frames (24 fps, 10 s) of 64 spheres and 64 axis-aligned boxes thrown on seeded ballistic
+    trajectories over a ground quad, bouncing with restitution 0.8. Four spheres are emitters
+    (moving lights); materials are 50/30/20 diffuse / metal / dielectric otherwise. Lit by the mixed
+    scene's sky. Positions are integrated in double precision with 8 sub-steps per frame and stored
+    as f32 per frame, so frame k is a pure function of (seed, k)."""
+
+    def __init__(self, seed: int = 0, width: int = 1280, height: int = 720, samples: int = 32, max_bounces: int = 8,
+                 frames: int = 240, fps: float = 24.0, environment: EnvironmentMap | None = None):
+        rng = np.random.default_rng(seed + 9000)
+        self.frames, self.fps = frames, fps
+        self.n_spheres, self.n_boxes = 64, 64
+        n = self.n_spheres + self.n_boxes
+        self.radius = np.concatenate([rng.uniform(0.1, 0.3, self.n_spheres), rng.uniform(0.1, 0.4, self.n_boxes) / 2])
+        self.box_size = 2.0 * self.radius[self.n_spheres:]
+        self.p0 = np.stack([rng.uniform(-3, 3, n), rng.uniform(0.5, 3.0, n), rng.uniform(-3, 3, n)], -1)
+        self.v0 = np.stack([rng.uniform(-2, 2, n), rng.uniform(2, 6, n), rng.uniform(-2, 2, n)], -1)
+        mats = [Material.diffuse((0.5, 0.5, 0.5), "ground")]
+        kinds = rng.uniform(0, 1, n)
+        self.mat = np.zeros(n, np.uint32)
+        for i in range(n):
+            if i < 4:
+                mats.append(Material.emissive(rng.uniform(0.6, 1.0, 3), 20.0, f"e{i}"))
+            elif kinds[i] < 0.5:
+                mats.append(Material.diffuse(rng.uniform(0.2, 0.8, 3), f"d{i}"))
+            elif kinds[i] < 0.8:
+                mats.append(Material.metal(rng.uniform(0.5, 0.95, 3), rng.uniform(0.0, 0.5), f"m{i}"))
+            else:
+                mats.append(Material.dielectric(1.5, f"g{i}"))
+            self.mat[i] = len(mats) - 1
+        self.materials = mats
+        self.width, self.height, self.samples, self.max_bounces = width, height, samples, max_bounces
+        self.environment = environment if environment is not None else sky_environment()
+        self._positions = self._simulate()
+
+    def _simulate(self) -> np.ndarray:
+        n = self.p0.shape[0]
+        pos = np.empty((self.frames, n, 3), np.float64)
+        p, v = self.p0.copy(), self.v0.copy()
+        g = np.array([0.0, -9.81, 0.0])
+        sub = 8
+        dt = 1.0 / (self.fps * sub)
+        for f in range(self.frames):
+            pos[f] = p
+            for _ in range(sub):
+                v = v + g * dt
+                p = p + v * dt
+                low = p[:, 1] < self.radius
+                p[low, 1] = self.radius[low]
+                v[low, 1] = np.abs(v[low, 1]) * 0.8
+        return pos
+
+    def scene(self, frame: int) -> Scene:
+        p = self._positions[frame].astype(np.float32)
+        ns = self.n_spheres
+        ground = np.array(_quad((-10, 0, -10), (-10, 0, 10), (10, 0, 10), (10, 0, -10)), np.float32)
+        boxes = [box_triangles(p[ns + i], (self.box_size[i],) * 3) for i in range(self.n_boxes)]
+        tris = np.concatenate([ground] + boxes).astype(np.float32)
+        tri_mat = np.concatenate([np.zeros(2, np.uint32), np.repeat(self.mat[ns:], 12)])
+        return Scene(camera_position=(0.0, 3.0, 10.0), camera_look_at=(0.0, 1.0, 0.0), fov_degrees=45.0,
+                     width=self.width, height=self.height, samples=self.samples, max_bounces=self.max_bounces,
+                     background=gt.ENVIRONMENT, materials=self.materials, sphere_centers=p[:ns],
+                     sphere_radii=self.radius[:ns].astype(np.float32), sphere_materials=self.mat[:ns],
+                     triangles=tris, triangle_materials=tri_mat, environment=self.environment)
+
+
+def uneven_batch(seed: int = 0, count: int = 16, samples: int = 32, max_bounces: int = 8,
+                 environment: EnvironmentMap | None = None) -> list:
+    """``count`` independent scenes for one batched launch: triangle counts log-uniform in
+    [128, 262,144] (seeded random triangles as in random_triangles, scaled to a 4-unit cube, half
+    diffuse, a quarter metal, a quarter dielectric, plus a ground sphere) and resolutions
+    log-uniform between 320x180 and 1280x720 (16:9, width a multiple of 16), lit by the mixed
+    scene's sky."""
+    rng = np.random.default_rng(seed + 7000)
+    env = environment if environment is not None else sky_environment()
+    out = []
+    for i in range(count):
+        n_tri = int(round(math.exp(rng.uniform(math.log(128), math.log(262144)))))
+        width = int(round(math.exp(rng.uniform(math.log(320), math.log(1280))) / 16)) * 16
+        height = width * 9 // 16
+        tris = random_triangles(n_tri, seed=seed * 100 + i) * np.float32(2.0)
+        kinds = rng.uniform(0, 1, n_tri)
+        mats = [Material.diffuse((0.5, 0.5, 0.5), "ground"), Material.diffuse((0.6, 0.5, 0.4), "d"),
+                Material.metal((0.8, 0.8, 0.8), 0.2, "m"), Material.dielectric(1.5, "g")]
+        tri_mat = np.where(kinds < 0.5, 1, np.where(kinds < 0.75, 2, 3)).astype(np.uint32)
+        out.append(Scene(camera_position=(0.0, 1.0, 7.0), camera_look_at=(0.0, 0.0, 0.0), fov_degrees=45.0,
+                         width=width, height=height, samples=samples, max_bounces=max_bounces,
+                         background=gt.ENVIRONMENT, materials=mats,
+                         sphere_centers=np.array([[0.0, -1002.0, 0.0]], np.float32),
+                         sphere_radii=np.array([1000.0], np.float32), sphere_materials=np.zeros(1, np.uint32),
+                         triangles=tris, triangle_materials=tri_mat, environment=env))
+    return out

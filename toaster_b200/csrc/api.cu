@@ -32,6 +32,9 @@ static_assert(sizeof(tc_gpu_primitive_ref) == 8, "GpuPrimitiveRef is 8 bytes");
 
 namespace {
 
+// Default dynamic-fetch threshold of the path kernel (tc_render_options.refill_lanes).
+constexpr int kDefaultRefillLanes = 1;
+
 thread_local std::string g_thread_error;
 
 struct DevBuf {
@@ -623,16 +626,24 @@ int tc_set_camera(tc_context* ctx, const tc_gpu_camera* cam) {
   return TC_OK;
 }
 
-int tc_render(tc_context* ctx, const tc_gpu_render_params* p, const tc_render_options* opt) {
-  if (!ctx) return fail(nullptr, TC_ERR_INVALID, "context is null");
-  if (int rc = check_render_params(ctx, p)) return rc;
-  TC_CUDA(ctx, cudaSetDevice(ctx->device));
-  tc_render_options o{};
-  if (opt) o = *opt;
+// Everything a render puts on `st` without synchronising the host: accumulation setup, the path
+// kernel (or the guided wavefront's rounds) and the counter readback into `counters_host`.
+// `timing` records the context's events around the kernels (left out while capturing a graph).
+// frame_index_dev / camera_dev, when set, make the kernels read those per-frame values from
+// device memory. On success ctx->accumulated is advanced.
+static int enqueue_render(tc_context* ctx, const tc_gpu_render_params* p, const tc_render_options& o, cudaStream_t st,
+                          bool timing, const uint32_t* frame_index_dev, const float* camera_dev,
+                          unsigned long long* counters_host) {
   const bool moments = o.keep_moments != 0;
   const uint32_t npix = p->width * p->height;
-  cudaStream_t st = ctx->stream;
-  TC_CUDA(ctx, cudaEventRecord(ctx->ev_begin, st));
+  const int block = o.block_size ? int(o.block_size) : 128;
+  if (block % 32 != 0 || block < 32 || block > 256)
+    return fail(ctx, TC_ERR_INVALID, "block_size must be a multiple of 32 in [32, 256]");
+  if (o.guiding && o.guide_record) return fail(ctx, TC_ERR_INVALID, "guiding and guide_record are exclusive");
+  if (o.guiding && !ctx->has_guide) return fail(ctx, TC_ERR_STATE, "guided rendering needs tc_guide_set_params first");
+  if (o.short_stack > 16) return fail(ctx, TC_ERR_INVALID, "short_stack must be at most 16 entries");
+  if (o.refill_lanes > 32) return fail(ctx, TC_ERR_INVALID, "refill_lanes must be at most 32");
+  if (timing) TC_CUDA(ctx, cudaEventRecord(ctx->ev_begin, st));
   if (int rc = prepare_accumulation(ctx, p, moments, st)) return rc;
 
   tcb::RenderLaunch L{};
@@ -645,20 +656,19 @@ int tc_render(tc_context* ctx, const tc_gpu_render_params* p, const tc_render_op
   L.f.sample_base = ctx->accumulated;
   L.f.samples_per_item = std::min<uint32_t>(o.samples_per_item ? o.samples_per_item : 1u, p->samples);
   L.f.items_per_pixel = (p->samples + L.f.samples_per_item - 1) / L.f.samples_per_item;
+  L.f.frame_index_dev = frame_index_dev;
+  L.f.camera_dev = camera_dev;
   L.total_items = uint64_t(npix) * L.f.items_per_pixel;
   L.f.accum = ctx->accum.as<double>();
   L.f.accum_sq = moments ? ctx->accum_sq.as<double>() : nullptr;
   L.work_counter = ctx->work_counter.as<unsigned long long>();
   L.counters = ctx->counters.as<unsigned long long>();
+  L.short_stack = int(o.short_stack);
+  L.min_active = int(o.refill_lanes ? o.refill_lanes : kDefaultRefillLanes);
   TC_CUDA(ctx, cudaMemsetAsync(ctx->work_counter.ptr, 0, sizeof(unsigned long long), st));
   TC_CUDA(ctx, cudaMemsetAsync(ctx->counters.ptr, 0, 4 * sizeof(unsigned long long), st));
-  const int block = o.block_size ? int(o.block_size) : 128;
-  if (block % 32 != 0 || block < 32 || block > 256)
-    return fail(ctx, TC_ERR_INVALID, "block_size must be a multiple of 32 in [32, 256]");
-  if (o.guiding && o.guide_record) return fail(ctx, TC_ERR_INVALID, "guiding and guide_record are exclusive");
-  if (o.guiding && !ctx->has_guide) return fail(ctx, TC_ERR_STATE, "guided rendering needs tc_guide_set_params first");
   const int mode = o.guiding ? tcb::kModeGuided : (o.guide_record ? tcb::kModeRecord : tcb::kModePlain);
-  int per_sm = tcb::render_max_blocks_per_sm(block, moments, mode);
+  int per_sm = tcb::render_max_blocks_per_sm(block, moments, mode, L.short_stack, L.min_active);
   if (per_sm <= 0) return fail(ctx, TC_ERR_CUDA, "render kernel cannot be resident with this block size");
   const int grid = per_sm * ctx->sm_count;
   if (mode == tcb::kModeRecord) {
@@ -675,15 +685,15 @@ int tc_render(tc_context* ctx, const tc_gpu_render_params* p, const tc_render_op
     L.g.record_capacity = ctx->rec_capacity;
     L.g.path_radiance = ctx->rec_path_rad.as<float4>();
   }
-  TC_CUDA(ctx, cudaEventRecord(ctx->ev_kernel0, st));
+  if (timing) TC_CUDA(ctx, cudaEventRecord(ctx->ev_kernel0, st));
   if (mode != tcb::kModeGuided) {
     TC_CUDA(ctx, tcb::launch_render(L, block, grid, moments, st, mode));
   } else {
     // Wavefront: waves of whole samples per pixel; within a wave, rounds of (path kernel ->
     // suspended diffuse vertices -> tensor-core inference of their mixtures -> resume). Counts
     // stay on the device, so the rounds need no host synchronisation.
-    const uint32_t kWaveCap = 1u << 21;
-    const uint32_t wave_spp = std::max<uint32_t>(1u, std::min<uint32_t>(p->samples, kWaveCap / npix));
+    const uint32_t wave_cap = o.wave_paths ? o.wave_paths : (1u << 23);
+    const uint32_t wave_spp = std::max<uint32_t>(1u, std::min<uint32_t>(p->samples, wave_cap / npix));
     const uint32_t cap = wave_spp * npix;
     const uint32_t rounds = p->max_bounces > 1 ? p->max_bounces - 1 : 0;
     TC_CUDA(ctx, ctx->w_state_a.reserve(sizeof(float4) * 6 * size_t(cap)));
@@ -723,23 +733,43 @@ int tc_render(tc_context* ctx, const tc_gpu_render_params* p, const tc_render_op
       }
     }
   }
-  TC_CUDA(ctx, cudaEventRecord(ctx->ev_kernel1, st));
-  unsigned long long counters[4] = {0, 0, 0, 0};
-  TC_CUDA(ctx, cudaMemcpyAsync(counters, ctx->counters.ptr, sizeof(counters), cudaMemcpyDeviceToHost, st));
-  TC_CUDA(ctx, cudaEventRecord(ctx->ev_end, st));
-  TC_CUDA(ctx, cudaStreamSynchronize(st));
+  if (timing) TC_CUDA(ctx, cudaEventRecord(ctx->ev_kernel1, st));
+  if (counters_host)
+    TC_CUDA(ctx, cudaMemcpyAsync(counters_host, ctx->counters.ptr, 4 * sizeof(unsigned long long),
+                                 cudaMemcpyDeviceToHost, st));
+  if (timing) TC_CUDA(ctx, cudaEventRecord(ctx->ev_end, st));
   ctx->accumulated += p->samples;
   if (mode == tcb::kModeRecord) ctx->has_records = true;
+  return TC_OK;
+}
+
+// Counters of a finished render into the context's statistics; fails when paths went missing.
+static int finish_render_stats(tc_context* ctx, const unsigned long long* counters, uint64_t expected_paths,
+                               bool timing) {
   ctx->stats.paths = counters[0];
   ctx->stats.extension_rays = counters[1];
   ctx->stats.shadow_rays = counters[2];
   ctx->stats.rays = counters[1] + counters[2];
-  cudaEventElapsedTime(&ctx->stats.kernel_ms, ctx->ev_kernel0, ctx->ev_kernel1);
-  cudaEventElapsedTime(&ctx->stats.total_ms, ctx->ev_begin, ctx->ev_end);
-  if (counters[0] != uint64_t(npix) * p->samples)
+  if (timing) {
+    cudaEventElapsedTime(&ctx->stats.kernel_ms, ctx->ev_kernel0, ctx->ev_kernel1);
+    cudaEventElapsedTime(&ctx->stats.total_ms, ctx->ev_begin, ctx->ev_end);
+  }
+  if (counters[0] != expected_paths)
     return fail(ctx, TC_ERR_DEVICE_STATUS, "path kernel completed " + std::to_string(counters[0]) + " of " +
-                                                std::to_string(uint64_t(npix) * p->samples) + " paths");
+                                                std::to_string(expected_paths) + " paths");
   return TC_OK;
+}
+
+int tc_render(tc_context* ctx, const tc_gpu_render_params* p, const tc_render_options* opt) {
+  if (!ctx) return fail(nullptr, TC_ERR_INVALID, "context is null");
+  if (int rc = check_render_params(ctx, p)) return rc;
+  TC_CUDA(ctx, cudaSetDevice(ctx->device));
+  tc_render_options o{};
+  if (opt) o = *opt;
+  unsigned long long counters[4] = {0, 0, 0, 0};
+  if (int rc = enqueue_render(ctx, p, o, ctx->stream, true, nullptr, nullptr, counters)) return rc;
+  TC_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return finish_render_stats(ctx, counters, uint64_t(p->width) * p->height * p->samples, true);
 }
 
 int tc_render_batch(tc_context* const* contexts, const tc_gpu_render_params* params, size_t n,
@@ -754,6 +784,8 @@ int tc_render_batch(tc_context* const* contexts, const tc_gpu_render_params* par
   const int block = o.block_size ? int(o.block_size) : 128;
   if (block % 32 != 0 || block < 32 || block > 256)
     return fail(lead, TC_ERR_INVALID, "block_size must be a multiple of 32 in [32, 256]");
+  if (o.short_stack > 16) return fail(lead, TC_ERR_INVALID, "short_stack must be at most 16 entries");
+  if (o.refill_lanes > 32) return fail(lead, TC_ERR_INVALID, "refill_lanes must be at most 32");
   for (size_t i = 0; i < n; ++i) {
     tc_context* c = contexts[i];
     if (!c) return fail(lead, TC_ERR_INVALID, "context " + std::to_string(i) + " of the batch is null");
@@ -805,9 +837,11 @@ int tc_render_batch(tc_context* const* contexts, const tc_gpu_render_params* par
   L.total_items = items;
   L.work_counter = lead->work_counter.as<unsigned long long>();
   L.counters = lead->counters.as<unsigned long long>();
+  L.short_stack = int(o.short_stack);
+  L.min_active = int(o.refill_lanes ? o.refill_lanes : kDefaultRefillLanes);
   TC_CUDA(lead, cudaMemsetAsync(lead->work_counter.ptr, 0, sizeof(unsigned long long), st));
   TC_CUDA(lead, cudaMemsetAsync(lead->counters.ptr, 0, 4 * sizeof(unsigned long long), st));
-  const int per_sm = tcb::render_batch_max_blocks_per_sm(block);
+  const int per_sm = tcb::render_batch_max_blocks_per_sm(block, L.short_stack);
   if (per_sm <= 0) return fail(lead, TC_ERR_CUDA, "batched render kernel cannot be resident with this block size");
   TC_CUDA(lead, cudaEventRecord(lead->ev_kernel0, st));
   TC_CUDA(lead, tcb::launch_render_batch(L, block, per_sm * lead->sm_count, st));
@@ -826,6 +860,261 @@ int tc_render_batch(tc_context* const* contexts, const tc_gpu_render_params* par
   if (counters[0] != paths)
     return fail(lead, TC_ERR_DEVICE_STATUS, "batched path kernel completed " + std::to_string(counters[0]) + " of " +
                                                 std::to_string(paths) + " paths");
+  return TC_OK;
+}
+
+// ------------------------------------------------------------------------ autotuner
+int tc_autotune(tc_context* ctx, const tc_gpu_render_params* params, const tc_render_options* base,
+                uint32_t probe_samples, tc_tune_result* out) {
+  if (!ctx) return fail(nullptr, TC_ERR_INVALID, "context is null");
+  if (!out) return fail(ctx, TC_ERR_INVALID, "result pointer is null");
+  if (int rc = check_render_params(ctx, params)) return rc;
+  tc_render_options b{};
+  if (base) b = *base;
+  if (b.guide_record || b.keep_moments)
+    return fail(ctx, TC_ERR_INVALID, "the autotuner times plain or guided renders only");
+  TC_CUDA(ctx, cudaSetDevice(ctx->device));
+  tc_gpu_render_params p = *params;
+  p.accumulated_samples = 0;
+  p.samples = probe_samples ? probe_samples : std::min<uint32_t>(params->samples, 4u);
+  // Coordinate search over the launch shape, one knob at a time in this order, each stage keeping
+  // the fastest value so far: block size, dynamic-fetch threshold (refill lanes), shared
+  // short-stack entries, then (plain) samples per work item or (guided) wavefront width.
+  tc_render_options best = b;
+  if (!best.block_size) best.block_size = 128;
+  if (!best.refill_lanes) best.refill_lanes = kDefaultRefillLanes;
+  if (!best.samples_per_item) best.samples_per_item = 1;
+  if (!best.wave_paths) best.wave_paths = 1u << 23;
+  float best_ms = -1.0f;
+  uint32_t tried = 0;
+  auto time_shape = [&](const tc_render_options& o, float& ms) -> int {
+    // One untimed run sizes the buffers and warms the caches, then one timed run.
+    unsigned long long counters[4] = {0, 0, 0, 0};
+    if (int rc = enqueue_render(ctx, &p, o, ctx->stream, false, nullptr, nullptr, counters)) return rc;
+    if (int rc = enqueue_render(ctx, &p, o, ctx->stream, true, nullptr, nullptr, counters)) return rc;
+    TC_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    if (int rc = finish_render_stats(ctx, counters, uint64_t(p.width) * p.height * p.samples, true)) return rc;
+    ms = ctx->stats.kernel_ms;
+    ++tried;
+    return TC_OK;
+  };
+  if (int rc = time_shape(best, best_ms)) return rc;
+  auto stage = [&](uint32_t tc_render_options::*field, std::initializer_list<uint32_t> values) -> int {
+    for (uint32_t v : values) {
+      if (best.*field == v) continue;
+      tc_render_options o = best;
+      o.*field = v;
+      float ms = 0.0f;
+      if (int rc = time_shape(o, ms)) return rc;
+      if (ms < best_ms) {
+        best_ms = ms;
+        best = o;
+      }
+    }
+    return TC_OK;
+  };
+  if (int rc = stage(&tc_render_options::block_size, {64u, 128u, 256u})) return rc;
+  if (int rc = stage(&tc_render_options::refill_lanes, {1u, 12u, 20u, 28u})) return rc;
+  if (int rc = stage(&tc_render_options::short_stack, {0u, 8u, 16u})) return rc;
+  if (b.guiding) {
+    if (int rc = stage(&tc_render_options::wave_paths, {1u << 21, 1u << 22, 1u << 23})) return rc;
+  } else {
+    if (int rc = stage(&tc_render_options::samples_per_item, {1u, 2u, 4u})) return rc;
+  }
+  out->best = best;
+  out->best_kernel_ms = best_ms;
+  out->best_mpaths_per_s = best_ms > 0.0f ? float(double(p.width) * p.height * p.samples / (1e3 * double(best_ms))) : 0.0f;
+  out->candidates = tried;
+  out->probe_samples = p.samples;
+  return TC_OK;
+}
+
+// ------------------------------------------------------------------------ animation frames
+// One captured CUDA graph per animation: pinned staging -> device geometry, refit, render (plain
+// or guided wavefront), display conversion and the RGBA8 readback. A frame only rewrites the
+// pinned staging (geometry, camera, frame index) and replays the graph.
+struct tc_animation {
+  tc_context* ctx = nullptr;
+  tc_gpu_render_params params{};
+  tc_render_options options{};
+  float exposure = 0.0f;
+  bool update_lights = false;
+  size_t npix = 0;
+  tc_gpu_sphere* h_spheres = nullptr;       // pinned staging
+  tc_gpu_triangle* h_triangles = nullptr;
+  tcb::DevLight* h_lights = nullptr;
+  float* h_frame = nullptr;                 // camera (16 floats) then the frame index (uint32)
+  uint8_t* h_rgba = nullptr;                // pinned output
+  unsigned long long* h_counters = nullptr;
+  DevBuf d_frame, d_rgba;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+};
+
+static void animation_free(tc_animation* a) {
+  if (!a) return;
+  if (a->ctx) cudaSetDevice(a->ctx->device);
+  if (a->exec) cudaGraphExecDestroy(a->exec);
+  if (a->graph) cudaGraphDestroy(a->graph);
+  for (void* h : {static_cast<void*>(a->h_spheres), static_cast<void*>(a->h_triangles), static_cast<void*>(a->h_lights),
+                  static_cast<void*>(a->h_frame), static_cast<void*>(a->h_rgba), static_cast<void*>(a->h_counters)})
+    if (h) cudaFreeHost(h);
+  delete a;
+}
+
+// Copies one evaluated frame into the pinned staging.
+static int animation_stage(tc_animation* a, const tc_scene_data* sd, uint32_t frame_index) {
+  tc_context* ctx = a->ctx;
+  if (sd->sphere_count != ctx->sphere_count || sd->triangle_count != ctx->triangle_count ||
+      sd->material_count != ctx->material_count || sd->light_count != ctx->light_count)
+    return fail(ctx, TC_ERR_INVALID,
+                "evaluated scenes must preserve GPU geometry, material, light, and BVH primitive counts");
+  if ((sd->sphere_count && !sd->spheres) || (sd->triangle_count && !sd->triangles) || !sd->materials)
+    return fail(ctx, TC_ERR_INVALID, "frame geometry or material pointer is null");
+  if (int rc = validate_geometry(ctx, sd, ctx->material_count)) return rc;
+  if (sd->sphere_count) std::memcpy(a->h_spheres, sd->spheres, sizeof(tc_gpu_sphere) * sd->sphere_count);
+  if (sd->triangle_count) std::memcpy(a->h_triangles, sd->triangles, sizeof(tc_gpu_triangle) * sd->triangle_count);
+  if (a->update_lights && sd->light_count) {
+    std::vector<tcb::DevLight> lights;
+    if (int rc = pack_lights(ctx, sd, ctx->material_count, lights)) return rc;
+    std::memcpy(a->h_lights, lights.data(), sizeof(tcb::DevLight) * lights.size());
+  }
+  const tc_gpu_camera& c = sd->camera;
+  for (int k = 0; k < 4; ++k) {
+    a->h_frame[k] = c.origin[k];
+    a->h_frame[4 + k] = c.lower_left_corner[k];
+    a->h_frame[8 + k] = c.horizontal[k];
+    a->h_frame[12 + k] = c.vertical[k];
+  }
+  std::memcpy(a->h_frame + 16, &frame_index, sizeof(uint32_t));
+  return TC_OK;
+}
+
+// Enqueues the device work of one frame (what the graph holds).
+static int animation_enqueue(tc_animation* a, cudaStream_t st) {
+  tc_context* ctx = a->ctx;
+  TC_CUDA(ctx, cudaMemcpyAsync(a->d_frame.ptr, a->h_frame, 20 * sizeof(float), cudaMemcpyHostToDevice, st));
+  if (ctx->sphere_count)
+    TC_CUDA(ctx, cudaMemcpyAsync(ctx->raw_spheres.ptr, a->h_spheres, sizeof(tc_gpu_sphere) * ctx->sphere_count,
+                                 cudaMemcpyHostToDevice, st));
+  if (ctx->triangle_count)
+    TC_CUDA(ctx, cudaMemcpyAsync(ctx->raw_triangles.ptr, a->h_triangles, sizeof(tc_gpu_triangle) * ctx->triangle_count,
+                                 cudaMemcpyHostToDevice, st));
+  if (a->update_lights && ctx->light_count)
+    TC_CUDA(ctx, cudaMemcpyAsync(ctx->lights.ptr, a->h_lights, sizeof(tcb::DevLight) * ctx->light_count,
+                                 cudaMemcpyHostToDevice, st));
+  tcb::RefitPlan plan;
+  plan.nodes = ctx->refit_nodes.as<uint32_t>();
+  plan.level_offsets = ctx->refit_levels;
+  TC_CUDA(ctx, tcb::launch_refit(plan, ctx->pairs.as<tcb::PairNode>(), ctx->root_buf.as<tcb::ChildRec>(),
+                                 ctx->prims.as<tcb::PrimRecord>(), ctx->bvh_prims, ctx->raw_spheres.as<tc_gpu_sphere>(),
+                                 ctx->raw_triangles.as<tc_gpu_triangle>(), st));
+  const float* cam = a->d_frame.as<float>();
+  const uint32_t* fi = reinterpret_cast<const uint32_t*>(cam + 16);
+  if (int rc = enqueue_render(ctx, &a->params, a->options, st, false, fi, cam, a->h_counters)) return rc;
+  TC_CUDA(ctx, tcb::launch_display_from_sums(ctx->accum.as<double>(), uint32_t(a->npix), 1.0 / double(a->params.samples),
+                                             a->exposure, a->d_rgba.as<uint32_t>(), st));
+  TC_CUDA(ctx, cudaMemcpyAsync(a->h_rgba, a->d_rgba.ptr, 4 * a->npix, cudaMemcpyDeviceToHost, st));
+  return TC_OK;
+}
+
+int tc_animation_create(tc_context* ctx, const tc_scene_data* first_frame, const tc_gpu_render_params* params,
+                        const tc_render_options* options, float exposure_stops, uint32_t update_lights,
+                        tc_animation** out) {
+  if (!ctx) return fail(nullptr, TC_ERR_INVALID, "context is null");
+  if (!out || !first_frame) return fail(ctx, TC_ERR_INVALID, "first frame or output pointer is null");
+  *out = nullptr;
+  if (int rc = check_render_params(ctx, params)) return rc;
+  if (!std::isfinite(exposure_stops)) return fail(ctx, TC_ERR_INVALID, "exposure must be finite");
+  tc_render_options o{};
+  if (options) o = *options;
+  if (o.guide_record || o.keep_moments)
+    return fail(ctx, TC_ERR_INVALID, "animation frames do not record training samples or keep moments");
+  TC_CUDA(ctx, cudaSetDevice(ctx->device));
+  auto* a = new tc_animation();
+  a->ctx = ctx;
+  a->params = *params;
+  a->params.accumulated_samples = 0;
+  a->options = o;
+  a->exposure = exposure_stops;
+  a->update_lights = update_lights != 0;
+  a->npix = size_t(params->width) * params->height;
+  cudaError_t e = cudaSuccess;
+  auto host = [&](void** p, size_t bytes) {
+    if (e == cudaSuccess && bytes) e = cudaHostAlloc(p, bytes, cudaHostAllocDefault);
+  };
+  host(reinterpret_cast<void**>(&a->h_spheres), sizeof(tc_gpu_sphere) * ctx->sphere_count);
+  host(reinterpret_cast<void**>(&a->h_triangles), sizeof(tc_gpu_triangle) * ctx->triangle_count);
+  host(reinterpret_cast<void**>(&a->h_lights), sizeof(tcb::DevLight) * ctx->light_count);
+  host(reinterpret_cast<void**>(&a->h_frame), 20 * sizeof(float));
+  host(reinterpret_cast<void**>(&a->h_rgba), 4 * a->npix);
+  host(reinterpret_cast<void**>(&a->h_counters), 4 * sizeof(unsigned long long));
+  if (e == cudaSuccess) e = a->d_frame.reserve(20 * sizeof(float));
+  if (e == cudaSuccess) e = a->d_rgba.reserve(4 * a->npix);
+  if (e == cudaSuccess && ctx->sphere_count) e = ctx->raw_spheres.reserve(sizeof(tc_gpu_sphere) * ctx->sphere_count);
+  if (e == cudaSuccess && ctx->triangle_count)
+    e = ctx->raw_triangles.reserve(sizeof(tc_gpu_triangle) * ctx->triangle_count);
+  if (e != cudaSuccess) {
+    animation_free(a);
+    return cuda_fail(ctx, e, "animation buffers");
+  }
+  cudaStream_t st = ctx->stream;
+  // One direct run sizes every buffer the frame needs; the capture then records the same work.
+  int rc = animation_stage(a, first_frame, params->frame_index);
+  if (rc == TC_OK) rc = animation_enqueue(a, st);
+  if (rc == TC_OK && (e = cudaStreamSynchronize(st)) != cudaSuccess) rc = cuda_fail(ctx, e, "animation warm-up");
+  if (rc == TC_OK) {
+    ctx->raw_spheres_valid = ctx->raw_triangles_valid = true;
+    if ((e = cudaStreamBeginCapture(st, cudaStreamCaptureModeRelaxed)) != cudaSuccess) {
+      rc = cuda_fail(ctx, e, "cudaStreamBeginCapture");
+    } else {
+      rc = animation_enqueue(a, st);
+      cudaGraph_t g = nullptr;
+      const cudaError_t e2 = cudaStreamEndCapture(st, &g);
+      a->graph = g;
+      if (rc == TC_OK && e2 != cudaSuccess) rc = cuda_fail(ctx, e2, "cudaStreamEndCapture");
+      if (rc == TC_OK && (e = cudaGraphInstantiate(&a->exec, a->graph, 0)) != cudaSuccess)
+        rc = cuda_fail(ctx, e, "cudaGraphInstantiate");
+    }
+  }
+  if (rc != TC_OK) {
+    animation_free(a);
+    return rc;
+  }
+  *out = a;
+  return TC_OK;
+}
+
+int tc_animation_frame(tc_animation* a, const tc_scene_data* frame, uint32_t frame_index, uint8_t* rgba,
+                       size_t n_bytes) {
+  if (!a) return fail(nullptr, TC_ERR_INVALID, "animation is null");
+  tc_context* ctx = a->ctx;
+  if (!frame) return fail(ctx, TC_ERR_INVALID, "frame is null");
+  if (rgba && n_bytes < 4 * a->npix) return fail(ctx, TC_ERR_INVALID, "output buffer holds fewer than 4*width*height bytes");
+  if (int rc = animation_stage(a, frame, frame_index)) return rc;
+  TC_CUDA(ctx, cudaSetDevice(ctx->device));
+  cudaStream_t st = ctx->stream;
+  TC_CUDA(ctx, cudaEventRecord(ctx->ev_begin, st));
+  TC_CUDA(ctx, cudaGraphLaunch(a->exec, st));
+  TC_CUDA(ctx, cudaEventRecord(ctx->ev_end, st));
+  TC_CUDA(ctx, cudaStreamSynchronize(st));
+  ctx->width = a->params.width;
+  ctx->height = a->params.height;
+  ctx->accumulated = a->params.samples;
+  cudaEventElapsedTime(&ctx->stats.total_ms, ctx->ev_begin, ctx->ev_end);
+  ctx->stats.kernel_ms = ctx->stats.total_ms;
+  if (int rc = finish_render_stats(ctx, a->h_counters, uint64_t(a->npix) * a->params.samples, false)) return rc;
+  if (rgba) std::memcpy(rgba, a->h_rgba, 4 * a->npix);
+  return TC_OK;
+}
+
+int tc_animation_destroy(tc_animation* a) {
+  if (!a) return TC_OK;
+  if (a->ctx) {
+    cudaSetDevice(a->ctx->device);
+    cudaStreamSynchronize(a->ctx->stream);
+  }
+  animation_free(a);
   return TC_OK;
 }
 
@@ -862,6 +1151,7 @@ int tc_render_no_alloc(tc_context* ctx, const tc_gpu_render_params* p, double* s
   L.f.accum_sq = nullptr;
   L.work_counter = scratch;
   L.counters = scratch + 1;
+  L.min_active = kDefaultRefillLanes;
   const int block = 128;
   const int per_sm = tcb::render_max_blocks_per_sm(block, false);
   if (per_sm <= 0) return fail(ctx, TC_ERR_CUDA, "render kernel cannot be resident with this block size");

@@ -72,6 +72,11 @@ struct FrameJob {
   uint32_t sample_base;        // samples already accumulated (decorrelates progressive batches)
   uint32_t samples_per_item;   // samples a lane traces for one pixel before fetching new work
   uint32_t items_per_pixel;
+  // Replayed frames (CUDA graphs): when set, the frame index and the camera (origin, lower-left
+  // corner, horizontal, vertical; 4 floats each) are read from device memory at run time instead
+  // of the values above, so one captured launch serves every frame.
+  const uint32_t* frame_index_dev;
+  const float* camera_dev;
 };
 
 struct RenderLaunch {
@@ -81,6 +86,8 @@ struct RenderLaunch {
   uint64_t total_items;
   unsigned long long* work_counter;
   unsigned long long* counters;  // [0] paths, [1] extension rays, [2] shadow rays
+  int short_stack;               // traversal stack entries per thread kept in shared memory
+  int min_active;                // a warp pauses traversal for refills below this many busy lanes
   GuideLaunch g;
 };
 
@@ -89,10 +96,11 @@ cudaError_t launch_trace_closest(const DevScene& s, const float* rays, uint64_t 
                                  float* t, cudaStream_t stream);
 cudaError_t launch_render(const RenderLaunch& r, int block_size, int grid_size, bool moments, cudaStream_t stream,
                           int mode = kModePlain);
-int render_max_blocks_per_sm(int block_size, bool moments, int mode = kModePlain);
+int render_max_blocks_per_sm(int block_size, bool moments, int mode = kModePlain, int short_stack = 0,
+                             int min_active = 1);
 // Batched plain launch over r.jobs (r.job_count frames, items concatenated in job order).
 cudaError_t launch_render_batch(const RenderLaunch& r, int block_size, int grid_size, cudaStream_t stream);
-int render_batch_max_blocks_per_sm(int block_size);
+int render_batch_max_blocks_per_sm(int block_size, int short_stack = 0);
 // Training samples (3 float4 each: position + weight, normal, direction) from recorded diffuse
 // scatters: weight = luminance of the radiance that arrived along the scattered direction. Only
 // positive-weight samples are written (compacted, order unspecified); *sample_count (zeroed by

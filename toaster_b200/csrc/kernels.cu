@@ -9,8 +9,10 @@
 // The estimator is the one of crates/toaster-cpu/src/integrator.rs:99-244, written as an
 // iterative state machine so that every lane issues exactly one ray per loop iteration
 // (extension, light shadow or environment shadow). All lanes therefore run the traversal loop
-// together; idle lanes are refilled with new (pixel, sample-range) work items through one
-// warp-aggregated atomic (ballot + popc + shuffle) instead of idling until the warp drains.
+// together. Optionally (the kPause instantiation) a warp pauses it as soon as too few lanes are
+// still traversing: the finished lanes consume their hit and produce their next ray while the
+// others keep their traversal state (dynamic ray fetching). Idle lanes are refilled with new
+// (pixel, sample-range) work items through one warp-aggregated atomic (ballot + popc + shuffle).
 #include <cuda_runtime.h>
 #include <math_constants.h>
 #include <stdint.h>
@@ -324,14 +326,24 @@ __device__ __forceinline__ uint32_t aggregated_increment(uint32_t* counter) {
 
 __device__ __forceinline__ void start_sample(const FrameJob& J, Lane& ln) {
   const DevScene& s = J.scene;
-  ln.rng.seed(J.frame_index, ln.pixel, ln.sample);
+  ln.rng.seed(J.frame_index_dev ? *J.frame_index_dev : J.frame_index, ln.pixel, ln.sample);
   const uint32_t x = ln.pixel % J.width, y = ln.pixel / J.width;
   const float u = (float(x) + ln.rng.uniform()) / float(J.width);
   const float v = 1.0f - (float(y) + ln.rng.uniform()) / float(J.height);
-  const V3 o = mk(s.cam_origin[0], s.cam_origin[1], s.cam_origin[2]);
-  const V3 ll = mk(s.cam_lower_left[0], s.cam_lower_left[1], s.cam_lower_left[2]);
-  const V3 h = mk(s.cam_horizontal[0], s.cam_horizontal[1], s.cam_horizontal[2]);
-  const V3 vv = mk(s.cam_vertical[0], s.cam_vertical[1], s.cam_vertical[2]);
+  V3 o, ll, h, vv;
+  if (J.camera_dev) {
+    const float4* c = reinterpret_cast<const float4*>(J.camera_dev);
+    const float4 c0 = c[0], c1 = c[1], c2 = c[2], c3 = c[3];
+    o = mk(c0.x, c0.y, c0.z);
+    ll = mk(c1.x, c1.y, c1.z);
+    h = mk(c2.x, c2.y, c2.z);
+    vv = mk(c3.x, c3.y, c3.z);
+  } else {
+    o = mk(s.cam_origin[0], s.cam_origin[1], s.cam_origin[2]);
+    ll = mk(s.cam_lower_left[0], s.cam_lower_left[1], s.cam_lower_left[2]);
+    h = mk(s.cam_horizontal[0], s.cam_horizontal[1], s.cam_horizontal[2]);
+    vv = mk(s.cam_vertical[0], s.cam_vertical[1], s.cam_vertical[2]);
+  }
   ln.ro = o;
   ln.rd = normalize(ll + u * h + v * vv - o);
   ln.thr = mk(1.f, 1.f, 1.f);
@@ -579,7 +591,10 @@ __device__ __forceinline__ void shade_hit(const RenderLaunch& L, const FrameJob&
   ln.phase = kExtend;
 }
 
-template <int kMode, bool kMoments, bool kBatch>
+// kPause selects the traversal: false = each ray traced to its end in one call (trace_ray);
+// true = resumable traversals that a warp pauses to refill finished lanes (dynamic ray fetching,
+// L.min_active) with an optional shared-memory short stack (L.short_stack).
+template <int kMode, bool kMoments, bool kBatch, bool kPause>
 __global__ void __launch_bounds__(256) render_kernel(const RenderLaunch L) {
   static_assert(!kBatch || kMode == kModePlain, "batched launches trace plain paths");
   // The root record lives in device memory (a geometry refit rewrites it between launches);
@@ -589,12 +604,20 @@ __global__ void __launch_bounds__(256) render_kernel(const RenderLaunch L) {
     if (threadIdx.x == 0) root = *L.f.scene.root;
     __syncthreads();
   }
+  extern __shared__ uint2 s_stack[];  // L.short_stack entries per thread, blockDim.x apart
+  uint2* const my_stack = s_stack + threadIdx.x;
   const unsigned lane = threadIdx.x & 31u;
   const uint32_t npix = L.f.width * L.f.height;  // single-frame launches
   Lane ln;
   ln.phase = kIdle;
   ln.mix_slot = -1;
   ln.job = 0;
+  // Pausing traversal only: the lane's ray in flight, kept across rounds of the loop.
+  Traversal T;
+  T.cur = kNoNode;
+  T.rec = kNoNode;
+  bool inflight = false;
+  uint2 st_local[kPause ? kMaxStack : 1];  // its local-memory stack, also kept across rounds
   ln.acc = ln.acc2 = mk(0.f, 0.f, 0.f);
   bool finished = false;
   uint32_t n_paths = 0, n_ext = 0, n_shadow = 0, node_visits = 0;
@@ -661,24 +684,22 @@ __global__ void __launch_bounds__(256) render_kernel(const RenderLaunch L) {
 
     // Advance the lane's state machine to its next ray.
     bool have = false;
-    bool any_hit = false;
-    while (!finished && !have && ln.phase != kIdle) {
+    while (!finished && !inflight && !have && ln.phase != kIdle) {
       switch (ln.phase) {
         case kExtend:
           if (ln.depth <= 0) {
             finish_sample<kMode, kMoments>(L, J, ln, n_paths);
           } else {
             have = true;
-            any_hit = false;
             ln.tmax = CUDART_INF_F;
           }
           break;
         case kShadowLight:
-          if (prepare_light_shadow(s, ln)) { have = true; any_hit = true; }
+          if (prepare_light_shadow(s, ln)) have = true;
           else ln.phase = kShadowEnv;
           break;
         case kShadowEnv:
-          if (prepare_env_shadow<kMode>(L, J, ln)) { have = true; any_hit = true; }
+          if (prepare_env_shadow<kMode>(L, J, ln)) have = true;
           else ln.phase = kScatter;
           break;
         default: {  // kScatter: cosine-weighted diffuse bounce (integrator.rs:277-289)
@@ -744,16 +765,47 @@ __global__ void __launch_bounds__(256) render_kernel(const RenderLaunch L) {
       }
     }
 
+    // The ray in flight is (ln.ro, ln.rd, ln.tmax): the state machine leaves them alone until it
+    // has been consumed. Shadow rays (light and environment phases) stop at the first hit.
+    const bool shadow = ln.phase == kShadowLight || ln.phase == kShadowEnv;
+    bool hit = false, done = false;
     TraceResult tr;
-    bool hit = false;
+    if constexpr (!kPause) {
+      if (have) {
+        const RayQ q = make_ray(ln.ro.x, ln.ro.y, ln.ro.z, ln.rd.x, ln.rd.y, ln.rd.z);
+        if constexpr (kBatch) {
+          const ChildRec rt = *s.root;
+          hit = trace_ray(s.pairs, s.prims, rt, q, kRayEps, ln.tmax, shadow, tr, node_visits);
+        } else {
+          hit = trace_ray(s.pairs, s.prims, root, q, kRayEps, ln.tmax, shadow, tr, node_visits);
+        }
+        done = true;
+      }
+    } else {
+    const RayQ q = make_ray(ln.ro.x, ln.ro.y, ln.ro.z, ln.rd.x, ln.rd.y, ln.rd.z);
     if (have) {
-      const RayQ q = make_ray(ln.ro.x, ln.ro.y, ln.ro.z, ln.rd.x, ln.rd.y, ln.rd.z);
       if constexpr (kBatch) {
         const ChildRec rt = *s.root;
-        hit = trace_ray(s.pairs, s.prims, rt, q, kRayEps, ln.tmax, any_hit, tr, node_visits);
+        trav_start(T, rt, q, kRayEps, ln.tmax);
       } else {
-        hit = trace_ray(s.pairs, s.prims, root, q, kRayEps, ln.tmax, any_hit, tr, node_visits);
+        trav_start(T, root, q, kRayEps, ln.tmax);
       }
+      inflight = true;
+    }
+    // Traverse until too few of the warp's lanes are still busy; the finished ones consume
+    // their result now and fetch their next ray in the next round while the others resume.
+    trav_advance(T, q, kRayEps, shadow, s.pairs, s.prims, st_local, my_stack, L.short_stack, int(blockDim.x),
+                 L.min_active, !finished, node_visits);
+    if (inflight && T.cur == kNoNode) {
+      inflight = false;
+      done = true;
+      hit = T.found();
+      tr.t = T.closest;
+      tr.tag = T.tag;
+      tr.rec = T.rec;
+    }
+    }
+    if (done) {
       if (ln.phase == kShadowLight) {
         ++n_shadow;
         if (!hit) ln.rad = ln.rad + ln.pend;
@@ -785,23 +837,37 @@ __global__ void __launch_bounds__(256) render_kernel(const RenderLaunch L) {
   }
 }
 
+static size_t stack_smem(int short_stack, int block_size) {
+  return sizeof(uint2) * size_t(short_stack > 0 ? short_stack : 0) * size_t(block_size);
+}
+
+// Plain renders without moments pause traversals when asked to (refill lanes above 1 or a shared
+// short stack); every other launch traces each ray to its end.
+static bool pausing(const RenderLaunch& r) { return r.min_active > 1 || r.short_stack > 0; }
+
 template <int kMode>
 static cudaError_t launch_mode(const RenderLaunch& r, int block_size, int grid_size, bool moments, cudaStream_t stream) {
-  if (moments) render_kernel<kMode, true, false><<<grid_size, block_size, 0, stream>>>(r);
-  else render_kernel<kMode, false, false><<<grid_size, block_size, 0, stream>>>(r);
+  if (kMode == kModePlain && !moments && pausing(r)) {
+    render_kernel<kModePlain, false, false, true>
+        <<<grid_size, block_size, stack_smem(r.short_stack, block_size), stream>>>(r);
+  } else if (moments) {
+    render_kernel<kMode, true, false, false><<<grid_size, block_size, 0, stream>>>(r);
+  } else {
+    render_kernel<kMode, false, false, false><<<grid_size, block_size, 0, stream>>>(r);
+  }
   return cudaGetLastError();
 }
 
 cudaError_t launch_render_batch(const RenderLaunch& r, int block_size, int grid_size, cudaStream_t stream) {
   if (!r.jobs || r.job_count == 0) return cudaErrorInvalidValue;
-  render_kernel<kModePlain, false, true><<<grid_size, block_size, 0, stream>>>(r);
+  render_kernel<kModePlain, false, true, false><<<grid_size, block_size, 0, stream>>>(r);
   return cudaGetLastError();
 }
 
-int render_batch_max_blocks_per_sm(int block_size) {
+int render_batch_max_blocks_per_sm(int block_size, int /*short_stack*/) {
   int blocks = 0;
   const cudaError_t e =
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, render_kernel<kModePlain, false, true>, block_size, 0);
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, render_kernel<kModePlain, false, true, false>, block_size, 0);
   return e == cudaSuccess ? blocks : 0;
 }
 
@@ -816,12 +882,18 @@ template <int kMode>
 static int blocks_for(int block_size, bool moments) {
   int blocks = 0;
   cudaError_t e = moments
-      ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, render_kernel<kMode, true, false>, block_size, 0)
-      : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, render_kernel<kMode, false, false>, block_size, 0);
+      ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, render_kernel<kMode, true, false, false>, block_size, 0)
+      : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, render_kernel<kMode, false, false, false>, block_size, 0);
   return e == cudaSuccess ? blocks : 0;
 }
 
-int render_max_blocks_per_sm(int block_size, bool moments, int mode) {
+int render_max_blocks_per_sm(int block_size, bool moments, int mode, int short_stack, int min_active) {
+  if (mode == kModePlain && !moments && (min_active > 1 || short_stack > 0)) {
+    int blocks = 0;
+    const cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+        &blocks, render_kernel<kModePlain, false, false, true>, block_size, stack_smem(short_stack, block_size));
+    return e == cudaSuccess ? blocks : 0;
+  }
   if (mode == kModeRecord) return blocks_for<kModeRecord>(block_size, moments);
   if (mode == kModeGuided) return blocks_for<kModeGuided>(block_size, moments);
   return blocks_for<kModePlain>(block_size, moments);

@@ -115,7 +115,7 @@ struct TraceResult {
 constexpr uint32_t kNoNode = 0xFFFFFFFFu;  // never a valid link (leaf links stay below 0xC0000000)
 
 // Ordered closest-hit traversal (any_hit = false) or first-hit occlusion query (any_hit = true)
-// over the sibling-pair hierarchy, returning whether a primitive was accepted in [tmin, tmax].
+// over the sibling-pair hierarchy, accepting primitives in [tmin, tmax].
 //
 // Closest-hit mode reproduces intersect.rs:172-263 exactly: children are tested against the
 // current closest distance; when both are hit the one with the smaller entry distance is taken
@@ -125,9 +125,134 @@ constexpr uint32_t kNoNode = 0xFFFFFFFFu;  // never a valid link (leaf links sta
 // Stack depth never exceeds the hierarchy depth, which the host checks against kMaxStack.
 //
 // The loop is the "while-while" form: an inner loop descends through interior nodes until every
-// lane holds a leaf (or has finished), then the lanes test their leaves together. A single loop
-// structure with one reconvergence point per phase keeps the warp's lanes executing together;
-// each ray still visits exactly the nodes, in exactly the order, of the sequential algorithm.
+// lane holds a leaf (or has finished), then the lanes test their leaves together. Each ray still
+// visits exactly the nodes, in exactly the order, of the sequential algorithm.
+//
+// The traversal is resumable, for persistent kernels that refill finished lanes while other lanes
+// of the warp are still traversing ("dynamic ray fetching"): a lane can hand control back after
+// any leaf, with its state in Traversal and its stack owned by the caller. Stack entries pack the
+// node reference and its entry distance; the first `n_short` live in shared memory
+// (`short_stack`, this thread's slots `stride` apart so a warp's accesses fall in distinct
+// banks), deeper ones in local memory.
+//
+// Only what must survive between calls is kept here (five words); the ray itself stays with the
+// caller, which passes it again on every call, so a persistent kernel holds no second copy of it
+// while the lane shades.
+struct Traversal {
+  uint32_t cur;      // next node or leaf reference; kNoNode when the traversal is over
+  int sp;
+  float closest;
+  uint32_t tag;      // PrimRecord tag of the accepted primitive
+  uint32_t rec;      // PrimRecord index of the accepted primitive; kNoNode while none is accepted
+  __device__ __forceinline__ bool found() const { return rec != kNoNode; }
+};
+
+__device__ __forceinline__ void trav_start(Traversal& T, const ChildRec& root, const RayQ& r, float tmin, float tmax) {
+  T.closest = tmax;
+  T.sp = 0;
+  T.tag = 0u;
+  T.rec = kNoNode;
+  float entry, tn;
+  T.cur = box_test(root.min_x, root.min_y, root.min_z, root.max_x, root.max_y, root.max_z, r, tmin, tmax, entry, tn)
+              ? root.link
+              : kNoNode;
+}
+
+// One step of a traversal that is not over: descend to the next leaf, test its primitives in
+// leaf order, and pop the next stacked node that survives the re-test against the updated closest
+// distance. The stack is the caller's: `st_local` (kMaxStack entries in local memory) below
+// `short_stack` (n_short entries in shared memory, `stride` apart).
+__device__ __forceinline__ void trav_step(Traversal& T, const RayQ& r, float tmin, bool any_hit,
+                                          const PairNode* __restrict__ pairs, const PrimRecord* __restrict__ prims,
+                                          uint2* st_local, uint2* short_stack, int n_short, int stride,
+                                          uint32_t& node_visits) {
+  uint32_t cur = T.cur;
+  int sp = T.sp;
+  float closest = T.closest;
+  auto push = [&](uint32_t ref, float t) {
+    const uint2 e = make_uint2(ref, __float_as_uint(t));
+    if (sp < n_short) short_stack[sp * stride] = e;
+    else st_local[sp - n_short] = e;
+    ++sp;
+  };
+  auto top = [&]() -> uint2 { return sp < n_short ? short_stack[sp * stride] : st_local[sp - n_short]; };
+  // Descend to a leaf.
+  while ((cur & kLeafBit) == 0u) {
+    ++node_visits;
+    const float4* q = reinterpret_cast<const float4*>(pairs + cur);
+    const float4 a0 = __ldg(q), a1 = __ldg(q + 1), b0 = __ldg(q + 2), b1 = __ldg(q + 3);
+    float ea, ta, eb, tb;
+    const bool ha = box_test(a0.x, a0.y, a0.z, a1.x, a1.y, a1.z, r, tmin, closest, ea, ta);
+    const bool hb = box_test(b0.x, b0.y, b0.z, b1.x, b1.y, b1.z, r, tmin, closest, eb, tb);
+    const uint32_t la = __float_as_uint(a0.w), lb = __float_as_uint(b0.w);
+    if (ha && hb) {
+      const bool a_first = ea < eb;
+      push(a_first ? lb : la, a_first ? tb : ta);
+      cur = a_first ? la : lb;
+    } else if (ha) {
+      cur = la;
+    } else if (hb) {
+      cur = lb;
+    } else {
+      cur = kNoNode;
+      while (sp > 0) {
+        --sp;
+        const uint2 e = top();
+        if (__uint_as_float(e.y) <= closest) {
+          cur = e.x;
+          break;
+        }
+      }
+      if (cur == kNoNode) break;
+    }
+  }
+  if (cur != kNoNode) {
+    // Leaf: primitives in leaf order.
+    uint32_t k = cur & ~kLeafBit;
+    bool stop = false;
+    for (;;) {
+      const float4* p = reinterpret_cast<const float4*>(prims + k);
+      const float4 A = __ldg(p);
+      const float4 B = __ldg(p + 1);
+      const uint32_t tag = __float_as_uint(A.w);
+      float t;
+      bool ok;
+      if (tag & kTagTriangle) {
+        const float4 C = __ldg(p + 2);
+        ok = hit_triangle(r, A, B, C, tmin, closest, t);
+      } else {
+        ok = hit_sphere(r, A, B, tmin, closest, t);
+      }
+      if (ok) {
+        closest = t;
+        T.tag = tag;
+        T.rec = k;
+        if (any_hit) {
+          stop = true;
+          break;
+        }
+      }
+      if (tag & kTagLast) break;
+      ++k;
+    }
+    cur = kNoNode;
+    while (!stop && sp > 0) {
+      --sp;
+      const uint2 e = top();
+      if (__uint_as_float(e.y) <= closest) {
+        cur = e.x;
+        break;
+      }
+    }
+  }
+  T.cur = cur;
+  T.sp = sp;
+  T.closest = closest;
+}
+
+// Whole traversal of one ray in one call (the form every launch uses unless it pauses traversals
+// for refills): the same node and primitive order as trav_step's, with the state in registers and
+// the stack in local memory.
 __device__ __forceinline__ bool trace_ray(const PairNode* __restrict__ pairs, const PrimRecord* __restrict__ prims,
                                           const ChildRec& root, const RayQ& r, float tmin, float tmax,
                                           bool any_hit, TraceResult& res, uint32_t& node_visits) {
@@ -211,6 +336,26 @@ __device__ __forceinline__ bool trace_ray(const PairNode* __restrict__ pairs, co
   }
   res.t = closest;
   return found;
+}
+
+// Advances the unfinished traversals of the warp one leaf visit per round. It returns when all
+// of them are done, or early when fewer than `min_active` lanes are still traversing and at
+// least one lane can use the pause: a lane whose traversal is over while it still has work to
+// take (`can_refill`). Lanes that cannot take work never stop the others, so every call makes
+// progress and the warp never pauses for nothing. Every lane of the warp must call it together.
+__device__ __forceinline__ void trav_advance(Traversal& T, const RayQ& r, float tmin, bool any_hit,
+                                             const PairNode* __restrict__ pairs,
+                                             const PrimRecord* __restrict__ prims, uint2* st_local, uint2* short_stack,
+                                             int n_short, int stride, int min_active, bool can_refill,
+                                             uint32_t& node_visits) {
+  for (;;) {
+    const unsigned act = __ballot_sync(0xffffffffu, T.cur != kNoNode);
+    if (act == 0u) return;
+    const unsigned ready = __ballot_sync(0xffffffffu, T.cur == kNoNode && can_refill);
+    if (ready != 0u && __popc(act) < min_active) return;
+    if (T.cur != kNoNode)
+      trav_step(T, r, tmin, any_hit, pairs, prims, st_local, short_stack, n_short, stride, node_visits);
+  }
 }
 
 }  // namespace tcb

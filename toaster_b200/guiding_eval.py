@@ -63,7 +63,16 @@ def rmse(a: np.ndarray, b: np.ndarray) -> float:
     return float(np.sqrt(np.mean((a - b) ** 2)))
 
 
-def timeline_plain(scene: Scene, reference: np.ndarray, total_spp: int, batch: int, device: int = 0):
+def trimmed_rmse(a: np.ndarray, b: np.ndarray, keep: float = 0.999) -> float:
+    """RMSE over the pixels whose squared error is at or below the ``keep`` quantile: the same
+    error with the rarest outliers (single bright samples) left out, a steadier statistic for
+    comparing two unbiased estimators from one run each."""
+    e = ((a - b) ** 2).mean(axis=-1).ravel()
+    return float(np.sqrt(e[e <= np.quantile(e, keep)].mean()))
+
+
+def timeline_plain(scene: Scene, reference: np.ndarray, total_spp: int, batch: int, device: int = 0,
+                   frame_offset: int = 0):
     points = []
     with GpuRenderer(device) as r:
         r.upload(scene_to_gpu(scene))
@@ -71,23 +80,26 @@ def timeline_plain(scene: Scene, reference: np.ndarray, total_spp: int, batch: i
         done = 0
         while done < total_spp:
             n = min(batch, total_spp - done)
-            r.render(samples=n, frame_index=done, accumulate=done > 0)
+            r.render(samples=n, frame_index=frame_offset + done, accumulate=done > 0)
             t += r.stats()["total_ms"] * 1e-3
             done += n
-            points.append((t, done, rmse(_image(r), reference)))
+            img = _image(r)
+            points.append((t, done, rmse(img, reference), trimmed_rmse(img, reference)))
     return points
 
 
 def timeline_guided(scene: Scene, reference: np.ndarray, total_spp: int, batch: int, record_spp: int,
-                    train_steps: int, train_batch: int, lr: float = 1e-2, seed: int = 0, device: int = 0):
+                    train_steps: int, train_batch: int, lr: float = 1e-2, seed: int = 0, device: int = 0,
+                    frame_offset: int = 0):
     points = []
     info = {}
     with GpuRenderer(device) as r:
         r.upload(scene_to_gpu(scene))
         r.guide_set_params(initial_params(seed), configs.scene_bounds(scene))
-        r.render(samples=record_spp, frame_index=0, guide_record=True)
+        r.render(samples=record_spp, frame_index=frame_offset, guide_record=True)
         t = r.stats()["total_ms"] * 1e-3
-        points.append((t, record_spp, rmse(_image(r), reference)))
+        img = _image(r)
+        points.append((t, record_spp, rmse(img, reference), trimmed_rmse(img, reference)))
         t0 = time.perf_counter()
         losses, n = r.guide_train_recorded(train_steps, train_batch, lr, seed)
         train_s = r.stats()["kernel_ms"] * 1e-3
@@ -97,64 +109,89 @@ def timeline_guided(scene: Scene, reference: np.ndarray, total_spp: int, batch: 
         done = record_spp
         while done < total_spp:
             m = min(batch, total_spp - done)
-            r.render(samples=m, frame_index=done, accumulate=True, guiding=True)
+            r.render(samples=m, frame_index=frame_offset + done, accumulate=True, guiding=True)
             t += r.stats()["total_ms"] * 1e-3
             done += m
-            points.append((t, done, rmse(_image(r), reference)))
+            img = _image(r)
+            points.append((t, done, rmse(img, reference), trimmed_rmse(img, reference)))
     return points, info
 
 
-def time_to_reach(points, target: float):
-    """Earliest (interpolated in log RMSE between batches) time at which RMSE <= target, or None."""
+def time_to_reach(points, target: float, col: int = 2):
+    """Earliest (interpolated in log error between batches) time at which the error in column
+    ``col`` (2 = RMSE, 3 = trimmed RMSE) is <= target, or None."""
     prev = None
-    for t, spp, e in points:
+    for p in points:
+        t, e = p[0], p[col]
         if e <= target:
-            if prev is None or prev[2] <= e:
+            if prev is None or prev[1] <= e:
                 return t
-            t0, _, e0 = prev
+            t0, e0 = prev
             f = (np.log(e0) - np.log(target)) / (np.log(e0) - np.log(e))
             return t0 + f * (t - t0)
-        prev = (t, spp, e)
+        prev = (t, e)
     return None
 
 
 def equal_time_comparison(scene: Scene, ref_spp: int, plain_spp: int = 256, batch: int = 16, record_spp: int = 16,
                           guided_spp: int | None = None, train_steps: int = 300, train_batch: int = 8192,
-                          seed: int = 0, device: int = 0) -> dict:
-    reference = reference_image(scene, ref_spp, device=device)
-    plain = timeline_plain(scene, reference, plain_spp, batch, device)
+                          seed: int = 0, device: int = 0, reference: np.ndarray | None = None) -> dict:
+    if reference is None:
+        reference = reference_image(scene, ref_spp, device=device)
+    # Each seed draws its own path samples (frame indices offset by 100,000 per seed).
+    plain = timeline_plain(scene, reference, plain_spp, batch, device, frame_offset=100_000 * seed)
     guided, info = timeline_guided(scene, reference, guided_spp or plain_spp, batch, record_spp, train_steps,
-                                   train_batch, seed=seed, device=device)
-    t_plain, _, e_plain = plain[-1]
+                                   train_batch, seed=seed, device=device, frame_offset=100_000 * seed)
+    t_plain, _, e_plain, et_plain = plain[-1]
     t_guided = time_to_reach(guided, e_plain)
-    e_guided_at_equal_time = None
-    for t, _, e in guided:
+    tt_guided = time_to_reach(guided, et_plain, col=3)
+    e_at, et_at = None, None
+    for t, _, e, et in guided:
         if t <= t_plain:
-            e_guided_at_equal_time = e
+            e_at, et_at = e, et
     return {
         "width": scene.width, "height": scene.height, "max_bounces": scene.max_bounces, "reference_spp": ref_spp,
         "plain_spp": plain_spp, "plain_seconds": t_plain, "plain_rmse": e_plain,
         "guided_seconds_to_plain_rmse": t_guided,
         "time_fraction": None if t_guided is None else t_guided / t_plain,
-        "guided_rmse_at_plain_time": e_guided_at_equal_time,
+        "guided_rmse_at_plain_time": e_at,
+        "plain_trimmed_rmse": et_plain,
+        "time_fraction_trimmed": None if tt_guided is None else tt_guided / t_plain,
+        "guided_trimmed_rmse_at_plain_time": et_at,
         "plain_timeline": plain, "guided_timeline": guided, **info,
     }
 
 
 def main():
+    """Defaults are the learned-guiding workload: the window room (8,192 clutter triangles, 30%
+    metal) at 1280x720, 8 bounces, a 65,536-spp reference, 256 plain spp, 16 recorded spp."""
     ap = argparse.ArgumentParser()
-    ap.add_argument("--width", type=int, default=320)
-    ap.add_argument("--height", type=int, default=180)
+    ap.add_argument("--width", type=int, default=1280)
+    ap.add_argument("--height", type=int, default=720)
     ap.add_argument("--ref-spp", type=int, default=65536)
     ap.add_argument("--plain-spp", type=int, default=256)
     ap.add_argument("--guided-spp", type=int, default=0)
-    ap.add_argument("--train-steps", type=int, default=300)
-    ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--record-spp", type=int, default=16)
+    ap.add_argument("--train-steps", type=int, default=600)
+    ap.add_argument("--clutter", type=int, default=8192)
+    ap.add_argument("--metal", type=float, default=0.3)
+    ap.add_argument("--seeds", type=int, default=1)
+    ap.add_argument("--timelines", action="store_true")
     args = ap.parse_args()
-    scene = configs.room_with_window(width=args.width, height=args.height)
-    out = equal_time_comparison(scene, args.ref_spp, args.plain_spp, guided_spp=args.guided_spp or None,
-                                train_steps=args.train_steps, seed=args.seed)
-    print(json.dumps(out))
+    scene = configs.room_with_window(width=args.width, height=args.height, clutter=args.clutter,
+                                     metal_fraction=args.metal)
+    t0 = time.perf_counter()
+    reference = reference_image(scene, args.ref_spp)
+    print(json.dumps({"reference_spp": args.ref_spp, "reference_seconds": time.perf_counter() - t0}), flush=True)
+    for seed in range(args.seeds):
+        out = equal_time_comparison(scene, args.ref_spp, args.plain_spp, record_spp=args.record_spp,
+                                    guided_spp=args.guided_spp or None, train_steps=args.train_steps, seed=seed,
+                                    reference=reference)
+        if not args.timelines:
+            out.pop("plain_timeline")
+            out.pop("guided_timeline")
+        out["seed"] = seed
+        print(json.dumps(out), flush=True)
 
 
 if __name__ == "__main__":

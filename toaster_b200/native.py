@@ -53,6 +53,10 @@ EXPORTED_SYMBOLS = (
     "tc_display_rgba8_async",
     "tc_render_batch",
     "tc_guide_recorded_samples",
+    "tc_animation_create",
+    "tc_animation_frame",
+    "tc_animation_destroy",
+    "tc_autotune",
 )
 
 GUIDE_PARAMS = 15584
@@ -105,8 +109,15 @@ class RenderOptions(ctypes.Structure):
         ("keep_moments", ctypes.c_uint32),
         ("guiding", ctypes.c_uint32),
         ("guide_record", ctypes.c_uint32),
-        ("_reserved", ctypes.c_uint32 * 3),
+        ("wave_paths", ctypes.c_uint32),
+        ("short_stack", ctypes.c_uint32),
+        ("refill_lanes", ctypes.c_uint32),
     ]
+
+
+class TuneResult(ctypes.Structure):
+    _fields_ = [("best", RenderOptions), ("best_kernel_ms", ctypes.c_float), ("best_mpaths_per_s", ctypes.c_float),
+                ("candidates", ctypes.c_uint32), ("probe_samples", ctypes.c_uint32)]
 
 
 class Stats(ctypes.Structure):
@@ -166,6 +177,11 @@ def load_library(path: os.PathLike | None = None) -> ctypes.CDLL:
     lib.tc_display_rgba8_async.argtypes = [vp, f32, vp, sz, vp]
     lib.tc_render_batch.argtypes = [ctypes.POINTER(vp), vp, sz, ctypes.POINTER(RenderOptions)]
     lib.tc_guide_recorded_samples.argtypes = [vp, vp, sz, ctypes.POINTER(u32)]
+    lib.tc_animation_create.argtypes = [vp, ctypes.POINTER(SceneData), vp, ctypes.POINTER(RenderOptions), f32, u32,
+                                        ctypes.POINTER(vp)]
+    lib.tc_animation_frame.argtypes = [vp, ctypes.POINTER(SceneData), u32, vp, sz]
+    lib.tc_animation_destroy.argtypes = [vp]
+    lib.tc_autotune.argtypes = [vp, vp, ctypes.POINTER(RenderOptions), u32, ctypes.POINTER(TuneResult)]
     for name in EXPORTED_SYMBOLS:
         if not hasattr(lib, name):
             raise RuntimeError(f"{p} does not export {name}")

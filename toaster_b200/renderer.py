@@ -20,8 +20,58 @@ from . import native
 from .scene import Scene, SceneGpuData, scene_to_gpu
 
 
+class Animation:
+    """Animated frames replayed through one captured CUDA graph (tc_animation_*).
+
+    The renderer must hold the uploaded first frame; every frame passed to ``frame`` must keep its
+    primitive counts. Frames are independent renders seeded by their frame index."""
+
+    def __init__(self, renderer: "GpuRenderer", first: SceneGpuData, samples: Optional[int] = None,
+                 max_bounces: Optional[int] = None, exposure_stops: float = 0.0, guiding: bool = False,
+                 update_lights: bool = False, block_size: int = 0, wave_paths: int = 0, refill_lanes: int = 0):
+        self._r = renderer
+        self._lib = renderer._lib
+        self._h = None
+        p = first.params.copy()
+        if samples is not None:
+            p["samples"] = samples
+        if max_bounces is not None:
+            p["max_bounces"] = max_bounces
+        p["accumulated_samples"] = 0
+        self.width, self.height = int(p["width"][0]), int(p["height"][0])
+        opts = native.RenderOptions()
+        opts.guiding = 1 if guiding else 0
+        opts.block_size = block_size
+        opts.wave_paths = wave_paths
+        opts.refill_lanes = refill_lanes
+        sd, keep = GpuRenderer._scene_struct(first)
+        h = ctypes.c_void_p()
+        renderer._check(self._lib.tc_animation_create(renderer._ctx, ctypes.byref(sd), p.ctypes.data, ctypes.byref(opts),
+                                                      float(exposure_stops), int(update_lights), ctypes.byref(h)))
+        self._h = h
+
+    def frame(self, data: SceneGpuData, frame_index: int, out: Optional[np.ndarray] = None) -> np.ndarray:
+        if out is None:
+            out = np.empty((self.height, self.width, 4), np.uint8)
+        sd, keep = GpuRenderer._scene_struct(data)
+        self._r._check(self._lib.tc_animation_frame(self._h, ctypes.byref(sd), frame_index, out.ctypes.data, out.nbytes))
+        self._r.width, self._r.height = self.width, self.height
+        return out
+
+    def close(self) -> None:
+        if self._h:
+            self._lib.tc_animation_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+
 def render_batch(renderers, samples=None, frame_index: int = 0, accumulate: bool = False, block_size: int = 0,
-                 samples_per_item: int = 0) -> dict:
+                 samples_per_item: int = 0, short_stack: int = 0, refill_lanes: int = 0) -> dict:
     """One persistent launch over the uploaded scenes of several renderers (same device).
 
     ``samples`` may be one count or one per renderer. Returns the batch's stats (paths, rays,
@@ -45,6 +95,8 @@ def render_batch(renderers, samples=None, frame_index: int = 0, accumulate: bool
     opts = native.RenderOptions()
     opts.block_size = block_size
     opts.samples_per_item = samples_per_item
+    opts.short_stack = short_stack
+    opts.refill_lanes = refill_lanes
     native.check(lib, renderers[0]._ctx, lib.tc_render_batch(ctxs, params.ctypes.data, n, ctypes.byref(opts)))
     for i, r in enumerate(renderers):
         r.width, r.height = int(params[i]["width"]), int(params[i]["height"])
@@ -157,7 +209,7 @@ class GpuRenderer:
     def render(self, samples: Optional[int] = None, max_bounces: Optional[int] = None, width: Optional[int] = None,
                height: Optional[int] = None, frame_index: int = 0, accumulate: bool = False,
                keep_moments: bool = False, block_size: int = 0, samples_per_item: int = 0, guiding: bool = False,
-               guide_record: bool = False) -> None:
+               guide_record: bool = False, wave_paths: int = 0, short_stack: int = 0, refill_lanes: int = 0) -> None:
         """Traces ``samples`` paths per pixel; ``accumulate`` adds them to the previous batches."""
         if self._params is None:
             raise RuntimeError("render before upload")
@@ -178,9 +230,35 @@ class GpuRenderer:
         opts.keep_moments = 1 if keep_moments else 0
         opts.guiding = 1 if guiding else 0
         opts.guide_record = 1 if guide_record else 0
+        opts.wave_paths = wave_paths
+        opts.short_stack = short_stack
+        opts.refill_lanes = refill_lanes
         self._check(self._lib.tc_render(self._ctx, p.ctypes.data, ctypes.byref(opts)))
         self.width, self.height = int(p["width"][0]), int(p["height"][0])
         self.accumulated = (self.accumulated if accumulate else 0) + int(p["samples"][0])
+
+    def autotune(self, samples: Optional[int] = None, width: Optional[int] = None, height: Optional[int] = None,
+                 guiding: bool = False, probe_samples: int = 0) -> dict:
+        """Fastest launch shape (block size, refill lanes, short stack, samples per item / wave
+        width) for the uploaded scene, with its probe throughput. Replaces the accumulated image."""
+        p = self._params.copy()
+        if samples is not None:
+            p["samples"] = samples
+        if width is not None:
+            p["width"] = width
+        if height is not None:
+            p["height"] = height
+        base = native.RenderOptions()
+        base.guiding = 1 if guiding else 0
+        res = native.TuneResult()
+        self._check(self._lib.tc_autotune(self._ctx, p.ctypes.data, ctypes.byref(base), probe_samples, ctypes.byref(res)))
+        self.width, self.height = int(p["width"][0]), int(p["height"][0])
+        self.accumulated = res.probe_samples
+        b = res.best
+        return {"block_size": b.block_size, "short_stack": b.short_stack, "samples_per_item": b.samples_per_item,
+                "wave_paths": b.wave_paths, "refill_lanes": b.refill_lanes, "kernel_ms": res.best_kernel_ms,
+                "mpaths_per_s": res.best_mpaths_per_s, "candidates": res.candidates,
+                "probe_samples": res.probe_samples}
 
     def readback(self, out: Optional[np.ndarray] = None) -> np.ndarray:
         """Linear-HDR float4 image (height, width, 4)."""
