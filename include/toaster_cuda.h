@@ -243,16 +243,24 @@ int tc_autotune(tc_context* ctx, const tc_gpu_render_params* params, const tc_re
  * render_gpu_with_sink, path_tracer.rs:591-840, with its per-frame host rebuild replaced by a
  * device refit). tc_animation_create renders `first_frame` once to size every buffer, then
  * captures a frame's whole device work: the copy of the frame's geometry, camera and frame index
- * from pinned staging, the hierarchy refit, the render of `params` (plain, or guided when
+ * from pinned staging, the hierarchy update, the render of `params` (plain, or guided when
  * options->guiding is set and the context holds trained guide weights), display conversion
- * (exposure_stops) and the RGBA8 readback. update_lights != 0 also re-packs the light records
- * every frame (moving emitters). tc_animation_frame copies one evaluated frame (same counts as
- * the uploaded scene) into the staging, replays the graph and writes 4*width*height bytes to rgba
- * (may be NULL). Each frame is independent (accumulated_samples = 0) and seeded by frame_index.
- * The context must not be used by other calls while an animation replays on it. */
+ * (exposure_stops) and the RGBA8 readback. tc_animation_frame copies one evaluated frame (same
+ * counts as the uploaded scene) into the staging, replays the graph and writes 4*width*height
+ * bytes to rgba (may be NULL). Each frame is independent (accumulated_samples = 0) and seeded by
+ * frame_index. The context must not be used by other calls while an animation replays on it.
+ * flags:
+ *   TC_ANIM_UPDATE_LIGHTS  re-pack the light records every frame (moving emitters);
+ *   TC_ANIM_REBUILD        build the frame's median-split hierarchy on the host (the reference's
+ *                          per-frame build, so hits stay bit-exact) and copy it in, instead of
+ *                          refitting the first frame's tree on the device. Refit costs nothing on
+ *                          the host but its boxes loosen as primitives move apart; a rebuild keeps
+ *                          traversal cost flat at the price of a host build per frame. */
+#define TC_ANIM_UPDATE_LIGHTS 1u
+#define TC_ANIM_REBUILD 2u
 typedef struct tc_animation tc_animation;
 int tc_animation_create(tc_context* ctx, const tc_scene_data* first_frame, const tc_gpu_render_params* params,
-                        const tc_render_options* options, float exposure_stops, uint32_t update_lights,
+                        const tc_render_options* options, float exposure_stops, uint32_t flags,
                         tc_animation** out);
 int tc_animation_frame(tc_animation* anim, const tc_scene_data* frame, uint32_t frame_index, uint8_t* rgba,
                        size_t n_bytes);

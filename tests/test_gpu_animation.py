@@ -43,6 +43,24 @@ def test_graph_frames_match_direct_calls(native_lib, anim):
                 assert ra.stats()["paths"] == 320 * 180 * 8
 
 
+def test_graph_frames_with_rebuild_match_fresh_uploads(native_lib, anim):
+    # Rebuild mode builds each frame's own median-split hierarchy, the one a fresh upload builds
+    # (and the reference builds), so the two trace identical paths.
+    first = scene_to_gpu(anim.scene(0))
+    with GpuRenderer(0) as ra, GpuRenderer(0) as rd:
+        ra.upload(first)
+        with Animation(ra, first, exposure_stops=0.5, update_lights=True, rebuild=True) as a:
+            for k in (3, 25, 47):
+                data = scene_to_gpu(anim.scene(k))
+                g = a.frame(data, k)
+                rd.upload(data)
+                rd.render(frame_index=k)
+                d = rd.readback_rgba8(0.5)
+                diff = np.abs(g.astype(np.int16) - d.astype(np.int16))
+                assert diff.max() <= 1
+                assert np.mean(diff == 0) > 0.999
+
+
 def test_graph_frames_follow_the_motion(native_lib, anim):
     first = scene_to_gpu(anim.scene(0))
     with GpuRenderer(0) as r:

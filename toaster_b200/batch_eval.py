@@ -7,9 +7,10 @@ Two workloads:
   320x180 to 1280x720) rendered by one persistent launch (tc_render_batch) versus one tc_render
   per scene. Reports aggregate Mpaths/s of both.
 - ``animation``: 240 frames of 64 spheres + 64 boxes on ballistic trajectories. The graph path
-  replays one captured CUDA graph per frame (pinned staging -> refit -> render -> device display
-  conversion -> RGBA8 readback), with plain sampling and again with guided sampling (network
-  trained on frame 0); the plain unbatched path does what the reference does per frame: a full
+  replays one captured CUDA graph per frame (pinned staging -> hierarchy update -> render -> device
+  display conversion -> RGBA8 readback): with a device refit of frame 0's tree, with a per-frame
+  host rebuild, and with the rebuild and guided sampling (network trained on frame 0); the plain
+  unbatched path does what the reference does per frame: a full
   scene upload with a host hierarchy build, a plain render, a float4 readback and display
   conversion on the host. Reports per-frame latency (p50 / p99, from the packed frame records to
   RGBA8 bytes on the host) and aggregate Mpaths/s of each.
@@ -91,8 +92,12 @@ def animation(frames: int = 240, width: int = 1280, height: int = 720, samples: 
     paths = width * height * samples
     out = {"frames": frames, "width": width, "height": height, "spp": samples, "max_bounces": max_bounces,
            "primitives": int(anim.n_spheres + 2 + 12 * anim.n_boxes)}
-    # Graph path: plain sampling, then guided sampling with the network trained on frame 0.
-    for guided in ([False, True] if guiding else [False]):
+    # Graph paths: refit and per-frame rebuild with plain sampling, then rebuild with guided
+    # sampling (network trained on frame 0).
+    variants = [("graph_refit", False, False), ("graph", False, True)]
+    if guiding:
+        variants.append(("graph_guided", True, True))
+    for key, guided, rebuild in variants:
         with GpuRenderer(device) as r:
             r.upload(first)
             train_ms = 0.0
@@ -102,7 +107,7 @@ def animation(frames: int = 240, width: int = 1280, height: int = 720, samples: 
                 r.guide_train_recorded(train_steps, 8192, 1e-2, 1)
                 train_ms = r.stats()["kernel_ms"]
             lat = []
-            with Animation(r, first, guiding=guided, update_lights=True) as a:
+            with Animation(r, first, guiding=guided, update_lights=True, rebuild=rebuild) as a:
                 img = np.empty((height, width, 4), np.uint8)
                 a.frame(first, 0, img)  # warm-up replay
                 for k in range(frames):
@@ -111,8 +116,9 @@ def animation(frames: int = 240, width: int = 1280, height: int = 720, samples: 
                     a.frame(data, k, img)
                     lat.append((time.perf_counter() - t) * 1e3)
             lat = np.array(lat)
-            out["graph_guided" if guided else "graph"] = {
-                "guided": guided, "train_ms": train_ms, "p50_ms": float(np.percentile(lat, 50)),
+            out[key] = {
+                "guided": guided, "hierarchy": "rebuild" if rebuild else "refit", "train_ms": train_ms,
+                "p50_ms": float(np.percentile(lat, 50)),
                 "p99_ms": float(np.percentile(lat, 99)), "mean_ms": float(lat.mean()),
                 "mpaths_per_s": paths * frames / (lat.sum() * 1e3)}
     # Plain unbatched path (the reference's per-frame flow).

@@ -80,6 +80,7 @@ struct tc_context {
   DevBuf env_rgb, env_marginal, env_conditional, env_pdf, env_row_sums, env_total;
   uint32_t sphere_count = 0, triangle_count = 0, material_count = 0, light_count = 0, bvh_prims = 0;
   uint32_t bvh_depth = 0;
+  size_t pair_count = 0;
   bool any_attr = false;
   // Geometry refit (tc_update_geometry): the root record, the scene-order geometry the prim
   // records are rewritten from, and pair-node indices grouped by depth.
@@ -284,6 +285,56 @@ int check_render_params(tc_context* ctx, const tc_gpu_render_params* p) {
   return TC_OK;
 }
 
+// Device hierarchy of a scene: the caller's flat BVH in the reference layout (when given and
+// use_given is set) or a fresh median-split build (crates/toaster-bvh/src/bvh.rs:92-154).
+int build_hierarchy(tc_context* ctx, const tc_scene_data* sd, bool use_given, tcb::DeviceHierarchy& dh) {
+  std::vector<tcb::SphereIn> sph(sd->sphere_count);
+  std::vector<uint32_t> sph_mat(sd->sphere_count);
+  for (size_t i = 0; i < sd->sphere_count; ++i) {
+    const tc_gpu_sphere& s = sd->spheres[i];
+    sph[i] = tcb::SphereIn{{s.center_radius[0], s.center_radius[1], s.center_radius[2]}, s.center_radius[3]};
+    sph_mat[i] = s.material_index;
+  }
+  std::vector<tcb::TriangleIn> tri(sd->triangle_count);
+  std::vector<uint32_t> tri_mat(sd->triangle_count), tri_flags(sd->triangle_count, 0u);
+  for (size_t i = 0; i < sd->triangle_count; ++i) {
+    const tc_gpu_triangle& t = sd->triangles[i];
+    for (int c = 0; c < 3; ++c) {
+      tri[i].v[0][c] = t.v0[c];
+      tri[i].v[1][c] = t.v1[c];
+      tri[i].v[2][c] = t.v2[c];
+    }
+    tri_mat[i] = t.material_index;
+    if (sd->triangle_attributes) tri_flags[i] = sd->triangle_attributes[i].flags & 3u;
+  }
+  tcb::FlatHierarchy flat;
+  if (use_given && sd->bvh_nodes && sd->bvh_node_count) {
+    if (!sd->bvh_primitives || sd->bvh_primitive_count != sd->sphere_count + sd->triangle_count)
+      return fail(ctx, TC_ERR_INVALID, "BVH primitive references must cover every sphere and triangle");
+    flat.nodes.resize(sd->bvh_node_count);
+    for (size_t i = 0; i < sd->bvh_node_count; ++i) {
+      const tc_gpu_bvh_node& n = sd->bvh_nodes[i];
+      tcb::FlatNode& f = flat.nodes[i];
+      for (int c = 0; c < 3; ++c) {
+        f.min[c] = n.min[c];
+        f.max[c] = n.max[c];
+      }
+      f.first_or_right = n.first_or_right;
+      f.count = n.primitive_count;
+    }
+    flat.prims.resize(sd->bvh_primitive_count);
+    for (size_t i = 0; i < sd->bvh_primitive_count; ++i)
+      flat.prims[i] = tcb::PrimRef{sd->bvh_primitives[i].kind, sd->bvh_primitives[i].index};
+  } else {
+    flat = tcb::build_median_split(sph.data(), sph.size(), tri.data(), tri.size());
+  }
+  std::string err;
+  if (!tcb::to_device_layout(flat, sph.data(), sph_mat.data(), sph.size(), tri.data(), tri_mat.data(),
+                             tri_flags.data(), tri.size(), dh, err))
+    return fail(ctx, TC_ERR_INVALID, err);
+  return TC_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -419,51 +470,8 @@ int tc_upload_scene(tc_context* ctx, const tc_scene_data* sd) {
   }
 
   // Hierarchy: the caller's (reference layout) or a fresh median-split build.
-  std::vector<tcb::SphereIn> sph(sd->sphere_count);
-  std::vector<uint32_t> sph_mat(sd->sphere_count);
-  for (size_t i = 0; i < sd->sphere_count; ++i) {
-    const tc_gpu_sphere& s = sd->spheres[i];
-    sph[i] = tcb::SphereIn{{s.center_radius[0], s.center_radius[1], s.center_radius[2]}, s.center_radius[3]};
-    sph_mat[i] = s.material_index;
-  }
-  std::vector<tcb::TriangleIn> tri(sd->triangle_count);
-  std::vector<uint32_t> tri_mat(sd->triangle_count), tri_flags(sd->triangle_count, 0u);
-  for (size_t i = 0; i < sd->triangle_count; ++i) {
-    const tc_gpu_triangle& t = sd->triangles[i];
-    for (int c = 0; c < 3; ++c) {
-      tri[i].v[0][c] = t.v0[c];
-      tri[i].v[1][c] = t.v1[c];
-      tri[i].v[2][c] = t.v2[c];
-    }
-    tri_mat[i] = t.material_index;
-    if (sd->triangle_attributes) tri_flags[i] = sd->triangle_attributes[i].flags & 3u;
-  }
-  tcb::FlatHierarchy flat;
-  if (sd->bvh_nodes && sd->bvh_node_count) {
-    if (!sd->bvh_primitives || sd->bvh_primitive_count != sd->sphere_count + sd->triangle_count)
-      return fail(ctx, TC_ERR_INVALID, "BVH primitive references must cover every sphere and triangle");
-    flat.nodes.resize(sd->bvh_node_count);
-    for (size_t i = 0; i < sd->bvh_node_count; ++i) {
-      const tc_gpu_bvh_node& n = sd->bvh_nodes[i];
-      tcb::FlatNode& f = flat.nodes[i];
-      for (int c = 0; c < 3; ++c) {
-        f.min[c] = n.min[c];
-        f.max[c] = n.max[c];
-      }
-      f.first_or_right = n.first_or_right;
-      f.count = n.primitive_count;
-    }
-    flat.prims.resize(sd->bvh_primitive_count);
-    for (size_t i = 0; i < sd->bvh_primitive_count; ++i)
-      flat.prims[i] = tcb::PrimRef{sd->bvh_primitives[i].kind, sd->bvh_primitives[i].index};
-  } else {
-    flat = tcb::build_median_split(sph.data(), sph.size(), tri.data(), tri.size());
-  }
   tcb::DeviceHierarchy dh;
-  std::string err;
-  if (!tcb::to_device_layout(flat, sph.data(), sph_mat.data(), sph.size(), tri.data(), tri_mat.data(),
-                             tri_flags.data(), tri.size(), dh, err))
-    return fail(ctx, TC_ERR_INVALID, err);
+  if (int rc = build_hierarchy(ctx, sd, true, dh)) return rc;
 
   // Lights: alias table over the GpuLight weights (light.rs:57-113 distribution).
   std::vector<tcb::DevLight> lights;
@@ -476,7 +484,8 @@ int tc_upload_scene(tc_context* ctx, const tc_scene_data* sd) {
   TC_CUDA(ctx, upload(ctx->materials, mats.data(), mats.size(), st));
   TC_CUDA(ctx, upload(ctx->lights, lights.data(), lights.size(), st));
   bool any_attr = false;
-  for (uint32_t f : tri_flags) any_attr |= f != 0u;
+  if (sd->triangle_attributes)
+    for (size_t i = 0; i < sd->triangle_count; ++i) any_attr |= (sd->triangle_attributes[i].flags & 3u) != 0u;
   TC_CUDA(ctx, upload(ctx->root_buf, &dh.root, 1, st));
   {
     // Pair nodes grouped by depth, root first, for the bottom-up refit.
@@ -551,10 +560,11 @@ int tc_upload_scene(tc_context* ctx, const tc_scene_data* sd) {
   ctx->triangle_count = uint32_t(sd->triangle_count);
   ctx->material_count = n_mat;
   ctx->light_count = uint32_t(sd->light_count);
-  ctx->bvh_prims = uint32_t(flat.prims.size());
+  ctx->bvh_prims = uint32_t(dh.prims.size());
   ctx->bvh_depth = dh.depth;
   ctx->stats.bvh_depth = dh.depth;
   ctx->any_attr = any_attr;
+  ctx->pair_count = dh.pairs.size();
   ctx->raw_spheres_valid = ctx->raw_triangles_valid = false;
   return TC_OK;
 }
@@ -939,10 +949,15 @@ struct tc_animation {
   tc_render_options options{};
   float exposure = 0.0f;
   bool update_lights = false;
+  bool rebuild = false;                     // per-frame median-split build instead of a refit
   size_t npix = 0;
   tc_gpu_sphere* h_spheres = nullptr;       // pinned staging
   tc_gpu_triangle* h_triangles = nullptr;
   tcb::DevLight* h_lights = nullptr;
+  tcb::PairNode* h_pairs = nullptr;         // rebuilt hierarchy (rebuild mode)
+  tcb::PrimRecord* h_prims = nullptr;
+  tcb::ChildRec* h_root = nullptr;
+  tc_gpu_triangle_attributes* h_attrs = nullptr;
   float* h_frame = nullptr;                 // camera (16 floats) then the frame index (uint32)
   uint8_t* h_rgba = nullptr;                // pinned output
   unsigned long long* h_counters = nullptr;
@@ -957,7 +972,9 @@ static void animation_free(tc_animation* a) {
   if (a->exec) cudaGraphExecDestroy(a->exec);
   if (a->graph) cudaGraphDestroy(a->graph);
   for (void* h : {static_cast<void*>(a->h_spheres), static_cast<void*>(a->h_triangles), static_cast<void*>(a->h_lights),
-                  static_cast<void*>(a->h_frame), static_cast<void*>(a->h_rgba), static_cast<void*>(a->h_counters)})
+                  static_cast<void*>(a->h_pairs), static_cast<void*>(a->h_prims), static_cast<void*>(a->h_root),
+                  static_cast<void*>(a->h_attrs), static_cast<void*>(a->h_frame), static_cast<void*>(a->h_rgba),
+                  static_cast<void*>(a->h_counters)})
     if (h) cudaFreeHost(h);
   delete a;
 }
@@ -972,8 +989,24 @@ static int animation_stage(tc_animation* a, const tc_scene_data* sd, uint32_t fr
   if ((sd->sphere_count && !sd->spheres) || (sd->triangle_count && !sd->triangles) || !sd->materials)
     return fail(ctx, TC_ERR_INVALID, "frame geometry or material pointer is null");
   if (int rc = validate_geometry(ctx, sd, ctx->material_count)) return rc;
-  if (sd->sphere_count) std::memcpy(a->h_spheres, sd->spheres, sizeof(tc_gpu_sphere) * sd->sphere_count);
-  if (sd->triangle_count) std::memcpy(a->h_triangles, sd->triangles, sizeof(tc_gpu_triangle) * sd->triangle_count);
+  if (a->rebuild) {
+    // The median-split tree's shape depends on the primitive count alone (degenerate-extent
+    // leaves aside), so the rebuilt hierarchy fills the same pair and record slots every frame.
+    tcb::DeviceHierarchy dh;
+    if (int rc = build_hierarchy(ctx, sd, false, dh)) return rc;
+    if (dh.pairs.size() != ctx->pair_count || dh.prims.size() != ctx->bvh_prims)
+      return fail(ctx, TC_ERR_INVALID, "the frame's hierarchy has " + std::to_string(dh.pairs.size()) +
+                                           " interior nodes, the uploaded one " + std::to_string(ctx->pair_count) +
+                                           " (degenerate leaves): upload the scene again");
+    if (!dh.pairs.empty()) std::memcpy(a->h_pairs, dh.pairs.data(), sizeof(tcb::PairNode) * dh.pairs.size());
+    if (!dh.prims.empty()) std::memcpy(a->h_prims, dh.prims.data(), sizeof(tcb::PrimRecord) * dh.prims.size());
+    *a->h_root = dh.root;
+  } else {
+    if (sd->sphere_count) std::memcpy(a->h_spheres, sd->spheres, sizeof(tc_gpu_sphere) * sd->sphere_count);
+    if (sd->triangle_count) std::memcpy(a->h_triangles, sd->triangles, sizeof(tc_gpu_triangle) * sd->triangle_count);
+  }
+  if (a->h_attrs && sd->triangle_attributes)
+    std::memcpy(a->h_attrs, sd->triangle_attributes, sizeof(tc_gpu_triangle_attributes) * sd->triangle_count);
   if (a->update_lights && sd->light_count) {
     std::vector<tcb::DevLight> lights;
     if (int rc = pack_lights(ctx, sd, ctx->material_count, lights)) return rc;
@@ -994,21 +1027,34 @@ static int animation_stage(tc_animation* a, const tc_scene_data* sd, uint32_t fr
 static int animation_enqueue(tc_animation* a, cudaStream_t st) {
   tc_context* ctx = a->ctx;
   TC_CUDA(ctx, cudaMemcpyAsync(a->d_frame.ptr, a->h_frame, 20 * sizeof(float), cudaMemcpyHostToDevice, st));
-  if (ctx->sphere_count)
-    TC_CUDA(ctx, cudaMemcpyAsync(ctx->raw_spheres.ptr, a->h_spheres, sizeof(tc_gpu_sphere) * ctx->sphere_count,
-                                 cudaMemcpyHostToDevice, st));
-  if (ctx->triangle_count)
-    TC_CUDA(ctx, cudaMemcpyAsync(ctx->raw_triangles.ptr, a->h_triangles, sizeof(tc_gpu_triangle) * ctx->triangle_count,
-                                 cudaMemcpyHostToDevice, st));
   if (a->update_lights && ctx->light_count)
     TC_CUDA(ctx, cudaMemcpyAsync(ctx->lights.ptr, a->h_lights, sizeof(tcb::DevLight) * ctx->light_count,
                                  cudaMemcpyHostToDevice, st));
-  tcb::RefitPlan plan;
-  plan.nodes = ctx->refit_nodes.as<uint32_t>();
-  plan.level_offsets = ctx->refit_levels;
-  TC_CUDA(ctx, tcb::launch_refit(plan, ctx->pairs.as<tcb::PairNode>(), ctx->root_buf.as<tcb::ChildRec>(),
-                                 ctx->prims.as<tcb::PrimRecord>(), ctx->bvh_prims, ctx->raw_spheres.as<tc_gpu_sphere>(),
-                                 ctx->raw_triangles.as<tc_gpu_triangle>(), st));
+  if (a->h_attrs)
+    TC_CUDA(ctx, cudaMemcpyAsync(ctx->attributes.ptr, a->h_attrs,
+                                 sizeof(tc_gpu_triangle_attributes) * ctx->triangle_count, cudaMemcpyHostToDevice, st));
+  if (a->rebuild) {
+    if (ctx->pair_count)
+      TC_CUDA(ctx, cudaMemcpyAsync(ctx->pairs.ptr, a->h_pairs, sizeof(tcb::PairNode) * ctx->pair_count,
+                                   cudaMemcpyHostToDevice, st));
+    if (ctx->bvh_prims)
+      TC_CUDA(ctx, cudaMemcpyAsync(ctx->prims.ptr, a->h_prims, sizeof(tcb::PrimRecord) * ctx->bvh_prims,
+                                   cudaMemcpyHostToDevice, st));
+    TC_CUDA(ctx, cudaMemcpyAsync(ctx->root_buf.ptr, a->h_root, sizeof(tcb::ChildRec), cudaMemcpyHostToDevice, st));
+  } else {
+    if (ctx->sphere_count)
+      TC_CUDA(ctx, cudaMemcpyAsync(ctx->raw_spheres.ptr, a->h_spheres, sizeof(tc_gpu_sphere) * ctx->sphere_count,
+                                   cudaMemcpyHostToDevice, st));
+    if (ctx->triangle_count)
+      TC_CUDA(ctx, cudaMemcpyAsync(ctx->raw_triangles.ptr, a->h_triangles,
+                                   sizeof(tc_gpu_triangle) * ctx->triangle_count, cudaMemcpyHostToDevice, st));
+    tcb::RefitPlan plan;
+    plan.nodes = ctx->refit_nodes.as<uint32_t>();
+    plan.level_offsets = ctx->refit_levels;
+    TC_CUDA(ctx, tcb::launch_refit(plan, ctx->pairs.as<tcb::PairNode>(), ctx->root_buf.as<tcb::ChildRec>(),
+                                   ctx->prims.as<tcb::PrimRecord>(), ctx->bvh_prims,
+                                   ctx->raw_spheres.as<tc_gpu_sphere>(), ctx->raw_triangles.as<tc_gpu_triangle>(), st));
+  }
   const float* cam = a->d_frame.as<float>();
   const uint32_t* fi = reinterpret_cast<const uint32_t*>(cam + 16);
   if (int rc = enqueue_render(ctx, &a->params, a->options, st, false, fi, cam, a->h_counters)) return rc;
@@ -1019,7 +1065,7 @@ static int animation_enqueue(tc_animation* a, cudaStream_t st) {
 }
 
 int tc_animation_create(tc_context* ctx, const tc_scene_data* first_frame, const tc_gpu_render_params* params,
-                        const tc_render_options* options, float exposure_stops, uint32_t update_lights,
+                        const tc_render_options* options, float exposure_stops, uint32_t flags,
                         tc_animation** out) {
   if (!ctx) return fail(nullptr, TC_ERR_INVALID, "context is null");
   if (!out || !first_frame) return fail(ctx, TC_ERR_INVALID, "first frame or output pointer is null");
@@ -1037,7 +1083,8 @@ int tc_animation_create(tc_context* ctx, const tc_scene_data* first_frame, const
   a->params.accumulated_samples = 0;
   a->options = o;
   a->exposure = exposure_stops;
-  a->update_lights = update_lights != 0;
+  a->update_lights = (flags & TC_ANIM_UPDATE_LIGHTS) != 0;
+  a->rebuild = (flags & TC_ANIM_REBUILD) != 0;
   a->npix = size_t(params->width) * params->height;
   cudaError_t e = cudaSuccess;
   auto host = [&](void** p, size_t bytes) {
@@ -1046,6 +1093,12 @@ int tc_animation_create(tc_context* ctx, const tc_scene_data* first_frame, const
   host(reinterpret_cast<void**>(&a->h_spheres), sizeof(tc_gpu_sphere) * ctx->sphere_count);
   host(reinterpret_cast<void**>(&a->h_triangles), sizeof(tc_gpu_triangle) * ctx->triangle_count);
   host(reinterpret_cast<void**>(&a->h_lights), sizeof(tcb::DevLight) * ctx->light_count);
+  if (a->rebuild) {
+    host(reinterpret_cast<void**>(&a->h_pairs), sizeof(tcb::PairNode) * ctx->pair_count);
+    host(reinterpret_cast<void**>(&a->h_prims), sizeof(tcb::PrimRecord) * ctx->bvh_prims);
+    host(reinterpret_cast<void**>(&a->h_root), sizeof(tcb::ChildRec));
+  }
+  if (ctx->any_attr) host(reinterpret_cast<void**>(&a->h_attrs), sizeof(tc_gpu_triangle_attributes) * ctx->triangle_count);
   host(reinterpret_cast<void**>(&a->h_frame), 20 * sizeof(float));
   host(reinterpret_cast<void**>(&a->h_rgba), 4 * a->npix);
   host(reinterpret_cast<void**>(&a->h_counters), 4 * sizeof(unsigned long long));

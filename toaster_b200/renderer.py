@@ -28,7 +28,8 @@ class Animation:
 
     def __init__(self, renderer: "GpuRenderer", first: SceneGpuData, samples: Optional[int] = None,
                  max_bounces: Optional[int] = None, exposure_stops: float = 0.0, guiding: bool = False,
-                 update_lights: bool = False, block_size: int = 0, wave_paths: int = 0, refill_lanes: int = 0):
+                 update_lights: bool = False, block_size: int = 0, wave_paths: int = 0, refill_lanes: int = 0,
+                 rebuild: bool = False):
         self._r = renderer
         self._lib = renderer._lib
         self._h = None
@@ -47,7 +48,8 @@ class Animation:
         sd, keep = GpuRenderer._scene_struct(first)
         h = ctypes.c_void_p()
         renderer._check(self._lib.tc_animation_create(renderer._ctx, ctypes.byref(sd), p.ctypes.data, ctypes.byref(opts),
-                                                      float(exposure_stops), int(update_lights), ctypes.byref(h)))
+                                                      float(exposure_stops), int(update_lights) | (2 if rebuild else 0),
+                                                      ctypes.byref(h)))
         self._h = h
 
     def frame(self, data: SceneGpuData, frame_index: int, out: Optional[np.ndarray] = None) -> np.ndarray:
