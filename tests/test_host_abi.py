@@ -139,3 +139,37 @@ def test_camera_packing_matches_oracle():  # scene_upload.rs:352-368 vs camera.r
     ref = camera_basis(s.camera_position, s.camera_look_at, s.camera_up, s.fov_degrees, s.width / s.height)
     got = np.stack([cam["origin"][:3], cam["lower_left_corner"][:3], cam["horizontal"][:3], cam["vertical"][:3]])
     assert np.allclose(got, ref, rtol=0, atol=1e-6)
+
+
+def test_host_display_conversion_of_the_baseline_matches_oracle():
+    # The plain unbatched animation path converts on the host as the reference does; it must give
+    # the oracle's bytes (color.rs:24-74) so latency comparisons compare equal work.
+    from oracle import binding as ob
+    from toaster_b200.batch_eval import host_display_rgba8
+
+    rng = np.random.default_rng(3)
+    hdr = np.concatenate([rng.exponential(0.5, (64, 96, 3)), np.ones((64, 96, 1))], -1).astype(np.float32)
+    hdr[0, 0, :3] = [np.nan, np.inf, -1.0]
+    for exposure in (0.0, 1.5, -2.0):
+        ref = ob.display_rgba8(hdr.reshape(-1, 4), exposure).reshape(hdr.shape)
+        got = host_display_rgba8(hdr, exposure)
+        assert np.abs(ref.astype(int) - got.astype(int)).max() <= 1
+        assert np.mean(ref == got) > 0.999
+
+
+def test_ballistic_animation_is_deterministic_and_keeps_counts():
+    a = configs.BallisticAnimation(frames=24, width=64, height=36)
+    b = configs.BallisticAnimation(frames=24, width=64, height=36)
+    s0, s23 = a.scene(0), a.scene(23)
+    assert s0.sphere_count == s23.sphere_count == 64
+    assert s0.triangle_count == s23.triangle_count == 2 + 64 * 12
+    assert np.array_equal(a.scene(17).triangles, b.scene(17).triangles)
+    assert not np.array_equal(s0.sphere_centers, s23.sphere_centers)
+    assert np.all(s23.sphere_centers[:, 1] >= s23.sphere_radii - 1e-5)  # bodies stay above the ground
+
+
+def test_uneven_batch_spans_sizes():
+    scenes = configs.uneven_batch(count=4, seed=1)
+    for s in scenes:
+        assert 128 <= s.triangle_count <= 262144
+        assert 320 <= s.width <= 1280 and s.width % 16 == 0 and s.height == s.width * 9 // 16

@@ -35,9 +35,11 @@ def host_display_rgba8(hdr: np.ndarray, exposure_stops: float = 0.0) -> np.ndarr
     """Host display conversion as the reference does it after readback (color.rs:24-74):
     exposure, ACES fitted, clamp, sRGB transfer, rounding."""
     rgb = hdr[..., :3].astype(np.float32) * np.float32(2.0 ** exposure_stops)
-    rgb = np.nan_to_num(rgb, nan=0.0, posinf=1.0, neginf=0.0)
-    c = np.maximum(rgb, 0.0)
-    t = np.clip((c * (2.51 * c + 0.03)) / (c * (2.43 * c + 0.59) + 0.14), 0.0, 1.0)
+    finite = np.isfinite(rgb)
+    c = np.maximum(np.where(finite, rgb, 0.0), 0.0)
+    with np.errstate(invalid="ignore"):
+        t = np.clip((c * (2.51 * c + 0.03)) / (c * (2.43 * c + 0.59) + 0.14), 0.0, 1.0)
+    t = np.where(finite, t, np.where(rgb == np.inf, 1.0, 0.0))  # NaN and -inf map to 0, +inf to 1
     s = np.where(t <= 0.0031308, 12.92 * t, 1.055 * np.power(t, 1.0 / 2.4) - 0.055)
     out = np.empty(hdr.shape[:-1] + (4,), np.uint8)
     out[..., :3] = np.round(np.clip(s, 0.0, 1.0) * 255.0)
