@@ -183,6 +183,14 @@ int tc_set_stream(tc_context* ctx, void* stream);
  * (crates/toaster-gpu/src/buffers.rs:117-271, path_tracer.rs:676-721). */
 int tc_upload_scene(tc_context* ctx, const tc_scene_data* scene);
 
+/* Where tc_upload_scene builds the median-split hierarchy when the scene brings none: 0 = on the
+ * device for scenes of at least 4,096 primitives, on the host below (default); 1 = always on the
+ * host; 2 = always on the device. Both builds produce the reference's tree (same topology,
+ * primitive order and bounds). The device build runs level by level with a segmented stable
+ * sort; a node whose centroids all coincide (a degenerate leaf of the reference) makes it fall
+ * back to the host build. Replaces the host-side FlatBvh::build of scene_upload.rs:296-340. */
+int tc_set_hierarchy_build(tc_context* ctx, int mode);
+
 /* Replaces the camera write_buffer (path_tracer.rs:680-684). */
 int tc_set_camera(tc_context* ctx, const tc_gpu_camera* camera);
 
@@ -251,11 +259,12 @@ int tc_autotune(tc_context* ctx, const tc_gpu_render_params* params, const tc_re
  * frame_index. The context must not be used by other calls while an animation replays on it.
  * flags:
  *   TC_ANIM_UPDATE_LIGHTS  re-pack the light records every frame (moving emitters);
- *   TC_ANIM_REBUILD        build the frame's median-split hierarchy on the host (the reference's
- *                          per-frame build, so hits stay bit-exact) and copy it in, instead of
- *                          refitting the first frame's tree on the device. Refit costs nothing on
- *                          the host but its boxes loosen as primitives move apart; a rebuild keeps
- *                          traversal cost flat at the price of a host build per frame. */
+ *   TC_ANIM_REBUILD        build the frame's median-split hierarchy on the device inside the graph
+ *                          (the reference's per-frame tree, so hits stay bit-exact) instead of
+ *                          refitting the first frame's tree. A refit is cheaper, but its boxes
+ *                          loosen as primitives move apart; a rebuild keeps traversal cost flat.
+ *                          A frame whose tree would need a degenerate leaf fails with
+ *                          TC_ERR_DEVICE_STATUS. */
 #define TC_ANIM_UPDATE_LIGHTS 1u
 #define TC_ANIM_REBUILD 2u
 typedef struct tc_animation tc_animation;

@@ -19,7 +19,8 @@ from pathlib import Path
 PKG = Path(__file__).resolve().parent
 CSRC = PKG / "csrc"
 LIB = PKG / "lib"
-SOURCES = ["api.cu", "kernels.cu", "guide.cu", "umma_selftest.cu", "display.cu", "refit.cu", "bvh_build.cpp"]
+SOURCES = ["api.cu", "kernels.cu", "guide.cu", "umma_selftest.cu", "display.cu", "refit.cu", "bvh_device.cu",
+           "bvh_build.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

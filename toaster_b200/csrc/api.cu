@@ -14,6 +14,7 @@
 
 #include "../../include/toaster_cuda.h"
 #include "bvh_build.h"
+#include "bvh_device.h"
 #include "device_scene.h"
 #include "display.h"
 #include "guide.h"
@@ -34,6 +35,8 @@ namespace {
 
 // Default dynamic-fetch threshold of the path kernel (tc_render_options.refill_lanes).
 constexpr int kDefaultRefillLanes = 1;
+// Scenes with at least this many primitives build their hierarchy on the device by default.
+constexpr size_t kDeviceBuildMin = 4096;
 
 thread_local std::string g_thread_error;
 
@@ -89,6 +92,12 @@ struct tc_context {
   bool raw_spheres_valid = false, raw_triangles_valid = false;
   // Display conversion output (packed RGBA8) and the job table of batched launches.
   DevBuf display, batch_jobs;
+  // Device hierarchy build (tc_set_hierarchy_build): mode, builder, triangle attribute flags and
+  // its status word.
+  int build_mode = 0;
+  bool device_built = false;
+  tcb::DeviceBvhBuilder builder;
+  DevBuf attr_flags, build_status;
 
   // Accumulation state (progressive contract of path_tracer.rs:900-923)
   uint32_t width = 0, height = 0, accumulated = 0;
@@ -469,25 +478,65 @@ int tc_upload_scene(tc_context* ctx, const tc_scene_data* sd) {
     mats[i] = d;
   }
 
-  // Hierarchy: the caller's (reference layout) or a fresh median-split build.
-  tcb::DeviceHierarchy dh;
-  if (int rc = build_hierarchy(ctx, sd, true, dh)) return rc;
-
   // Lights: alias table over the GpuLight weights (light.rs:57-113 distribution).
   std::vector<tcb::DevLight> lights;
   if (int rc = pack_lights(ctx, sd, n_mat, lights)) return rc;
 
-  // Upload.
   cudaStream_t st = ctx->stream;
-  TC_CUDA(ctx, upload(ctx->pairs, dh.pairs.data(), dh.pairs.size(), st));
-  TC_CUDA(ctx, upload(ctx->prims, dh.prims.data(), dh.prims.size(), st));
-  TC_CUDA(ctx, upload(ctx->materials, mats.data(), mats.size(), st));
-  TC_CUDA(ctx, upload(ctx->lights, lights.data(), lights.size(), st));
   bool any_attr = false;
   if (sd->triangle_attributes)
     for (size_t i = 0; i < sd->triangle_count; ++i) any_attr |= (sd->triangle_attributes[i].flags & 3u) != 0u;
-  TC_CUDA(ctx, upload(ctx->root_buf, &dh.root, 1, st));
-  {
+
+  // Hierarchy: the caller's (reference layout), or the median-split build, on the device
+  // (tc_set_hierarchy_build) or on the host. A device build that meets a degenerate node falls
+  // back to the host build, which makes such nodes leaves.
+  const size_t n_prims = sd->sphere_count + sd->triangle_count;
+  const bool given = sd->bvh_nodes && sd->bvh_node_count;
+  const bool on_device = !given && (ctx->build_mode == 2 || (ctx->build_mode == 0 && n_prims >= kDeviceBuildMin));
+  bool built = false;
+  uint32_t pair_count = 0, prim_count = 0, depth = 0;
+  if (on_device) {
+    TC_CUDA(ctx, ctx->builder.plan(uint32_t(sd->sphere_count), uint32_t(sd->triangle_count)));
+    TC_CUDA(ctx, upload(ctx->raw_spheres, sd->spheres, sd->sphere_count, st));
+    TC_CUDA(ctx, upload(ctx->raw_triangles, sd->triangles, sd->triangle_count, st));
+    const uint32_t* flags = nullptr;
+    if (any_attr) {
+      std::vector<uint32_t> f(sd->triangle_count);
+      for (size_t i = 0; i < f.size(); ++i) f[i] = sd->triangle_attributes[i].flags & 3u;
+      TC_CUDA(ctx, upload(ctx->attr_flags, f.data(), f.size(), st));
+      TC_CUDA(ctx, cudaStreamSynchronize(st));
+      flags = ctx->attr_flags.as<uint32_t>();
+    }
+    TC_CUDA(ctx, ctx->pairs.reserve(sizeof(tcb::PairNode) * std::max<size_t>(ctx->builder.pair_count(), 1)));
+    TC_CUDA(ctx, ctx->prims.reserve(sizeof(tcb::PrimRecord) * n_prims));
+    TC_CUDA(ctx, ctx->root_buf.reserve(sizeof(tcb::ChildRec)));
+    TC_CUDA(ctx, ctx->build_status.reserve(sizeof(uint32_t)));
+    TC_CUDA(ctx, cudaMemsetAsync(ctx->build_status.ptr, 0, sizeof(uint32_t), st));
+    TC_CUDA(ctx, ctx->builder.build(ctx->raw_spheres.as<tc_gpu_sphere>(), ctx->raw_triangles.as<tc_gpu_triangle>(),
+                                    flags, ctx->pairs.as<tcb::PairNode>(), ctx->root_buf.as<tcb::ChildRec>(),
+                                    ctx->prims.as<tcb::PrimRecord>(), ctx->build_status.as<uint32_t>(), st));
+    uint32_t degenerate = 0;
+    TC_CUDA(ctx, cudaMemcpyAsync(&degenerate, ctx->build_status.ptr, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+    TC_CUDA(ctx, cudaStreamSynchronize(st));
+    if (!degenerate) {
+      built = true;
+      pair_count = ctx->builder.pair_count();
+      prim_count = uint32_t(n_prims);
+      depth = ctx->builder.depth();
+      const size_t refit_count = ctx->builder.refit_levels().back();
+      TC_CUDA(ctx, ctx->refit_nodes.reserve(sizeof(uint32_t) * std::max<size_t>(refit_count, 1)));
+      if (refit_count)
+        TC_CUDA(ctx, cudaMemcpyAsync(ctx->refit_nodes.ptr, ctx->builder.refit_nodes(), sizeof(uint32_t) * refit_count,
+                                     cudaMemcpyDeviceToDevice, st));
+      ctx->refit_levels = ctx->builder.refit_levels();
+    }
+  }
+  if (!built) {
+    tcb::DeviceHierarchy dh;
+    if (int rc = build_hierarchy(ctx, sd, true, dh)) return rc;
+    TC_CUDA(ctx, upload(ctx->pairs, dh.pairs.data(), dh.pairs.size(), st));
+    TC_CUDA(ctx, upload(ctx->prims, dh.prims.data(), dh.prims.size(), st));
+    TC_CUDA(ctx, upload(ctx->root_buf, &dh.root, 1, st));
     // Pair nodes grouped by depth, root first, for the bottom-up refit.
     std::vector<uint32_t> order, offsets{0u};
     if (!(dh.root.link & tcb::kLeafBit)) {
@@ -504,7 +553,12 @@ int tc_upload_scene(tc_context* ctx, const tc_scene_data* sd) {
     }
     TC_CUDA(ctx, upload(ctx->refit_nodes, order.data(), order.size(), st));
     ctx->refit_levels = std::move(offsets);
+    pair_count = uint32_t(dh.pairs.size());
+    prim_count = uint32_t(dh.prims.size());
+    depth = dh.depth;
   }
+  TC_CUDA(ctx, upload(ctx->materials, mats.data(), mats.size(), st));
+  TC_CUDA(ctx, upload(ctx->lights, lights.data(), lights.size(), st));
   if (any_attr) TC_CUDA(ctx, upload(ctx->attributes, sd->triangle_attributes, sd->triangle_count, st));
   if (sd->texture_pixels && sd->texture_pixel_count)
     TC_CUDA(ctx, upload(ctx->texels, sd->texture_pixels, sd->texture_pixel_count, st));
@@ -560,12 +614,20 @@ int tc_upload_scene(tc_context* ctx, const tc_scene_data* sd) {
   ctx->triangle_count = uint32_t(sd->triangle_count);
   ctx->material_count = n_mat;
   ctx->light_count = uint32_t(sd->light_count);
-  ctx->bvh_prims = uint32_t(dh.prims.size());
-  ctx->bvh_depth = dh.depth;
-  ctx->stats.bvh_depth = dh.depth;
+  ctx->bvh_prims = prim_count;
+  ctx->bvh_depth = depth;
+  ctx->stats.bvh_depth = depth;
   ctx->any_attr = any_attr;
-  ctx->pair_count = dh.pairs.size();
-  ctx->raw_spheres_valid = ctx->raw_triangles_valid = false;
+  ctx->pair_count = pair_count;
+  ctx->device_built = built && on_device;
+  ctx->raw_spheres_valid = ctx->raw_triangles_valid = ctx->device_built;
+  return TC_OK;
+}
+
+int tc_set_hierarchy_build(tc_context* ctx, int mode) {
+  if (!ctx) return fail(nullptr, TC_ERR_INVALID, "context is null");
+  if (mode < 0 || mode > 2) return fail(ctx, TC_ERR_INVALID, "hierarchy build mode must be 0 (auto), 1 (host) or 2 (device)");
+  ctx->build_mode = mode;
   return TC_OK;
 }
 
@@ -954,10 +1016,9 @@ struct tc_animation {
   tc_gpu_sphere* h_spheres = nullptr;       // pinned staging
   tc_gpu_triangle* h_triangles = nullptr;
   tcb::DevLight* h_lights = nullptr;
-  tcb::PairNode* h_pairs = nullptr;         // rebuilt hierarchy (rebuild mode)
-  tcb::PrimRecord* h_prims = nullptr;
-  tcb::ChildRec* h_root = nullptr;
   tc_gpu_triangle_attributes* h_attrs = nullptr;
+  uint32_t* h_attr_flags = nullptr;         // rebuild mode: the build's triangle attribute flags
+  uint32_t* h_status = nullptr;             // rebuild mode: the device build's status word
   float* h_frame = nullptr;                 // camera (16 floats) then the frame index (uint32)
   uint8_t* h_rgba = nullptr;                // pinned output
   unsigned long long* h_counters = nullptr;
@@ -972,9 +1033,8 @@ static void animation_free(tc_animation* a) {
   if (a->exec) cudaGraphExecDestroy(a->exec);
   if (a->graph) cudaGraphDestroy(a->graph);
   for (void* h : {static_cast<void*>(a->h_spheres), static_cast<void*>(a->h_triangles), static_cast<void*>(a->h_lights),
-                  static_cast<void*>(a->h_pairs), static_cast<void*>(a->h_prims), static_cast<void*>(a->h_root),
-                  static_cast<void*>(a->h_attrs), static_cast<void*>(a->h_frame), static_cast<void*>(a->h_rgba),
-                  static_cast<void*>(a->h_counters)})
+                  static_cast<void*>(a->h_attrs), static_cast<void*>(a->h_attr_flags), static_cast<void*>(a->h_status),
+                  static_cast<void*>(a->h_frame), static_cast<void*>(a->h_rgba), static_cast<void*>(a->h_counters)})
     if (h) cudaFreeHost(h);
   delete a;
 }
@@ -989,24 +1049,13 @@ static int animation_stage(tc_animation* a, const tc_scene_data* sd, uint32_t fr
   if ((sd->sphere_count && !sd->spheres) || (sd->triangle_count && !sd->triangles) || !sd->materials)
     return fail(ctx, TC_ERR_INVALID, "frame geometry or material pointer is null");
   if (int rc = validate_geometry(ctx, sd, ctx->material_count)) return rc;
-  if (a->rebuild) {
-    // The median-split tree's shape depends on the primitive count alone (degenerate-extent
-    // leaves aside), so the rebuilt hierarchy fills the same pair and record slots every frame.
-    tcb::DeviceHierarchy dh;
-    if (int rc = build_hierarchy(ctx, sd, false, dh)) return rc;
-    if (dh.pairs.size() != ctx->pair_count || dh.prims.size() != ctx->bvh_prims)
-      return fail(ctx, TC_ERR_INVALID, "the frame's hierarchy has " + std::to_string(dh.pairs.size()) +
-                                           " interior nodes, the uploaded one " + std::to_string(ctx->pair_count) +
-                                           " (degenerate leaves): upload the scene again");
-    if (!dh.pairs.empty()) std::memcpy(a->h_pairs, dh.pairs.data(), sizeof(tcb::PairNode) * dh.pairs.size());
-    if (!dh.prims.empty()) std::memcpy(a->h_prims, dh.prims.data(), sizeof(tcb::PrimRecord) * dh.prims.size());
-    *a->h_root = dh.root;
-  } else {
-    if (sd->sphere_count) std::memcpy(a->h_spheres, sd->spheres, sizeof(tc_gpu_sphere) * sd->sphere_count);
-    if (sd->triangle_count) std::memcpy(a->h_triangles, sd->triangles, sizeof(tc_gpu_triangle) * sd->triangle_count);
-  }
-  if (a->h_attrs && sd->triangle_attributes)
+  if (sd->sphere_count) std::memcpy(a->h_spheres, sd->spheres, sizeof(tc_gpu_sphere) * sd->sphere_count);
+  if (sd->triangle_count) std::memcpy(a->h_triangles, sd->triangles, sizeof(tc_gpu_triangle) * sd->triangle_count);
+  if (a->h_attrs && sd->triangle_attributes) {
     std::memcpy(a->h_attrs, sd->triangle_attributes, sizeof(tc_gpu_triangle_attributes) * sd->triangle_count);
+    if (a->h_attr_flags)
+      for (size_t i = 0; i < sd->triangle_count; ++i) a->h_attr_flags[i] = sd->triangle_attributes[i].flags & 3u;
+  }
   if (a->update_lights && sd->light_count) {
     std::vector<tcb::DevLight> lights;
     if (int rc = pack_lights(ctx, sd, ctx->material_count, lights)) return rc;
@@ -1033,21 +1082,24 @@ static int animation_enqueue(tc_animation* a, cudaStream_t st) {
   if (a->h_attrs)
     TC_CUDA(ctx, cudaMemcpyAsync(ctx->attributes.ptr, a->h_attrs,
                                  sizeof(tc_gpu_triangle_attributes) * ctx->triangle_count, cudaMemcpyHostToDevice, st));
+  if (ctx->sphere_count)
+    TC_CUDA(ctx, cudaMemcpyAsync(ctx->raw_spheres.ptr, a->h_spheres, sizeof(tc_gpu_sphere) * ctx->sphere_count,
+                                 cudaMemcpyHostToDevice, st));
+  if (ctx->triangle_count)
+    TC_CUDA(ctx, cudaMemcpyAsync(ctx->raw_triangles.ptr, a->h_triangles, sizeof(tc_gpu_triangle) * ctx->triangle_count,
+                                 cudaMemcpyHostToDevice, st));
   if (a->rebuild) {
-    if (ctx->pair_count)
-      TC_CUDA(ctx, cudaMemcpyAsync(ctx->pairs.ptr, a->h_pairs, sizeof(tcb::PairNode) * ctx->pair_count,
+    // The frame's own median-split hierarchy, built on the device into the same buffers.
+    if (a->h_attr_flags)
+      TC_CUDA(ctx, cudaMemcpyAsync(ctx->attr_flags.ptr, a->h_attr_flags, sizeof(uint32_t) * ctx->triangle_count,
                                    cudaMemcpyHostToDevice, st));
-    if (ctx->bvh_prims)
-      TC_CUDA(ctx, cudaMemcpyAsync(ctx->prims.ptr, a->h_prims, sizeof(tcb::PrimRecord) * ctx->bvh_prims,
-                                   cudaMemcpyHostToDevice, st));
-    TC_CUDA(ctx, cudaMemcpyAsync(ctx->root_buf.ptr, a->h_root, sizeof(tcb::ChildRec), cudaMemcpyHostToDevice, st));
+    TC_CUDA(ctx, cudaMemsetAsync(ctx->build_status.ptr, 0, sizeof(uint32_t), st));
+    TC_CUDA(ctx, ctx->builder.build(ctx->raw_spheres.as<tc_gpu_sphere>(), ctx->raw_triangles.as<tc_gpu_triangle>(),
+                                    a->h_attr_flags ? ctx->attr_flags.as<uint32_t>() : nullptr,
+                                    ctx->pairs.as<tcb::PairNode>(), ctx->root_buf.as<tcb::ChildRec>(),
+                                    ctx->prims.as<tcb::PrimRecord>(), ctx->build_status.as<uint32_t>(), st));
+    TC_CUDA(ctx, cudaMemcpyAsync(a->h_status, ctx->build_status.ptr, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
   } else {
-    if (ctx->sphere_count)
-      TC_CUDA(ctx, cudaMemcpyAsync(ctx->raw_spheres.ptr, a->h_spheres, sizeof(tc_gpu_sphere) * ctx->sphere_count,
-                                   cudaMemcpyHostToDevice, st));
-    if (ctx->triangle_count)
-      TC_CUDA(ctx, cudaMemcpyAsync(ctx->raw_triangles.ptr, a->h_triangles,
-                                   sizeof(tc_gpu_triangle) * ctx->triangle_count, cudaMemcpyHostToDevice, st));
     tcb::RefitPlan plan;
     plan.nodes = ctx->refit_nodes.as<uint32_t>();
     plan.level_offsets = ctx->refit_levels;
@@ -1093,12 +1145,16 @@ int tc_animation_create(tc_context* ctx, const tc_scene_data* first_frame, const
   host(reinterpret_cast<void**>(&a->h_spheres), sizeof(tc_gpu_sphere) * ctx->sphere_count);
   host(reinterpret_cast<void**>(&a->h_triangles), sizeof(tc_gpu_triangle) * ctx->triangle_count);
   host(reinterpret_cast<void**>(&a->h_lights), sizeof(tcb::DevLight) * ctx->light_count);
-  if (a->rebuild) {
-    host(reinterpret_cast<void**>(&a->h_pairs), sizeof(tcb::PairNode) * ctx->pair_count);
-    host(reinterpret_cast<void**>(&a->h_prims), sizeof(tcb::PrimRecord) * ctx->bvh_prims);
-    host(reinterpret_cast<void**>(&a->h_root), sizeof(tcb::ChildRec));
-  }
   if (ctx->any_attr) host(reinterpret_cast<void**>(&a->h_attrs), sizeof(tc_gpu_triangle_attributes) * ctx->triangle_count);
+  if (a->rebuild) {
+    host(reinterpret_cast<void**>(&a->h_status), sizeof(uint32_t));
+    if (ctx->any_attr) host(reinterpret_cast<void**>(&a->h_attr_flags), sizeof(uint32_t) * ctx->triangle_count);
+    if (e == cudaSuccess) e = ctx->builder.plan(ctx->sphere_count, ctx->triangle_count);
+    if (e == cudaSuccess)
+      e = ctx->pairs.reserve(sizeof(tcb::PairNode) * std::max<size_t>(ctx->builder.pair_count(), 1));
+    if (e == cudaSuccess) e = ctx->build_status.reserve(sizeof(uint32_t));
+    if (e == cudaSuccess && a->h_attr_flags) e = ctx->attr_flags.reserve(sizeof(uint32_t) * ctx->triangle_count);
+  }
   host(reinterpret_cast<void**>(&a->h_frame), 20 * sizeof(float));
   host(reinterpret_cast<void**>(&a->h_rgba), 4 * a->npix);
   host(reinterpret_cast<void**>(&a->h_counters), 4 * sizeof(unsigned long long));
@@ -1154,6 +1210,10 @@ int tc_animation_frame(tc_animation* a, const tc_scene_data* frame, uint32_t fra
   ctx->width = a->params.width;
   ctx->height = a->params.height;
   ctx->accumulated = a->params.samples;
+  if (a->rebuild && *a->h_status)
+    return fail(ctx, TC_ERR_DEVICE_STATUS,
+                "the frame's centroids coincide in a node of more than four primitives (a degenerate leaf); "
+                "animate this scene with refits or upload its frames");
   cudaEventElapsedTime(&ctx->stats.total_ms, ctx->ev_begin, ctx->ev_end);
   ctx->stats.kernel_ms = ctx->stats.total_ms;
   if (int rc = finish_render_stats(ctx, a->h_counters, uint64_t(a->npix) * a->params.samples, false)) return rc;

@@ -57,6 +57,7 @@ EXPORTED_SYMBOLS = (
     "tc_animation_frame",
     "tc_animation_destroy",
     "tc_autotune",
+    "tc_set_hierarchy_build",
 )
 
 GUIDE_PARAMS = 15584
@@ -182,6 +183,7 @@ def load_library(path: os.PathLike | None = None) -> ctypes.CDLL:
     lib.tc_animation_frame.argtypes = [vp, ctypes.POINTER(SceneData), u32, vp, sz]
     lib.tc_animation_destroy.argtypes = [vp]
     lib.tc_autotune.argtypes = [vp, vp, ctypes.POINTER(RenderOptions), u32, ctypes.POINTER(TuneResult)]
+    lib.tc_set_hierarchy_build.argtypes = [vp, i32]
     for name in EXPORTED_SYMBOLS:
         if not hasattr(lib, name):
             raise RuntimeError(f"{p} does not export {name}")

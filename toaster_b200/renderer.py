@@ -200,6 +200,10 @@ class GpuRenderer:
         ch = native.SceneChanges(int(camera), int(spheres), int(triangles), int(emissive_geometry))
         self._check(self._lib.tc_update_geometry(self._ctx, ctypes.byref(sd), ctypes.byref(ch)))
 
+    def set_hierarchy_build(self, mode: str) -> None:
+        """Where uploads build the hierarchy: "auto", "host" or "device"."""
+        self._check(self._lib.tc_set_hierarchy_build(self._ctx, {"auto": 0, "host": 1, "device": 2}[mode]))
+
     def set_stream(self, stream: int) -> None:
         """Enqueue on a caller-owned cudaStream_t (0 = the context's own stream)."""
         self._check(self._lib.tc_set_stream(self._ctx, stream or None))
