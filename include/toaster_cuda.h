@@ -286,6 +286,17 @@ int tc_readback(tc_context* ctx, float* rgba, size_t n_floats);
  * host after copying 16 bytes per pixel. n_bytes >= 4*width*height. */
 int tc_readback_rgba8(tc_context* ctx, float exposure_stops, uint8_t* rgba, size_t n_bytes);
 
+/* JPEG frame of the accumulated image at `quality` 1..100: display conversion (as
+ * tc_readback_rgba8, alpha dropped) and baseline JPEG encoding (4:2:0) on the device with nvJPEG;
+ * only the compressed bytes cross to the host. Replaces encode_pixels_to_jpeg
+ * (crates/toaster-gpu/src/image_output.rs:27-56), which the MJPEG preview stream of
+ * toaster-server sends frame by frame (routes.rs:84-106). *length receives the frame's size; with
+ * out = NULL nothing is copied (a size query), and a capacity below the size fails. The
+ * encoder's bytes differ from the image crate's; both decode to the same picture within JPEG
+ * error. */
+int tc_encode_jpeg(tc_context* ctx, uint32_t quality, float exposure_stops, uint8_t* out, size_t capacity,
+                   size_t* length);
+
 /* The same conversion into caller-owned device memory (d_rgba, n_bytes >= 4*width*height),
  * enqueued on `stream` (NULL = the context's stream) without synchronising, for sinks that
  * consume frames on the device. No reference counterpart. */

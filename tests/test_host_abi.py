@@ -173,3 +173,12 @@ def test_uneven_batch_spans_sizes():
     for s in scenes:
         assert 128 <= s.triangle_count <= 262144
         assert 320 <= s.width <= 1280 and s.width % 16 == 0 and s.height == s.width * 9 // 16
+
+
+def test_mjpeg_part_framing():  # toaster-server routes.rs: formats_mjpeg_part
+    from toaster_b200.stream import mjpeg_part, split_mjpeg
+
+    part = mjpeg_part(bytes([0xFF, 0xD8, 0xFF, 0xD9]))
+    assert part == b"--frame\r\nContent-Type: image/jpeg\r\nContent-Length: 4\r\n\r\n\xff\xd8\xff\xd9\r\n"
+    frames = [bytes([0xFF, 0xD8, i, 0xFF, 0xD9]) for i in range(3)]
+    assert split_mjpeg(b"".join(mjpeg_part(f) for f in frames)) == frames

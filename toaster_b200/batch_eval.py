@@ -33,17 +33,22 @@ from .scene import scene_to_gpu
 
 def host_display_rgba8(hdr: np.ndarray, exposure_stops: float = 0.0) -> np.ndarray:
     """Host display conversion as the reference does it after readback (color.rs:24-74):
-    exposure, ACES fitted, clamp, sRGB transfer, rounding."""
+    exposure, ACES fitted, clamp, sRGB transfer, rounding half away from zero, in f32."""
     rgb = hdr[..., :3].astype(np.float32) * np.float32(2.0 ** exposure_stops)
     finite = np.isfinite(rgb)
-    c = np.maximum(np.where(finite, rgb, 0.0), 0.0)
-    with np.errstate(invalid="ignore"):
-        t = np.clip((c * (2.51 * c + 0.03)) / (c * (2.43 * c + 0.59) + 0.14), 0.0, 1.0)
-    t = np.where(finite, t, np.where(rgb == np.inf, 1.0, 0.0))  # NaN and -inf map to 0, +inf to 1
-    s = np.where(t <= 0.0031308, 12.92 * t, 1.055 * np.power(t, 1.0 / 2.4) - 0.055)
+    c = np.where(finite, rgb, np.float32(0.0))
+    np.maximum(c, np.float32(0.0), out=c)
+    t = (c * (np.float32(2.51) * c + np.float32(0.03))) / (c * (np.float32(2.43) * c + np.float32(0.59)) + np.float32(0.14))
+    np.clip(t, np.float32(0.0), np.float32(1.0), out=t)
+    if not finite.all():  # NaN and -inf map to 0, +inf to 1
+        t[~finite] = (rgb[~finite] == np.inf).astype(np.float32)
+    lin = t <= np.float32(0.0031308)
+    srgb = np.empty_like(t)
+    srgb[lin] = np.float32(12.92) * t[lin]
+    srgb[~lin] = np.float32(1.055) * np.power(t[~lin], np.float32(1.0 / 2.4)) - np.float32(0.055)
     out = np.empty(hdr.shape[:-1] + (4,), np.uint8)
-    out[..., :3] = np.round(np.clip(s, 0.0, 1.0) * 255.0)
-    out[..., 3] = np.round(np.clip(hdr[..., 3], 0.0, 1.0) * 255.0)
+    out[..., :3] = np.floor(np.clip(srgb, 0.0, 1.0) * np.float32(255.0) + np.float32(0.5))
+    out[..., 3] = np.floor(np.clip(hdr[..., 3], 0.0, 1.0) * np.float32(255.0) + np.float32(0.5))
     return out
 
 
@@ -125,7 +130,7 @@ def animation(frames: int = 240, width: int = 1280, height: int = 720, samples: 
                 "mpaths_per_s": paths * frames / (lat.sum() * 1e3)}
     # Plain unbatched path (the reference's per-frame flow).
     with GpuRenderer(device) as r:
-        lat = []
+        lat, conv = [], []
         r.upload(first)
         r.render(frame_index=0)
         for k in range(frames):
@@ -133,11 +138,16 @@ def animation(frames: int = 240, width: int = 1280, height: int = 720, samples: 
             t = time.perf_counter()
             r.upload(data)
             r.render(frame_index=k)
-            host_display_rgba8(r.readback())
-            lat.append((time.perf_counter() - t) * 1e3)
+            hdr = r.readback()
+            t1 = time.perf_counter()
+            host_display_rgba8(hdr)
+            t2 = time.perf_counter()
+            lat.append((t2 - t) * 1e3)
+            conv.append((t2 - t1) * 1e3)
         lat = np.array(lat)
         out["plain_unbatched"] = {"p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
-                                  "mean_ms": float(lat.mean()), "mpaths_per_s": paths * frames / (lat.sum() * 1e3)}
+                                  "mean_ms": float(lat.mean()), "mpaths_per_s": paths * frames / (lat.sum() * 1e3),
+                                  "host_conversion_ms": float(np.mean(conv))}
     out["host_pack_ms_per_frame"] = float(np.mean(pack_times))
     return out
 

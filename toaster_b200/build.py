@@ -63,7 +63,7 @@ def build(force: bool = False, verbose: bool = False) -> Path:
         subprocess.run(cmd, check=True)
         objs.append(str(obj))
     tmp = so.with_suffix(".so.tmp")
-    subprocess.run([nvcc()] + ARCH + ["-shared", "-o", str(tmp)] + objs, check=True)
+    subprocess.run([nvcc()] + ARCH + ["-shared", "-o", str(tmp)] + objs + ["-lnvjpeg"], check=True)
     os.replace(tmp, so)
     static = LIB / "libtoaster_cuda.a"
     if static.exists():

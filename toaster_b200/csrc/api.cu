@@ -4,6 +4,7 @@
 // the caller owns host arrays, the context owns every device buffer and one stream, and each
 // call is synchronous like dispatch_compute_2d's device.poll(Wait) (dispatch.rs:57).
 #include <cuda_runtime.h>
+#include <nvjpeg.h>
 
 #include <algorithm>
 #include <cmath>
@@ -98,6 +99,11 @@ struct tc_context {
   bool device_built = false;
   tcb::DeviceBvhBuilder builder;
   DevBuf attr_flags, build_status;
+  // JPEG frames (tc_encode_jpeg): encoder created on first use, RGB8 input on the device.
+  nvjpegHandle_t jpeg = nullptr;
+  nvjpegEncoderState_t jpeg_state = nullptr;
+  nvjpegEncoderParams_t jpeg_params = nullptr;
+  DevBuf jpeg_rgb;
 
   // Accumulation state (progressive contract of path_tracer.rs:900-923)
   uint32_t width = 0, height = 0, accumulated = 0;
@@ -414,6 +420,9 @@ int tc_destroy(tc_context* ctx) {
   if (ctx->ev_kernel0) cudaEventDestroy(ctx->ev_kernel0);
   if (ctx->ev_kernel1) cudaEventDestroy(ctx->ev_kernel1);
   if (ctx->ev_end) cudaEventDestroy(ctx->ev_end);
+  if (ctx->jpeg_params) nvjpegEncoderParamsDestroy(ctx->jpeg_params);
+  if (ctx->jpeg_state) nvjpegEncoderStateDestroy(ctx->jpeg_state);
+  if (ctx->jpeg) nvjpegDestroy(ctx->jpeg);
   if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
   delete ctx;
   return TC_OK;
@@ -1311,6 +1320,59 @@ int tc_readback_rgba8(tc_context* ctx, float exposure_stops, uint8_t* rgba, size
   if (int rc = tc_display_rgba8_async(ctx, exposure_stops, ctx->display.ptr, 4 * npix, nullptr)) return rc;
   TC_CUDA(ctx, cudaMemcpyAsync(rgba, ctx->display.ptr, 4 * npix, cudaMemcpyDeviceToHost, ctx->stream));
   TC_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return TC_OK;
+}
+
+int tc_encode_jpeg(tc_context* ctx, uint32_t quality, float exposure_stops, uint8_t* out, size_t capacity,
+                   size_t* length) {
+  if (!ctx) return fail(nullptr, TC_ERR_INVALID, "context is null");
+  if (!length) return fail(ctx, TC_ERR_INVALID, "length pointer is null");
+  if (quality < 1 || quality > 100) return fail(ctx, TC_ERR_INVALID, "JPEG quality must be between 1 and 100");
+  if (ctx->accumulated == 0) return fail(ctx, TC_ERR_STATE, "tc_encode_jpeg before tc_render");
+  if (!std::isfinite(exposure_stops)) return fail(ctx, TC_ERR_INVALID, "exposure must be finite");
+  TC_CUDA(ctx, cudaSetDevice(ctx->device));
+  cudaStream_t st = ctx->stream;
+  auto jpeg_fail = [&](nvjpegStatus_t status, const char* what) {
+    return fail(ctx, TC_ERR_CUDA, std::string(what) + " failed with nvJPEG status " + std::to_string(int(status)));
+  };
+  nvjpegStatus_t js;
+  if (!ctx->jpeg) {
+    if ((js = nvjpegCreateSimple(&ctx->jpeg)) != NVJPEG_STATUS_SUCCESS) {
+      ctx->jpeg = nullptr;
+      return jpeg_fail(js, "nvjpegCreateSimple");
+    }
+    if ((js = nvjpegEncoderStateCreate(ctx->jpeg, &ctx->jpeg_state, st)) != NVJPEG_STATUS_SUCCESS)
+      return jpeg_fail(js, "nvjpegEncoderStateCreate");
+    if ((js = nvjpegEncoderParamsCreate(ctx->jpeg, &ctx->jpeg_params, st)) != NVJPEG_STATUS_SUCCESS)
+      return jpeg_fail(js, "nvjpegEncoderParamsCreate");
+  }
+  if ((js = nvjpegEncoderParamsSetQuality(ctx->jpeg_params, int(quality), st)) != NVJPEG_STATUS_SUCCESS)
+    return jpeg_fail(js, "nvjpegEncoderParamsSetQuality");
+  if ((js = nvjpegEncoderParamsSetSamplingFactors(ctx->jpeg_params, NVJPEG_CSS_420, st)) != NVJPEG_STATUS_SUCCESS)
+    return jpeg_fail(js, "nvjpegEncoderParamsSetSamplingFactors");
+  const size_t npix = size_t(ctx->width) * ctx->height;
+  TC_CUDA(ctx, ctx->jpeg_rgb.reserve(3 * npix));
+  TC_CUDA(ctx, tcb::launch_display_rgb8_from_sums(ctx->accum.as<double>(), uint32_t(npix), 1.0 / double(ctx->accumulated),
+                                                  exposure_stops, ctx->jpeg_rgb.as<uint8_t>(), st));
+  nvjpegImage_t img{};
+  img.channel[0] = ctx->jpeg_rgb.as<unsigned char>();
+  img.pitch[0] = 3 * size_t(ctx->width);
+  if ((js = nvjpegEncodeImage(ctx->jpeg, ctx->jpeg_state, ctx->jpeg_params, &img, NVJPEG_INPUT_RGBI, int(ctx->width),
+                              int(ctx->height), st)) != NVJPEG_STATUS_SUCCESS)
+    return jpeg_fail(js, "nvjpegEncodeImage");
+  TC_CUDA(ctx, cudaStreamSynchronize(st));
+  size_t len = 0;
+  if ((js = nvjpegEncodeRetrieveBitstream(ctx->jpeg, ctx->jpeg_state, nullptr, &len, st)) != NVJPEG_STATUS_SUCCESS)
+    return jpeg_fail(js, "nvjpegEncodeRetrieveBitstream");
+  *length = len;
+  if (!out) return TC_OK;
+  if (capacity < len)
+    return fail(ctx, TC_ERR_INVALID, "output buffer holds " + std::to_string(capacity) + " bytes; the frame needs " +
+                                         std::to_string(len));
+  if ((js = nvjpegEncodeRetrieveBitstream(ctx->jpeg, ctx->jpeg_state, out, &len, st)) != NVJPEG_STATUS_SUCCESS)
+    return jpeg_fail(js, "nvjpegEncodeRetrieveBitstream");
+  TC_CUDA(ctx, cudaStreamSynchronize(st));
+  *length = len;
   return TC_OK;
 }
 

@@ -63,6 +63,27 @@ __global__ void display_rgba_kernel(const float4* __restrict__ px, uint32_t pixe
   out[i] = display_pixel(p.x, p.y, p.z, p.w, scale);
 }
 
+// From FP64 per-pixel sums to interleaved RGB8 (the input of the JPEG encoder; JPEG drops alpha).
+__global__ void display_rgb8_sums_kernel(const double* __restrict__ sums, uint32_t pixels, double inv_samples,
+                                         float scale, uint8_t* __restrict__ out) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= pixels) return;
+  const double* s = sums + size_t(3) * i;
+  const uint32_t p =
+      display_pixel(float(s[0] * inv_samples), float(s[1] * inv_samples), float(s[2] * inv_samples), 1.0f, scale);
+  out[3 * size_t(i)] = uint8_t(p);
+  out[3 * size_t(i) + 1] = uint8_t(p >> 8);
+  out[3 * size_t(i) + 2] = uint8_t(p >> 16);
+}
+
+cudaError_t launch_display_rgb8_from_sums(const double* sums, uint32_t pixels, double inv_samples,
+                                          float exposure_stops, uint8_t* out, cudaStream_t stream) {
+  if (pixels == 0) return cudaSuccess;
+  display_rgb8_sums_kernel<<<(pixels + 255) / 256, 256, 0, stream>>>(sums, pixels, inv_samples,
+                                                                     std::exp2(exposure_stops), out);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_display_from_sums(const double* sums, uint32_t pixels, double inv_samples, float exposure_stops,
                                      uint32_t* out, cudaStream_t stream) {
   if (pixels == 0) return cudaSuccess;

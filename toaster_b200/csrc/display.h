@@ -10,6 +10,8 @@ namespace tcb {
 
 cudaError_t launch_display_from_sums(const double* sums, uint32_t pixels, double inv_samples, float exposure_stops,
                                      uint32_t* out, cudaStream_t stream);
+cudaError_t launch_display_rgb8_from_sums(const double* sums, uint32_t pixels, double inv_samples,
+                                          float exposure_stops, uint8_t* out, cudaStream_t stream);
 cudaError_t launch_display_from_rgba(const float4* px, uint32_t pixels, float exposure_stops, uint32_t* out,
                                      cudaStream_t stream);
 

@@ -58,6 +58,7 @@ EXPORTED_SYMBOLS = (
     "tc_animation_destroy",
     "tc_autotune",
     "tc_set_hierarchy_build",
+    "tc_encode_jpeg",
 )
 
 GUIDE_PARAMS = 15584
@@ -184,6 +185,7 @@ def load_library(path: os.PathLike | None = None) -> ctypes.CDLL:
     lib.tc_animation_destroy.argtypes = [vp]
     lib.tc_autotune.argtypes = [vp, vp, ctypes.POINTER(RenderOptions), u32, ctypes.POINTER(TuneResult)]
     lib.tc_set_hierarchy_build.argtypes = [vp, i32]
+    lib.tc_encode_jpeg.argtypes = [vp, u32, f32, vp, sz, ctypes.POINTER(sz)]
     for name in EXPORTED_SYMBOLS:
         if not hasattr(lib, name):
             raise RuntimeError(f"{p} does not export {name}")

@@ -280,6 +280,15 @@ class GpuRenderer:
         self._check(self._lib.tc_readback_rgba8(self._ctx, float(exposure_stops), out.ctypes.data, out.nbytes))
         return out
 
+    def encode_jpeg(self, quality: int = 90, exposure_stops: float = 0.0) -> bytes:
+        """JPEG bytes of the accumulated image, display-converted and encoded on the device."""
+        n = ctypes.c_size_t()
+        cap = 4 * self.width * self.height + 65536  # above any baseline 4:2:0 frame of this size
+        buf = (ctypes.c_uint8 * cap)()
+        self._check(self._lib.tc_encode_jpeg(self._ctx, int(quality), float(exposure_stops), buf, cap,
+                                             ctypes.byref(n)))
+        return bytes(buf[: n.value])
+
     def display_rgba8_device(self, exposure_stops: float, d_out: int, nbytes: int, stream: int = 0) -> None:
         """Display conversion into caller-owned device memory, enqueued without synchronising."""
         self._check(self._lib.tc_display_rgba8_async(self._ctx, float(exposure_stops), d_out, nbytes, stream or None))
