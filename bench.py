@@ -214,6 +214,7 @@ def run_ours(args):
 
     from toaster_b200 import build, configs
     from toaster_b200.renderer import GpuRenderer
+    from toaster_b200.replicas import job_throughput, max_over_ranks
     from toaster_b200.scene import SceneGpuData, scene_to_gpu
 
     world, rank, local = dist_env()
@@ -264,12 +265,8 @@ def run_ours(args):
     torch.cuda.synchronize()
     clk = clocks.stop()
     barrier()
-    total_ms = sum(step_ms)
-    if world > 1:
-        t = torch.tensor([total_ms], dtype=torch.float64, device=f"cuda:{local}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
-    value = world * paths_per_step * args.steps / (total_ms * 1e-3) / 1e6
+    total_ms = max_over_ranks(sum(step_ms), device=f"cuda:{local}")
+    value = job_throughput(paths_per_step, args.steps, world, total_ms * 1e-3)
 
     # ---------------- end-to-end through the C ABI with pinned host buffers
     keep = []
@@ -291,11 +288,8 @@ def run_ours(args):
         r2.readback(out)
     e2e_s = time.perf_counter() - t0
     barrier()
-    if world > 1:
-        t = torch.tensor([e2e_s], dtype=torch.float64, device=f"cuda:{local}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
-    e2e_value = world * paths_per_step * args.steps / e2e_s / 1e6
+    e2e_s = max_over_ranks(e2e_s, device=f"cuda:{local}")
+    e2e_value = job_throughput(paths_per_step, args.steps, world, e2e_s)
     assert np.all(np.isfinite(out)), "non-finite pixels in the benchmark image"
     r2.close()
 

@@ -140,7 +140,8 @@ typedef struct tc_render_options {
   uint32_t keep_moments;     /* 1: also accumulate per-pixel sums of squared samples (FP64) */
   uint32_t guiding;          /* 1: learned path guiding at diffuse vertices (needs tc_guide_set_params) */
   uint32_t guide_record;     /* 1: record (position, normal, direction, incident radiance) training
-                                samples at every diffuse scatter of this batch (plain sampling) */
+                                samples at every diffuse scatter of this batch and at every
+                                environment shadow ray that reaches the sky (plain sampling) */
   uint32_t wave_paths;       /* guided wavefront width: paths in flight per wave; 0 = 2^23 */
   uint32_t short_stack;      /* traversal stack entries per thread held in shared memory (0..16;
                                 deeper entries live in local memory); 0 = none */
@@ -365,9 +366,10 @@ int tc_guide_train(tc_context* ctx, const float* samples, size_t n, uint32_t ste
 
 /* Builds training samples from the diffuse scatters recorded by the last tc_render with
  * guide_record = 1 (weight = luminance of the radiance that arrived along each scattered
- * direction, normalised by its mean and clamped at 50x the mean; directions that carried no
- * radiance are dropped, as they add nothing to the weighted likelihood) and runs `steps` Adam
- * steps on batches of `batch` samples drawn at random. losses (optional) receives one value per
+ * direction, or, for an environment shadow ray that reached the sky, its radiance times the BSDF
+ * side's MIS share over the light pdf; normalised by the mean and clamped at 50x the mean;
+ * directions that carried no radiance are dropped, as they add nothing to the weighted
+ * likelihood) and runs `steps` Adam steps on batches of `batch` samples drawn at random. losses (optional) receives one value per
  * step and n_samples (optional) the number of samples. */
 int tc_guide_train_recorded(tc_context* ctx, uint32_t steps, uint32_t batch, float lr, uint64_t seed, float* losses,
                             uint32_t* n_samples);

@@ -753,10 +753,11 @@ static int enqueue_render(tc_context* ctx, const tc_gpu_render_params* p, const 
   if (per_sm <= 0) return fail(ctx, TC_ERR_CUDA, "render kernel cannot be resident with this block size");
   const int grid = per_sm * ctx->sm_count;
   if (mode == tcb::kModeRecord) {
-    // One record per diffuse scatter (capped) and the final radiance of every path of the batch.
+    // One record per diffuse scatter and per unoccluded environment shadow ray (capped), and the
+    // final radiance of every path of the batch.
     const uint64_t paths = uint64_t(npix) * p->samples;
     if (paths > (1ull << 31)) return fail(ctx, TC_ERR_INVALID, "too many paths to record in one batch");
-    ctx->rec_capacity = uint32_t(std::min<uint64_t>(2 * paths, uint64_t(1) << 25));
+    ctx->rec_capacity = uint32_t(std::min<uint64_t>(3 * paths, uint64_t(1) << 25));
     TC_CUDA(ctx, ctx->rec_records.reserve(sizeof(float4) * 4 * size_t(ctx->rec_capacity)));
     TC_CUDA(ctx, ctx->rec_count.reserve(sizeof(uint32_t)));
     TC_CUDA(ctx, ctx->rec_path_rad.reserve(sizeof(float4) * size_t(paths)));

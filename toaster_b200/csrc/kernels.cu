@@ -55,6 +55,7 @@ __device__ __forceinline__ uint64_t splitmix64(uint64_t x) {
   x = (x ^ (x >> 27)) * 0x94D049BB133111EBull;
   return x ^ (x >> 31);
 }
+__device__ __forceinline__ float luminance(V3 c) { return 0.2126f * c.x + 0.7152f * c.y + 0.0722f * c.z; }
 struct Pcg {
   uint64_t state, inc;
   __device__ __forceinline__ void seed(uint32_t frame, uint32_t pixel, uint32_t sample) {
@@ -243,6 +244,9 @@ cudaError_t launch_trace_closest(const DevScene& s, const float* rays, uint64_t 
 // ------------------------------------------------------------------------ path kernel
 enum Phase : int { kIdle = 0, kExtend = 1, kShadowLight = 2, kShadowEnv = 3, kScatter = 4 };
 
+// Path-id word of a training record written for an unoccluded environment shadow ray.
+constexpr uint32_t kNeeRecord = 0xFFFFFFFFu;
+
 struct Lane {
   V3 ro, rd;         // next ray
   V3 thr;            // path throughput
@@ -258,6 +262,7 @@ struct Lane {
   bool include_emission;
   uint32_t pixel, item_samples, item_done, sample;
   int mix_slot;      // guided mode: decoded mixture of the current diffuse vertex, or -1
+  float nee_w;       // record mode: training weight of the pending environment shadow ray
   uint32_t job;      // batched launch: frame of the current work item
   Pcg rng;
 };
@@ -438,6 +443,12 @@ __device__ __forceinline__ bool prepare_env_shadow(const RenderLaunch& L, const 
   }
   const float mis = power_heuristic(pdf, indirect_pdf);
   ln.pend = ln.thr * ln.alb * rad * (cs * mis / (kPiF * pdf));
+  if constexpr (kMode == kModeRecord) {
+    // As a training sample this direction stands for the share of the incident radiance that
+    // the BSDF side carries (1 - mis), the share a guided direction has to find: NEE samples the
+    // visible sky far more often than cosine sampling does, and the sun's share stays near 0.
+    ln.nee_w = luminance(rad) * (cs * (1.0f - mis) / (kPiF * pdf));
+  }
   ln.ro = ln.hp + ln.hn * kRayEps;
   ln.rd = dir;
   ln.tmax = CUDART_INF_F;
@@ -812,7 +823,21 @@ __global__ void __launch_bounds__(256) render_kernel(const RenderLaunch L) {
         ln.phase = kShadowEnv;
       } else if (ln.phase == kShadowEnv) {
         ++n_shadow;
-        if (!hit) ln.rad = ln.rad + ln.pend;
+        if (!hit) {
+          ln.rad = ln.rad + ln.pend;
+          if constexpr (kMode == kModeRecord) {
+            if (ln.nee_w > 0.0f) {
+              const uint32_t slot = aggregated_increment(L.g.record_count);
+              if (slot < L.g.record_capacity) {
+                float4* r = L.g.records + 4 * size_t(slot);
+                r[0] = make_float4(ln.hp.x, ln.hp.y, ln.hp.z, __uint_as_float(kNeeRecord));
+                r[1] = make_float4(ln.hn.x, ln.hn.y, ln.hn.z, 0.0f);
+                r[2] = make_float4(ln.rd.x, ln.rd.y, ln.rd.z, 0.0f);
+                r[3] = make_float4(ln.nee_w, 0.0f, 0.0f, 0.0f);
+              }
+            }
+          }
+        }
         ln.phase = kScatter;
       } else {
         ++n_ext;
@@ -917,13 +942,17 @@ __global__ void guide_samples_kernel(const float4* __restrict__ rec, const uint3
     b = rec[4 * size_t(i) + 1];
     c = rec[4 * size_t(i) + 2];
     const float4 d = rec[4 * size_t(i) + 3];
-    const float4 end = path_rad[__float_as_uint(a.w)];
-    // Radiance that arrived along the scattered direction: what the path gathered after this
-    // vertex, divided by the throughput it had just after scattering.
-    const float lx = b.w > 0.0f ? fmaxf(end.x - d.x, 0.0f) / b.w : 0.0f;
-    const float ly = c.w > 0.0f ? fmaxf(end.y - d.y, 0.0f) / c.w : 0.0f;
-    const float lz = d.w > 0.0f ? fmaxf(end.z - d.z, 0.0f) / d.w : 0.0f;
-    w = 0.2126f * lx + 0.7152f * ly + 0.0722f * lz;
+    if (__float_as_uint(a.w) == kNeeRecord) {
+      w = d.x;  // environment shadow ray that reached the sky: its weight was computed at record time
+    } else {
+      const float4 end = path_rad[__float_as_uint(a.w)];
+      // Radiance that arrived along the scattered direction: what the path gathered after this
+      // vertex, divided by the throughput it had just after scattering.
+      const float lx = b.w > 0.0f ? fmaxf(end.x - d.x, 0.0f) / b.w : 0.0f;
+      const float ly = c.w > 0.0f ? fmaxf(end.y - d.y, 0.0f) / c.w : 0.0f;
+      const float lz = d.w > 0.0f ? fmaxf(end.z - d.z, 0.0f) / d.w : 0.0f;
+      w = 0.2126f * lx + 0.7152f * ly + 0.0722f * lz;
+    }
     if (!(w > 0.0f) || !isfinite(w)) w = 0.0f;
   }
   const bool keep = w > 0.0f;
