@@ -401,6 +401,23 @@ long tc_build_bvh_host(const tc_gpu_sphere* spheres, size_t n_spheres, const tc_
 /* Byte sizes of the record types as compiled into the library (layout check). */
 int tc_record_sizes(uint32_t* out, size_t n);
 
+/* Scene files (host only) ------------------------------------------------------------------
+ * Replaces toaster_gpu::scene_upload::load_scene_gpu (crates/toaster-gpu/src/scene_upload.rs:54-57:
+ * toaster_scene::load_scene, crates/toaster-scene/src/loader.rs:534-971, then scene_to_gpu,
+ * scene_upload.rs:79-294) for a caller without the Rust loader: reads a scene JSON file with its glTF / GLB meshes
+ * (crates/toaster-assets/src/gltf_loader.rs:11-233; 8-bit PNG base-colour textures) and its
+ * Radiance .hdr or PNG environment map, validates it with the reference loader's rules and packs
+ * the records. The hierarchy is not packed (bvh_nodes NULL): tc_upload_scene builds it.
+ * Animation, physics, triggers, spawn points and event reactions are skipped. On failure returns
+ * TC_ERR_INVALID with the message in error (NUL-terminated, truncated to error_capacity). */
+typedef struct tc_loaded_scene tc_loaded_scene;
+int tc_scene_load(const char* path, tc_loaded_scene** out, char* error, size_t error_capacity);
+/* The packed records; valid until tc_loaded_scene_free. */
+const tc_scene_data* tc_loaded_scene_data(const tc_loaded_scene* scene);
+/* The scene's display exposure in stops (its "display" block, 0 when absent). */
+int tc_loaded_scene_display(const tc_loaded_scene* scene, float* exposure_stops);
+int tc_loaded_scene_free(tc_loaded_scene* scene);
+
 #ifdef __cplusplus
 }
 #endif

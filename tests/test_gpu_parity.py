@@ -131,7 +131,7 @@ def _blocks(x, b):
     return x[:h2, :w2].reshape(h2 // b, b, w2 // b, b).sum(axis=(1, 3))
 
 
-def statistical_parity(renderer, scene, gpu_spp=4096, cpu_spp=256, block=2):
+def statistical_parity(renderer, scene, gpu_spp=4096, cpu_spp=256, block=2, upload=None):
     """GPU image vs the oracle's at the same scene.
 
     Path-tracing samples are heavy-tailed (small lights, a 1e4 sun), so z-scores use the
@@ -139,9 +139,13 @@ def statistical_parity(renderer, scene, gpu_spp=4096, cpu_spp=256, block=2):
     blocks. Thresholds were calibrated by running the oracle against itself with independent
     seeds at the same sample counts (worst seen: 3.5% of blocks beyond 3 sigma, |median z| 0.21,
     |global dz/se| 3.3): at most 6% of blocks outside 3 sigma, |median z| <= 0.35, global mean
-    within 6 standard errors and 3% relative.
+    within 6 standard errors and 3% relative. ``upload`` replaces the default upload of
+    ``scene_to_gpu(scene)`` (the oracle always renders ``scene``).
     """
-    renderer.upload(scene_to_gpu(scene))
+    if upload is None:
+        renderer.upload(scene_to_gpu(scene))
+    else:
+        upload()
     renderer.render(samples=gpu_spp, keep_moments=True, frame_index=17)
     s, q, n = renderer.readback_sums(moments=True)
     assert n == gpu_spp

@@ -17,7 +17,7 @@ ROOT = Path(__file__).resolve().parents[1]
 
 def declared_functions():
     text = (ROOT / "include" / "toaster_cuda.h").read_text()
-    return sorted(set(re.findall(r"^\s*(?:int|long|const char\*)\s+(tc_\w+)\s*\(", text, re.M)))
+    return sorted(set(re.findall(r"^\s*(?:int|long|const \w+\s*\*)\s+(tc_\w+)\s*\(", text, re.M)))
 
 
 def test_library_exports_every_declared_function(native_lib):

@@ -32,7 +32,7 @@ def _rank(rank, world, port, out):
 
 def test_two_gloo_ranks_agree_on_the_slowest_time():
     world = 2
-    manager = mp.Manager()
+    manager = mp.get_context("spawn").Manager()
     out = manager.dict()
     mp.spawn(_rank, args=(world, _free_port(), out), nprocs=world, join=True)
     assert out[0] == out[1]

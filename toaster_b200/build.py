@@ -20,7 +20,7 @@ PKG = Path(__file__).resolve().parent
 CSRC = PKG / "csrc"
 LIB = PKG / "lib"
 SOURCES = ["api.cu", "kernels.cu", "guide.cu", "umma_selftest.cu", "display.cu", "refit.cu", "bvh_device.cu",
-           "bvh_build.cpp"]
+           "bvh_build.cpp", "scene_loader.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
@@ -63,7 +63,7 @@ def build(force: bool = False, verbose: bool = False) -> Path:
         subprocess.run(cmd, check=True)
         objs.append(str(obj))
     tmp = so.with_suffix(".so.tmp")
-    subprocess.run([nvcc()] + ARCH + ["-shared", "-o", str(tmp)] + objs + ["-lnvjpeg"], check=True)
+    subprocess.run([nvcc()] + ARCH + ["-shared", "-o", str(tmp)] + objs + ["-lnvjpeg", "-lz"], check=True)
     os.replace(tmp, so)
     static = LIB / "libtoaster_cuda.a"
     if static.exists():

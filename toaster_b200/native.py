@@ -59,6 +59,10 @@ EXPORTED_SYMBOLS = (
     "tc_autotune",
     "tc_set_hierarchy_build",
     "tc_encode_jpeg",
+    "tc_scene_load",
+    "tc_loaded_scene_data",
+    "tc_loaded_scene_display",
+    "tc_loaded_scene_free",
 )
 
 GUIDE_PARAMS = 15584
@@ -186,6 +190,11 @@ def load_library(path: os.PathLike | None = None) -> ctypes.CDLL:
     lib.tc_autotune.argtypes = [vp, vp, ctypes.POINTER(RenderOptions), u32, ctypes.POINTER(TuneResult)]
     lib.tc_set_hierarchy_build.argtypes = [vp, i32]
     lib.tc_encode_jpeg.argtypes = [vp, u32, f32, vp, sz, ctypes.POINTER(sz)]
+    lib.tc_scene_load.argtypes = [ctypes.c_char_p, ctypes.POINTER(vp), ctypes.c_char_p, sz]
+    lib.tc_loaded_scene_data.argtypes = [vp]
+    lib.tc_loaded_scene_data.restype = ctypes.POINTER(SceneData)
+    lib.tc_loaded_scene_display.argtypes = [vp, ctypes.POINTER(f32)]
+    lib.tc_loaded_scene_free.argtypes = [vp]
     for name in EXPORTED_SYMBOLS:
         if not hasattr(lib, name):
             raise RuntimeError(f"{p} does not export {name}")
@@ -229,6 +238,43 @@ def umma_selftest(a: np.ndarray, b: np.ndarray, a_mn_major: bool = False, b_mn_m
     check(lib, None, lib.tc_umma_selftest(a.ctypes.data, b.ctypes.data, d.ctypes.data, n, k, int(a_mn_major),
                                           int(b_mn_major)))
     return d
+
+
+class LoadedScene:
+    """A scene file loaded and packed by the library (tc_scene_load); frees itself on close."""
+
+    def __init__(self, path: os.PathLike):
+        self._handle = None
+        self._lib = load_library()
+        handle = ctypes.c_void_p()
+        err = ctypes.create_string_buffer(4096)
+        code = self._lib.tc_scene_load(os.fsencode(path), ctypes.byref(handle), err, len(err))
+        if code != TC_OK:
+            raise TcError(code, err.value.decode(errors="replace"))
+        self._handle = handle
+
+    def data(self):
+        """The packed records (a SceneData view valid until close())."""
+        return self._lib.tc_loaded_scene_data(self._handle).contents
+
+    def exposure_stops(self) -> float:
+        out = ctypes.c_float()
+        check(self._lib, None, self._lib.tc_loaded_scene_display(self._handle, ctypes.byref(out)))
+        return float(out.value)
+
+    def close(self) -> None:
+        if getattr(self, "_handle", None):
+            self._lib.tc_loaded_scene_free(self._handle)
+            self._handle = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        self.close()
 
 
 def record_sizes() -> list:

@@ -193,6 +193,16 @@ class GpuRenderer:
         self._params = data.params.copy()
         self.accumulated = 0
 
+    def upload_file(self, path) -> float:
+        """Loads a scene file with the native loader (tc_scene_load) and uploads its records
+        straight from the library's buffers; returns the scene's display exposure in stops."""
+        with native.LoadedScene(path) as loaded:
+            sd = loaded.data()
+            self._check(self._lib.tc_upload_scene(self._ctx, ctypes.byref(sd)))
+            self._params = np.frombuffer(bytes(sd.params), gt.RENDER_PARAMS, 1).copy()
+            self.accumulated = 0
+            return loaded.exposure_stops()
+
     def update_geometry(self, data: SceneGpuData, camera: bool = False, spheres: bool = True, triangles: bool = True,
                         emissive_geometry: bool = False) -> None:
         """Per-frame update: copies changed geometry and refits the hierarchy on the device."""

@@ -45,3 +45,24 @@ def write_mjpeg(frames: Iterable[bytes], sink: BinaryIO) -> int:
         sink.write(mjpeg_part(jpeg))
         n += 1
     return n
+
+
+def encode_png(rgba) -> bytes:
+    """An (height, width, 4) uint8 image as a PNG file (8-bit RGBA, filter type 0), the format
+    the reference's ``save_png`` writes (crates/toaster-gpu/src/image_output.rs:59)."""
+    import struct
+    import zlib
+
+    import numpy as np
+
+    img = np.ascontiguousarray(rgba, np.uint8)
+    h, w, c = img.shape
+    if c != 4:
+        raise ValueError("expected an RGBA image")
+    rows = np.concatenate([np.zeros((h, 1), np.uint8), img.reshape(h, w * 4)], axis=1)
+
+    def chunk(kind: bytes, body: bytes) -> bytes:
+        return struct.pack(">I", len(body)) + kind + body + struct.pack(">I", zlib.crc32(kind + body) & 0xFFFFFFFF)
+
+    return (b"\x89PNG\r\n\x1a\n" + chunk(b"IHDR", struct.pack(">IIBBBBB", w, h, 8, 6, 0, 0, 0)) +
+            chunk(b"IDAT", zlib.compress(rows.tobytes(), 6)) + chunk(b"IEND", b""))
