@@ -38,6 +38,12 @@ WORKLOAD = ("mixed scene: 2,048 seeded triangles + 128 spheres (50/30/20 diffuse
             "triangles), 1024x512 FP32 sky + 0.5-degree sun (1e4), 1280x720, 64 spp, 8 bounces")
 
 
+
+def ordinal(n: int) -> str:
+    """1st, 2nd, 3rd, 4th, ..., 11th-13th, 21st."""
+    suffix = "th" if 10 <= n % 100 <= 20 else {1: "st", 2: "nd", 3: "rd"}.get(n % 10, "th")
+    return f"{n}{suffix}"
+
 def parse_args():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -50,6 +56,9 @@ def parse_args():
     ap.add_argument("--no-equal-time", action="store_true", help="skip the guided-vs-plain equal-time comparison")
     ap.add_argument("--equal-time-ref-spp", type=int, default=4096,
                     help="samples per pixel of the plain FP64 reference the equal-time RMSE is measured against")
+    ap.add_argument("--cpu-table", action="store_true",
+                    help="only time the CPU baseline (the oracle) at 1 thread and all threads on the plain-small, "
+                         "mixed, large-mesh and window-room workloads, one JSON line each")
     ap.add_argument("--batch-eval", action="store_true",
                     help="also run the batched-scenes and animated-frames evaluation (a few minutes)")
     return ap.parse_args()
@@ -186,7 +195,7 @@ def run_reference(args):
         "config": {"workload": WORKLOAD, "width": 1280, "height": 720, "spp": 64, "max_bounces": 8},
         "cpu_baseline": {
             "value": value, "unit": UNIT, "cores": samples[0]["cores"], "kind": "port",
-            "sample": f"every {samples[0]['row_step']}th row ({samples[0]['rows']} rows x 1280 px x 64 spp) per step; "
+            "sample": f"every {ordinal(samples[0]['row_step'])} row ({samples[0]['rows']} rows x 1280 px x 64 spp) per step; "
                       "oracle = C++ restatement of crates/toaster-cpu (reference is Rust, unbuildable here)"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -342,7 +351,7 @@ def run_ours(args):
         if cpu is not None:
             line["cpu_baseline"] = {
                 "value": cpu["mpaths_s"], "unit": UNIT, "cores": cpu["cores"], "kind": "port",
-                "sample": f"oracle (C++ restatement of crates/toaster-cpu) on every {cpu['row_step']}th row "
+                "sample": f"oracle (C++ restatement of crates/toaster-cpu) on every {ordinal(cpu['row_step'])} row "
                           f"({cpu['rows']} rows x {w} px x {spp} spp, {cpu['seconds']:.1f} s)"}
         print(json.dumps(line), flush=True)
     r.set_stream(0)
@@ -386,8 +395,29 @@ def read_traffic(rays_per_launch):
         return None
 
 
+def cpu_table(args) -> int:
+    """The CPU baseline beside every GPU workload: the oracle at 1 thread and at all host threads,
+    on the whole plain-small frame and on strided row samples of the others."""
+    from toaster_b200 import configs
+
+    workloads = [("plain_small", configs.plain_small), ("mixed", configs.mixed),
+                 ("large_mesh", configs.large_mesh), ("room", configs.room_with_window)]
+    for name, make in workloads:
+        scene = make()
+        for threads in (1, 0):
+            t = cpu_sample(scene, args.cpu_seconds, threads=threads)
+            rays = t["counts"][0]
+            print(json.dumps({"workload": name, "width": scene.width, "height": scene.height, "spp": scene.samples,
+                              "max_bounces": scene.max_bounces, "threads": t["cores"], "mpaths_per_s": t["mpaths_s"],
+                              "mrays_per_s": rays / t["seconds"] / 1e6, "rows": t["rows"],
+                              "row_step": t["row_step"], "seconds": t["seconds"]}), flush=True)
+    return 0
+
+
 def main():
     args = parse_args()
+    if args.cpu_table:
+        return cpu_table(args)
     if args.impl == "reference":
         return run_reference(args)
     return run_ours(args)
