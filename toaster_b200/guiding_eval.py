@@ -18,6 +18,7 @@ from __future__ import annotations
 import argparse
 import json
 import time
+from pathlib import Path
 
 import numpy as np
 
@@ -162,6 +163,44 @@ def equal_time_comparison(scene: Scene, ref_spp: int, plain_spp: int = 256, batc
     }
 
 
+def kernel_timings(width: int = 1280, height: int = 720, record_spp: int = 16, train_steps: int = 600,
+                   train_batch: int = 8192, queries: int = 1 << 20, guided_spp: int = 16, device: int = 0) -> dict:
+    """Throughput of the network kernels on the guiding workload: training (fused forward +
+    backward + Adam per step) on the recorded samples, inference on `queries` recorded
+    (position, normal) pairs, and one guided batch. FLOP counts: 30,080 per inference query,
+    90,240 per training sample (forward + two backward contractions); rates against the
+    measured burst bf16 tensor peak."""
+    peaks = json.loads((Path(__file__).resolve().parents[1] / "MEASURED_PEAKS.json").read_text()) \
+        if (Path(__file__).resolve().parents[1] / "MEASURED_PEAKS.json").exists() else {}
+    peak = float(peaks.get("bf16_tflops", 1590.0))
+    scene = configs.room_with_window(width=width, height=height)
+    with GpuRenderer(device) as r:
+        r.upload(scene_to_gpu(scene))
+        r.guide_set_params(initial_params(0), configs.scene_bounds(scene))
+        r.render(samples=record_spp, frame_index=0, guide_record=True)
+        _, n = r.guide_train_recorded(train_steps, train_batch, 1e-2, 0)
+        train_ms = r.stats()["kernel_ms"]
+        rec = r.guide_recorded_samples()
+        idx = np.resize(np.arange(len(rec)), queries)
+        pts, nrm = rec[idx, :3], rec[idx, 4:7]
+        infer_ms = []
+        for _ in range(5):
+            r.guide_infer(pts, nrm)
+            infer_ms.append(r.stats()["kernel_ms"])
+        r.render(samples=guided_spp, frame_index=record_spp, accumulate=True, guiding=True)
+        guided = r.stats()
+    train_tflops = train_steps * train_batch * 90240 / (train_ms * 1e-3) / 1e12
+    infer = float(np.median(infer_ms))
+    infer_tflops = queries * 30080 / (infer * 1e-3) / 1e12
+    return {"width": width, "height": height, "training_samples": n, "train_steps": train_steps,
+            "train_batch": train_batch, "train_ms": train_ms, "train_us_per_step": train_ms * 1e3 / train_steps,
+            "train_tflops": train_tflops, "train_frac_of_measured_peak": train_tflops / peak,
+            "infer_queries": queries, "infer_ms": infer, "infer_mqueries_per_s": queries / infer / 1e3,
+            "infer_tflops": infer_tflops, "infer_frac_of_measured_peak": infer_tflops / peak,
+            "guided_spp": guided_spp, "guided_kernel_ms": guided["kernel_ms"], "guided_total_ms": guided["total_ms"],
+            "peak_bf16_tflops": peak}
+
+
 def main():
     """Defaults are the learned-guiding workload: the window room (8,192 clutter triangles, 30%
     metal) at 1280x720, 8 bounces, a 65,536-spp reference, 256 plain spp, 16 recorded spp."""
@@ -177,7 +216,12 @@ def main():
     ap.add_argument("--metal", type=float, default=0.3)
     ap.add_argument("--seeds", type=int, default=1)
     ap.add_argument("--timelines", action="store_true")
+    ap.add_argument("--kernels", action="store_true",
+                    help="only time the network kernels (training, inference, one guided batch)")
     args = ap.parse_args()
+    if args.kernels:
+        print(json.dumps(kernel_timings(args.width, args.height, args.record_spp, args.train_steps)), flush=True)
+        return
     scene = configs.room_with_window(width=args.width, height=args.height, clutter=args.clutter,
                                      metal_fraction=args.metal)
     t0 = time.perf_counter()
