@@ -150,6 +150,9 @@ typedef struct tc_render_options {
                                 when all have finished); 0 = default. refill_lanes > 1 or
                                 short_stack > 0 select the resumable traversal, for plain renders
                                 without moments; other launches ignore both */
+  float guide_fraction;      /* guided renders: probability of sampling the network's mixture at a
+                                diffuse vertex (one-sample MIS with cosine sampling, the mixture pdf
+                                (1 - f) cos/pi + f q); in [0, 1), 0 = default 0.5 */
 } tc_render_options;
 
 /* Counters of the most recent tc_render / tc_trace_* call. */

@@ -722,6 +722,8 @@ static int enqueue_render(tc_context* ctx, const tc_gpu_render_params* p, const 
     return fail(ctx, TC_ERR_INVALID, "block_size must be a multiple of 32 in [32, 256]");
   if (o.guiding && o.guide_record) return fail(ctx, TC_ERR_INVALID, "guiding and guide_record are exclusive");
   if (o.guiding && !ctx->has_guide) return fail(ctx, TC_ERR_STATE, "guided rendering needs tc_guide_set_params first");
+  if (!(o.guide_fraction >= 0.0f && o.guide_fraction < 1.0f))
+    return fail(ctx, TC_ERR_INVALID, "guide_fraction must be in [0, 1)");
   if (o.short_stack > 16) return fail(ctx, TC_ERR_INVALID, "short_stack must be at most 16 entries");
   if (o.refill_lanes > 32) return fail(ctx, TC_ERR_INVALID, "refill_lanes must be at most 32");
   if (timing) TC_CUDA(ctx, cudaEventRecord(ctx->ev_begin, st));
@@ -775,6 +777,7 @@ static int enqueue_render(tc_context* ctx, const tc_gpu_render_params* p, const 
     // suspended diffuse vertices -> tensor-core inference of their mixtures -> resume). Counts
     // stay on the device, so the rounds need no host synchronisation.
     const uint32_t wave_cap = o.wave_paths ? o.wave_paths : (1u << 23);
+    L.g.guide_fraction = o.guide_fraction > 0.0f ? o.guide_fraction : 0.5f;
     const uint32_t wave_spp = std::max<uint32_t>(1u, std::min<uint32_t>(p->samples, wave_cap / npix));
     const uint32_t cap = wave_spp * npix;
     const uint32_t rounds = p->max_bounces > 1 ? p->max_bounces - 1 : 0;

@@ -55,6 +55,7 @@ struct GuideLaunch {
   uint32_t resume;         // 0: start the wave's camera paths, 1: resume in_state
   uint32_t wave_first_sample;
   uint32_t wave_spp;
+  float guide_fraction;    // probability of sampling the guide's mixture at a diffuse vertex
 };
 
 // Path kernel modes.

@@ -439,7 +439,9 @@ __device__ __forceinline__ bool prepare_env_shadow(const RenderLaunch& L, const 
   if (cs <= 0.0f || pdf <= 0.0f) return false;
   float indirect_pdf = cs / kPiF;
   if constexpr (kMode == kModeGuided) {
-    if (ln.mix_slot >= 0) indirect_pdf = 0.5f * indirect_pdf + 0.5f * mix_pdf(L.g.in_mix + 10 * size_t(ln.mix_slot), dir);
+    if (ln.mix_slot >= 0)
+      indirect_pdf = (1.0f - L.g.guide_fraction) * indirect_pdf +
+                     L.g.guide_fraction * mix_pdf(L.g.in_mix + 10 * size_t(ln.mix_slot), dir);
   }
   const float mis = power_heuristic(pdf, indirect_pdf);
   ln.pend = ln.thr * ln.alb * rad * (cs * mis / (kPiF * pdf));
@@ -721,12 +723,13 @@ __global__ void __launch_bounds__(256) render_kernel(const RenderLaunch L) {
           }
           if constexpr (kMode == kModeGuided) {
             if (ln.mix_slot >= 0) {
-              // One-sample MIS of BSDF and guide sampling (the balance heuristic = the 50/50
-              // mixture pdf), so the estimator stays unbiased whatever the network predicts.
+              // One-sample MIS of BSDF and guide sampling (the balance heuristic = the mixture
+              // pdf, guide taken with probability guide_fraction), so the estimator stays
+              // unbiased whatever the network predicts.
               const float4* mix = L.g.in_mix + 10 * size_t(ln.mix_slot);
               const float ut = ln.rng.uniform();
               V3 dir;
-              if (ut < 0.5f) {
+              if (ut < 1.0f - L.g.guide_fraction) {
                 dir = ln.hn + uniform_sphere(ln.rng.uniform(), ln.rng.uniform());
                 if (dot(dir, dir) < 1e-8f) dir = ln.hn;
                 dir = normalize(dir);
@@ -740,7 +743,7 @@ __global__ void __launch_bounds__(256) render_kernel(const RenderLaunch L) {
                 finish_sample<kMode, kMoments>(L, J, ln, n_paths);
                 break;
               }
-              const float p = 0.5f * cs / kPiF + 0.5f * mix_pdf(mix, dir);
+              const float p = (1.0f - L.g.guide_fraction) * cs / kPiF + L.g.guide_fraction * mix_pdf(mix, dir);
               ln.ro = ln.hp;
               ln.rd = dir;
               ln.thr = ln.thr * ln.alb * (cs / (kPiF * p));

@@ -118,6 +118,7 @@ class RenderOptions(ctypes.Structure):
         ("wave_paths", ctypes.c_uint32),
         ("short_stack", ctypes.c_uint32),
         ("refill_lanes", ctypes.c_uint32),
+        ("guide_fraction", ctypes.c_float),
     ]
 
 

@@ -225,8 +225,11 @@ class GpuRenderer:
     def render(self, samples: Optional[int] = None, max_bounces: Optional[int] = None, width: Optional[int] = None,
                height: Optional[int] = None, frame_index: int = 0, accumulate: bool = False,
                keep_moments: bool = False, block_size: int = 0, samples_per_item: int = 0, guiding: bool = False,
-               guide_record: bool = False, wave_paths: int = 0, short_stack: int = 0, refill_lanes: int = 0) -> None:
-        """Traces ``samples`` paths per pixel; ``accumulate`` adds them to the previous batches."""
+               guide_record: bool = False, wave_paths: int = 0, short_stack: int = 0, refill_lanes: int = 0,
+               guide_fraction: float = 0.0) -> None:
+        """Traces ``samples`` paths per pixel; ``accumulate`` adds them to the previous batches.
+        ``guide_fraction``: probability of sampling the network's mixture at a guided diffuse
+        vertex (0 = the library's default, 0.5)."""
         if self._params is None:
             raise RuntimeError("render before upload")
         p = self._params.copy()
@@ -249,6 +252,7 @@ class GpuRenderer:
         opts.wave_paths = wave_paths
         opts.short_stack = short_stack
         opts.refill_lanes = refill_lanes
+        opts.guide_fraction = guide_fraction
         self._check(self._lib.tc_render(self._ctx, p.ctypes.data, ctypes.byref(opts)))
         self.width, self.height = int(p["width"][0]), int(p["height"][0])
         self.accumulated = (self.accumulated if accumulate else 0) + int(p["samples"][0])
