@@ -7,6 +7,7 @@ import pytest
 
 from oracle import guide_net as gn
 from toaster_b200 import configs, guiding_eval
+from toaster_b200.native import TcError
 from toaster_b200.renderer import GpuRenderer
 from toaster_b200.scene import scene_to_gpu
 
@@ -34,14 +35,15 @@ def render_moments(r, spp, **kw):
 @pytest.mark.parametrize("make", [lambda: configs.mixed(width=64, height=36, samples=64),
                                   lambda: configs.room_with_window(width=64, height=36, samples=64, clutter=1024)],
                          ids=["mixed", "room"])
-def test_guided_sampling_is_unbiased(renderer, make):
+@pytest.mark.parametrize("fraction", [0.0, 0.85], ids=["default_mix", "guide_heavy"])
+def test_guided_sampling_is_unbiased(renderer, make, fraction):
     # Untrained (random) network: the one-sample MIS of BSDF and guide sampling must still give
-    # the plain estimator's expectation.
+    # the plain estimator's expectation, at the default mixing probability and a guide-heavy one.
     scene = make()
     renderer.upload(scene_to_gpu(scene))
     renderer.guide_set_params(guiding_eval.initial_params(7), configs.scene_bounds(scene))
     pl, pv, n = render_moments(renderer, 2048, frame_index=3)
-    gl, gv, m = render_moments(renderer, 2048, frame_index=4, guiding=True)
+    gl, gv, m = render_moments(renderer, 2048, frame_index=4, guiding=True, guide_fraction=fraction)
     d = blocks(gl - pl, 2) / 4
     var = (blocks(pv, 2) / n + blocks(gv, 2) / m) / 16
     nz = var > 0
@@ -50,6 +52,15 @@ def test_guided_sampling_is_unbiased(renderer, make):
     assert abs(np.median(z)) <= 0.35
     se = math.sqrt((pv.sum() / n + gv.sum() / m)) / pv.size
     assert abs(gl.mean() - pl.mean()) <= 6 * se, (gl.mean(), pl.mean(), se)
+
+
+def test_guide_fraction_outside_unit_interval_is_rejected(renderer):
+    scene = configs.mixed(width=16, height=8, samples=4)
+    renderer.upload(scene_to_gpu(scene))
+    renderer.guide_set_params(guiding_eval.initial_params(7), configs.scene_bounds(scene))
+    for bad in (1.0, -0.25, float("nan")):
+        with pytest.raises(TcError, match="guide_fraction"):
+            renderer.render(samples=4, guiding=True, guide_fraction=bad)
 
 
 def test_record_train_and_render_guided(renderer):
