@@ -54,6 +54,8 @@ def parse_args():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--spp", type=int, default=64, help="samples per pixel per frame (64 = the benchmark workload)")
     ap.add_argument("--no-equal-time", action="store_true", help="skip the guided-vs-plain equal-time comparison")
+    ap.add_argument("--no-reference-suite", action="store_true",
+                    help="skip the reference's own benchmark fixtures under its protocol")
     ap.add_argument("--equal-time-ref-spp", type=int, default=4096,
                     help="samples per pixel of the plain FP64 reference the equal-time RMSE is measured against")
     ap.add_argument("--cpu-table", action="store_true",
@@ -344,6 +346,8 @@ def run_ours(args):
             line["roofline"] = roofline
         if world == 1 and not args.no_equal_time:
             line["equal_time"] = equal_time_block(args.equal_time_ref_spp, local)
+        if world == 1 and not args.no_reference_suite:
+            line["reference_suite"] = reference_suite_block(local)
         if world == 1 and args.batch_eval:
             from toaster_b200 import batch_eval
             line["batched"] = batch_eval.uneven()
@@ -359,6 +363,23 @@ def run_ours(args):
     if world > 1:
         dist.destroy_process_group()
     return 0
+
+
+def reference_suite_block(device: int) -> dict:
+    """The reference's seven benchmark fixtures (regenerated byte for byte; 320x180, 4 spp,
+    4 bounces) under its own protocol (2 warm-up + 5 measured frames, seed 0, medians), beside the
+    RTX 2080 Ti medians it publishes. Loaded through the native scene loader."""
+    import tempfile
+
+    from toaster_b200 import bench_fixtures
+
+    with tempfile.TemporaryDirectory() as tmp:
+        rows = bench_fixtures.run(tmp, device=device)
+    keep = ("dispatch_ms", "kernel_ms", "total_ms", "published_2080ti_dispatch_ms", "published_2080ti_total_ms",
+            "dispatch_speedup_vs_published", "total_speedup_vs_published")
+    return {"protocol": "320x180, 4 spp, 4 bounces; median of 5 frames after 2 warm-up frames; seed 0",
+            "published": "RTX 2080 Ti / Vulkan medians from the reference's README",
+            "fixtures": {row["scene"].split(".")[0]: {k: row[k] for k in keep} for row in rows}}
 
 
 def equal_time_block(ref_spp: int, device: int) -> dict:

@@ -627,3 +627,23 @@ def test_reference_known_answers():
         p = n.params[0]
         assert (p["triangle_count"], p["sphere_count"], p["background_kind"] == 2) == (tris, spheres, env), name
         assert (p["width"], p["height"], p["samples"], p["max_bounces"]) == (320, 180, 4, 4), name
+
+
+def test_c_abi_arguments_and_error_truncation(tmp_path):
+    import ctypes
+
+    from toaster_b200 import native
+
+    lib = native.load_library()
+    out = ctypes.c_void_p()
+    err = ctypes.create_string_buffer(16)
+    assert lib.tc_scene_load(None, ctypes.byref(out), err, len(err)) == native.TC_ERR_INVALID
+    assert lib.tc_scene_load(b"x.json", None, err, len(err)) == native.TC_ERR_INVALID
+    missing = str(tmp_path / "absent.json").encode()
+    assert lib.tc_scene_load(missing, ctypes.byref(out), err, len(err)) == native.TC_ERR_INVALID
+    assert not out.value and len(err.value) == 15 and err.value.startswith(b"failed to open")
+    assert lib.tc_scene_load(missing, ctypes.byref(out), None, 0) == native.TC_ERR_INVALID
+    assert lib.tc_loaded_scene_data(None) is None or not lib.tc_loaded_scene_data(None)
+    exposure = ctypes.c_float()
+    assert lib.tc_loaded_scene_display(None, ctypes.byref(exposure)) == native.TC_ERR_INVALID
+    assert lib.tc_loaded_scene_free(None) == native.TC_OK

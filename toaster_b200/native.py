@@ -19,6 +19,11 @@ LIB_DIR = Path(__file__).resolve().parent / "lib"
 LIB_PATH = LIB_DIR / "libtoaster_cuda.so"
 
 TC_OK = 0
+TC_ERR_INVALID = -1
+TC_ERR_CUDA = -2
+TC_ERR_NO_DEVICE = -3
+TC_ERR_STATE = -4
+TC_ERR_DEVICE_STATUS = -5
 TC_MISS = 0xFFFFFFFF
 TC_PRIM_TRIANGLE_BIT = 0x80000000
 
