@@ -35,15 +35,17 @@ def render_moments(r, spp, **kw):
 @pytest.mark.parametrize("make", [lambda: configs.mixed(width=64, height=36, samples=64),
                                   lambda: configs.room_with_window(width=64, height=36, samples=64, clutter=1024)],
                          ids=["mixed", "room"])
-@pytest.mark.parametrize("fraction", [0.0, 0.85], ids=["default_mix", "guide_heavy"])
-def test_guided_sampling_is_unbiased(renderer, make, fraction):
+@pytest.mark.parametrize("fraction,spp", [(0.0, 2048), (0.85, 8192)], ids=["default_mix", "guide_heavy"])
+def test_guided_sampling_is_unbiased(renderer, make, fraction, spp):
     # Untrained (random) network: the one-sample MIS of BSDF and guide sampling must still give
     # the plain estimator's expectation, at the default mixing probability and a guide-heavy one.
+    # The sun makes both estimators heavy-tailed, so the guide-heavy case takes more samples for
+    # its per-pixel variance estimates to hold.
     scene = make()
     renderer.upload(scene_to_gpu(scene))
     renderer.guide_set_params(guiding_eval.initial_params(7), configs.scene_bounds(scene))
-    pl, pv, n = render_moments(renderer, 2048, frame_index=3)
-    gl, gv, m = render_moments(renderer, 2048, frame_index=4, guiding=True, guide_fraction=fraction)
+    pl, pv, n = render_moments(renderer, spp, frame_index=3)
+    gl, gv, m = render_moments(renderer, spp, frame_index=4, guiding=True, guide_fraction=fraction)
     d = blocks(gl - pl, 2) / 4
     var = (blocks(pv, 2) / n + blocks(gv, 2) / m) / 16
     nz = var > 0
