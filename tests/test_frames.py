@@ -14,7 +14,7 @@ import pytest
 
 from toaster_b200 import configs
 from toaster_b200.frames import (AnimationConfig, BenchmarkFrameSink, FrameSink, FunctionSceneEvaluator,
-                                 GpuBenchmarkConfig, ProgressiveRenderConfig, StaticSceneEvaluator,
+                                 GpuBenchmarkConfig, MjpegFrameSink, ProgressiveRenderConfig, StaticSceneEvaluator,
                                  benchmark_gpu_evaluator, frame_output_path, render_evaluated_gpu_animation,
                                  render_gpu_progressive_with_sink, render_gpu_with_sink)
 from toaster_b200.scene import load_scene, scene_to_gpu
@@ -93,6 +93,10 @@ class RecordingRenderer:
 
     def stats(self):
         return {"kernel_ms": 1.0}
+
+    def encode_jpeg(self, quality=90, exposure_stops=0.0):
+        self.calls.append(("jpeg", quality, exposure_stops))
+        return b"\xff\xd8" + bytes([len(self.calls) % 256]) + b"\xff\xd9"
 
     def readback_rgba8(self, exposure_stops=0.0):
         self.calls.append(("readback", exposure_stops))
@@ -191,3 +195,18 @@ def test_loaded_scene_exposure_reaches_the_display(tmp_path):
     r = RecordingRenderer()
     render_gpu_with_sink(StaticSceneEvaluator(load_scene(p)), AnimationConfig.single_frame(), ListSink(), renderer=r)
     assert [c[1] for c in r.calls if c[0] == "readback"] == [-1.25]
+
+
+def test_mjpeg_sink_streams_device_jpegs():
+    import io
+
+    from toaster_b200.stream import split_mjpeg
+
+    buf = io.BytesIO()
+    r = RecordingRenderer()
+    sink = MjpegFrameSink(buf, quality=70, max_frames=3)
+    render_gpu_with_sink(StaticSceneEvaluator(small_scene()), AnimationConfig.indefinite(30), sink, renderer=r)
+    jpegs = split_mjpeg(buf.getvalue())
+    assert len(jpegs) == 3 and all(j[:2] == b"\xff\xd8" for j in jpegs)
+    assert [c for c in r.calls if c[0] == "readback"] == []
+    assert {c[1] for c in r.calls if c[0] == "jpeg"} == {70}

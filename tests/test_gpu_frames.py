@@ -1,13 +1,15 @@
 """The host frame loop on the GPU (needs a B200): PNG animation frames equal direct renders of the
-same evaluated scenes, and a progressive render reaches its exact sample target."""
+same evaluated scenes, a progressive render reaches its exact sample target, and the MJPEG sink
+streams device-encoded frames."""
 
 import numpy as np
 import pytest
 
 from toaster_b200 import configs
 from toaster_b200.frames import (AnimationConfig, FrameSink, FunctionSceneEvaluator, GpuBenchmarkConfig,
-                                 ProgressiveRenderConfig, StaticSceneEvaluator, benchmark_gpu_evaluator,
-                                 render_evaluated_gpu_animation, render_gpu_progressive_with_sink)
+                                 MjpegFrameSink, ProgressiveRenderConfig, StaticSceneEvaluator, benchmark_gpu_evaluator,
+                                 render_evaluated_gpu_animation, render_gpu_progressive_with_sink,
+                                 render_gpu_with_sink)
 from toaster_b200.renderer import GpuRenderer
 from toaster_b200.scene import _decode_png, scene_to_gpu
 
@@ -47,3 +49,17 @@ def test_progressive_reaches_target_and_benchmark_measures(native_lib):
     res = benchmark_gpu_evaluator(StaticSceneEvaluator(scene), GpuBenchmarkConfig(1, 2))
     assert len(res.frames) == 2 and res.final_image.shape == (36, 64, 4)
     assert all(t.kernel_ms > 0 for t in res.frames)
+
+
+def test_mjpeg_sink_streams_device_encoded_frames(native_lib):
+    import io
+
+    from toaster_b200.stream import split_mjpeg
+
+    anim = configs.BallisticAnimation(width=96, height=54, samples=4, max_bounces=4, frames=4)
+    ev = FunctionSceneEvaluator(lambda t: anim.scene(int(round(t * 24)) % 4))
+    buf = io.BytesIO()
+    render_gpu_with_sink(ev, AnimationConfig.indefinite(24), MjpegFrameSink(buf, quality=80, max_frames=3))
+    jpegs = split_mjpeg(buf.getvalue())
+    assert len(jpegs) == 3
+    assert all(j[:2] == b"\xff\xd8" and j[-2:] == b"\xff\xd9" and len(j) > 500 for j in jpegs)

@@ -4,8 +4,9 @@ Mirrors the public surface of ``toaster_gpu`` (crates/toaster-gpu/src/lib.rs:28-
 drives the reference through it can switch backends:
 
 - ``AnimationConfig`` and ``frame_output_path`` (crates/toaster-gpu/src/animation.rs:8-153);
-- ``FrameSink`` / ``CompletedFrame`` / ``GpuFrameTimings`` (path_tracer.rs:30-180) and the PNG and
-  benchmark sinks (:183-255);
+- ``FrameSink`` / ``CompletedFrame`` / ``GpuFrameTimings`` (path_tracer.rs:30-180), the PNG and
+  benchmark sinks (:183-255) and an MJPEG sink like the preview server's stream
+  (crates/toaster-server/src/routes.rs:82-110) fed by the device JPEG encoder;
 - ``render_evaluated_gpu_animation``, ``render_evaluated_gpu_animation_with_sink``,
   ``render_gpu_progressive_with_sink`` and ``benchmark_gpu_evaluator`` (:268-515), all running the
   loop of ``render_gpu_with_sink`` (:517-840): evaluate, pack, update the device scene, render,
@@ -31,7 +32,7 @@ import numpy as np
 
 from .renderer import GpuRenderer, progressive_batch, render_frame_seed
 from .scene import Scene, SceneGpuData, scene_to_gpu
-from .stream import encode_png
+from .stream import encode_png, mjpeg_part
 
 
 # ------------------------------------------------------------------------------------ schedules
@@ -162,12 +163,18 @@ class CompletedFrame:
     max_bounces: int
     timings: GpuFrameTimings
     render_time: float
-    image: np.ndarray  # (height, width, 4) uint8, valid only during deliver()
+    image: Optional[np.ndarray]  # (height, width, 4) uint8, valid only during deliver(); None for JPEG sinks
     counters: dict
+    jpeg: Optional[bytes] = None  # the frame as JPEG bytes, for sinks that ask for them
 
 
 class FrameSink:
-    """Consumer of completed frames (path_tracer.rs:162-180); delivery applies backpressure."""
+    """Consumer of completed frames (path_tracer.rs:162-180); delivery applies backpressure.
+
+    A sink whose ``jpeg_quality`` is set receives the frame JPEG-encoded on the device
+    (``CompletedFrame.jpeg``) instead of RGBA8 pixels, as a preview stream wants it."""
+
+    jpeg_quality: Optional[int] = None
 
     def deliver(self, frame: CompletedFrame) -> None:
         raise NotImplementedError
@@ -193,6 +200,23 @@ class PngFrameSink(FrameSink):
         path = frame_output_path(self.out_path, frame.index, self.frame_count)
         path.write_bytes(encode_png(frame.image))
         self.written.append(path)
+
+
+class MjpegFrameSink(FrameSink):
+    """Writes every frame as one ``multipart/x-mixed-replace`` part to a binary stream, the way the
+    reference's preview server publishes frames (crates/toaster-server/src/routes.rs:82-110); the
+    JPEG is made on the device. ``max_frames`` ends the stream after that many frames."""
+
+    def __init__(self, stream, quality: int = 85, max_frames: Optional[int] = None):
+        self.stream, self.jpeg_quality, self.max_frames = stream, quality, max_frames
+        self.frames = 0
+
+    def deliver(self, frame: CompletedFrame) -> None:
+        self.stream.write(mjpeg_part(frame.jpeg))
+        self.frames += 1
+
+    def should_continue(self) -> bool:
+        return self.max_frames is None or self.frames < self.max_frames
 
 
 class BenchmarkFrameSink(FrameSink):
@@ -350,7 +374,11 @@ def render_gpu_with_sink(evaluator, animation: AnimationConfig, sink: FrameSink,
             timings.dispatch_wait = time.perf_counter() - d0
             timings.kernel_ms = float(r.stats()["kernel_ms"])
             b0 = time.perf_counter()
-            image = r.readback_rgba8(exposure)
+            image, jpeg = None, None
+            if sink.jpeg_quality is not None:
+                jpeg = r.encode_jpeg(int(sink.jpeg_quality), exposure)
+            else:
+                image = r.readback_rgba8(exposure)
             timings.readback = time.perf_counter() - b0
             render_time = time.perf_counter() - f0
             timings.total = render_time
@@ -358,7 +386,7 @@ def render_gpu_with_sink(evaluator, animation: AnimationConfig, sink: FrameSink,
             o0 = time.perf_counter()
             sink.deliver(CompletedFrame(frame, t_sec, r.width, r.height, samples, completed,
                                         int(data.params["max_bounces"][0]), timings, render_time, image,
-                                        dict(evaluated.counters)))
+                                        dict(evaluated.counters), jpeg))
             timings.output = time.perf_counter() - o0
             timings.total = time.perf_counter() - f0
             sink.record_timings(frame, timings)
