@@ -210,3 +210,19 @@ def test_mjpeg_sink_streams_device_jpegs():
     assert len(jpegs) == 3 and all(j[:2] == b"\xff\xd8" for j in jpegs)
     assert [c for c in r.calls if c[0] == "readback"] == []
     assert {c[1] for c in r.calls if c[0] == "jpeg"} == {70}
+
+
+def test_video_export_writes_an_mjpeg_avi(tmp_path):
+    from toaster_b200.frames import render_evaluated_gpu_video
+    from toaster_b200.stream import read_avi_mjpeg
+
+    r = RecordingRenderer()
+    n = render_evaluated_gpu_video(StaticSceneEvaluator(small_scene()), tmp_path / "clip.avi",
+                                   AnimationConfig.from_frame_count(12, 4), quality=75, renderer=r)
+    w, h, fps, frames = read_avi_mjpeg(tmp_path / "clip.avi")
+    assert (n, w, h, fps, len(frames)) == (4, 16, 8, 12, 4)
+    assert all(f[:2] == b"\xff\xd8" for f in frames)
+    assert {c[1] for c in r.calls if c[0] == "jpeg"} == {75}
+    with pytest.raises(ValueError, match="FPS"):
+        render_evaluated_gpu_video(StaticSceneEvaluator(small_scene()), tmp_path / "x.avi",
+                                   AnimationConfig.single_frame(), renderer=r)

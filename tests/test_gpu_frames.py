@@ -63,3 +63,15 @@ def test_mjpeg_sink_streams_device_encoded_frames(native_lib):
     jpegs = split_mjpeg(buf.getvalue())
     assert len(jpegs) == 3
     assert all(j[:2] == b"\xff\xd8" and j[-2:] == b"\xff\xd9" and len(j) > 500 for j in jpegs)
+
+
+def test_video_export_holds_the_device_jpegs(native_lib, tmp_path):
+    from toaster_b200.frames import render_evaluated_gpu_video
+    from toaster_b200.stream import read_avi_mjpeg
+
+    anim = configs.BallisticAnimation(width=96, height=54, samples=4, max_bounces=4, frames=3)
+    ev = FunctionSceneEvaluator(lambda t: anim.scene(int(round(t * 24))))
+    assert render_evaluated_gpu_video(ev, tmp_path / "clip.avi", AnimationConfig.from_frame_count(24, 3)) == 3
+    w, h, fps, frames = read_avi_mjpeg(tmp_path / "clip.avi")
+    assert (w, h, fps, len(frames)) == (96, 54, 24, 3)
+    assert all(f[:2] == b"\xff\xd8" and f[-2:] == b"\xff\xd9" for f in frames)

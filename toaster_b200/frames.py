@@ -7,8 +7,9 @@ drives the reference through it can switch backends:
 - ``FrameSink`` / ``CompletedFrame`` / ``GpuFrameTimings`` (path_tracer.rs:30-180), the PNG and
   benchmark sinks (:183-255) and an MJPEG sink like the preview server's stream
   (crates/toaster-server/src/routes.rs:82-110) fed by the device JPEG encoder;
-- ``render_evaluated_gpu_animation``, ``render_evaluated_gpu_animation_with_sink``,
-  ``render_gpu_progressive_with_sink`` and ``benchmark_gpu_evaluator`` (:268-515), all running the
+- ``render_evaluated_gpu_animation``, ``render_evaluated_gpu_video`` (Motion-JPEG AVI),
+  ``render_evaluated_gpu_animation_with_sink``, ``render_gpu_progressive_with_sink`` and
+  ``benchmark_gpu_evaluator`` (:268-515), all running the
   loop of ``render_gpu_with_sink`` (:517-840): evaluate, pack, update the device scene, render,
   convert for display, deliver, record timings.
 
@@ -32,7 +33,7 @@ import numpy as np
 
 from .renderer import GpuRenderer, progressive_batch, render_frame_seed
 from .scene import Scene, SceneGpuData, scene_to_gpu
-from .stream import encode_png, mjpeg_part
+from .stream import AviMjpegWriter, encode_png, mjpeg_part
 
 
 # ------------------------------------------------------------------------------------ schedules
@@ -217,6 +218,21 @@ class MjpegFrameSink(FrameSink):
 
     def should_continue(self) -> bool:
         return self.max_frames is None or self.frames < self.max_frames
+
+
+class VideoFrameSink(FrameSink):
+    """Motion-JPEG AVI video of every frame (path_tracer.rs:206-234 writes through ffmpeg; here the
+    frames are JPEG-encoded on the device and muxed by AviMjpegWriter). ``finish`` closes it."""
+
+    def __init__(self, path, width: int, height: int, fps: int, quality: int = 90):
+        self.writer = AviMjpegWriter(path, width, height, fps)
+        self.jpeg_quality = quality
+
+    def deliver(self, frame: CompletedFrame) -> None:
+        self.writer.write_frame(frame.jpeg)
+
+    def finish(self) -> None:
+        self.writer.close()
 
 
 class BenchmarkFrameSink(FrameSink):
@@ -419,6 +435,25 @@ def render_evaluated_gpu_animation(evaluator, out_path, animation: AnimationConf
     sink = PngFrameSink(out_path, animation.frame_limit)
     render_gpu_with_sink(evaluator, animation, sink, **kw)
     return sink.written
+
+
+def render_evaluated_gpu_video(evaluator, video_path, animation: AnimationConfig, quality: int = 90, **kw) -> int:
+    """Every frame into one Motion-JPEG AVI file (path_tracer.rs:316-356: finite frames and an
+    FPS are required); returns the frame count. The file is finalised even if rendering fails."""
+    if animation.fps is None:
+        raise ValueError("video export requires an animated render with an FPS")
+    if animation.frame_limit is None:
+        raise ValueError("video export requires a finite frame count")
+    first = evaluator.evaluate(*animation.evaluation_request(0)).scene
+    params = first.params[0] if isinstance(first, SceneGpuData) else None
+    width = int(params["width"]) if params is not None else first.width
+    height = int(params["height"]) if params is not None else first.height
+    sink = VideoFrameSink(video_path, width, height, animation.fps, quality)
+    try:
+        render_gpu_with_sink(evaluator, animation, sink, **kw)
+    finally:
+        sink.finish()
+    return sink.writer.frames
 
 
 def render_gpu_progressive_with_sink(scene: Union[Scene, SceneGpuData], schedule: AnimationConfig,
