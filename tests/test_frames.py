@@ -226,3 +226,35 @@ def test_video_export_writes_an_mjpeg_avi(tmp_path):
     with pytest.raises(ValueError, match="FPS"):
         render_evaluated_gpu_video(StaticSceneEvaluator(small_scene()), tmp_path / "x.avi",
                                    AnimationConfig.single_frame(), renderer=r)
+
+
+def test_path_based_helpers(tmp_path):
+    import json
+
+    from toaster_b200.frames import (FramePacing, benchmark_gpu_scene, render_scene_gpu, render_scene_gpu_animation,
+                                     render_scene_gpu_animation_with_sink, render_scene_gpu_video)
+    from toaster_b200.stream import read_avi_mjpeg
+
+    doc = {"camera": {"position": [0, 0, 3], "look_at": [0, 0, 0], "fov_degrees": 40},
+           "render": {"width": 8, "height": 4, "samples": 2, "max_bounces": 2},
+           "display": {"exposure_stops": 0.5},
+           "materials": [{"name": "m", "type": "diffuse", "albedo": [0.5, 0.5, 0.5]}],
+           "objects": [{"type": "sphere", "center": [0, 0, 0], "radius": 1, "material": "m"}]}
+    p = tmp_path / "s.json"
+    p.write_text(json.dumps(doc))
+    r = RecordingRenderer()
+    assert [q.name for q in render_scene_gpu(p, tmp_path / "one.png", renderer=r)] == ["one.png"]
+    assert len(render_scene_gpu_animation(p, tmp_path / "f.png", AnimationConfig.from_frame_count(24, 2),
+                                          renderer=r)) == 2
+    assert render_scene_gpu_video(p, tmp_path / "v.avi", AnimationConfig.from_frame_count(24, 2), renderer=r) == 2
+    assert read_avi_mjpeg(tmp_path / "v.avi")[:3] == (8, 4, 24)
+    sink = ListSink()
+    render_scene_gpu_animation_with_sink(p, AnimationConfig.from_frame_count(24, 3), FramePacing.UNPACED, sink,
+                                         renderer=r)
+    assert len(sink.frames) == 3
+    assert len(benchmark_gpu_scene(p, GpuBenchmarkConfig(1, 2), renderer=r).frames) == 2
+    assert {c[1] for c in r.calls if c[0] == "readback"} == {0.5}
+    doc["animation"] = {"tracks": [{"type": "translation"}]}
+    p.write_text(json.dumps(doc))
+    with pytest.raises(ValueError, match="animation tracks"):
+        render_scene_gpu(p, tmp_path / "x.png", renderer=r)

@@ -11,7 +11,10 @@ drives the reference through it can switch backends:
   ``render_evaluated_gpu_animation_with_sink``, ``render_gpu_progressive_with_sink`` and
   ``benchmark_gpu_evaluator`` (:268-515), all running the
   loop of ``render_gpu_with_sink`` (:517-840): evaluate, pack, update the device scene, render,
-  convert for display, deliver, record timings.
+  convert for display, deliver, record timings;
+- the path-based helpers ``render_scene_gpu``, ``render_scene_gpu_animation``,
+  ``render_scene_gpu_video``, ``render_scene_gpu_animation_with_sink``,
+  ``render_gpu_animation_with_sink`` and ``benchmark_gpu_scene``, over the native scene loader.
 
 Differences by design: the display conversion runs on the device inside ``readback`` (the
 ``conversion`` timing is zero); a frame whose geometry changed is re-uploaded, which rebuilds
@@ -34,6 +37,13 @@ import numpy as np
 from .renderer import GpuRenderer, progressive_batch, render_frame_seed
 from .scene import Scene, SceneGpuData, scene_to_gpu
 from .stream import AviMjpegWriter, encode_png, mjpeg_part
+
+
+class FramePacing:
+    """Frame pacing of the loop (path_tracer.rs): as fast as possible, or one frame per 1/fps."""
+
+    UNPACED = "unpaced"
+    REAL_TIME = "realtime"
 
 
 # ------------------------------------------------------------------------------------ schedules
@@ -485,3 +495,52 @@ def benchmark_gpu_evaluator(evaluator, config: GpuBenchmarkConfig, **kw) -> GpuB
     if sink.final_image is None:
         raise RuntimeError("GPU benchmark did not produce a measured image")
     return GpuBenchmarkResult(summary.setup_time, sink.timings, sink.final_image)
+
+
+# ------------------------------------------------------------------------ path-based helpers
+def _static_file_evaluator(scene_path) -> StaticSceneEvaluator:
+    """A scene file's frames for the path-based helpers: loaded and packed by the native loader.
+    Animation tracks would need toaster-scene's evaluator, which this package does not include."""
+    import json
+
+    from .scene import load_scene_gpu
+
+    doc = json.loads(Path(scene_path).read_text(encoding="utf-8"))
+    if isinstance(doc, dict) and ((doc.get("animation") or {}).get("tracks") or []):
+        raise ValueError("the scene has animation tracks: evaluate them with an evaluator and call "
+                         "render_evaluated_gpu_animation")
+    data, exposure = load_scene_gpu(scene_path)
+    return StaticSceneEvaluator(data, exposure)
+
+
+def render_scene_gpu(scene_path, out_path, **kw) -> list:
+    """One frame of a scene file as PNG (path_tracer.rs:266-268)."""
+    return render_scene_gpu_animation(scene_path, out_path, AnimationConfig.single_frame(), **kw)
+
+
+def render_scene_gpu_animation(scene_path, out_path, animation: AnimationConfig, **kw) -> list:
+    """Numbered PNG frames of a scene file (path_tracer.rs:270-283)."""
+    return render_evaluated_gpu_animation(_static_file_evaluator(scene_path), out_path, animation, **kw)
+
+
+def render_scene_gpu_video(scene_path, video_path, animation: AnimationConfig, **kw) -> int:
+    """A scene file as Motion-JPEG AVI video (path_tracer.rs:302-314)."""
+    return render_evaluated_gpu_video(_static_file_evaluator(scene_path), video_path, animation, **kw)
+
+
+def render_scene_gpu_animation_with_sink(scene_path, animation: AnimationConfig, pacing: str, sink: FrameSink,
+                                         **kw) -> None:
+    """A scene file's frames into a sink (path_tracer.rs:358-372)."""
+    render_gpu_with_sink(_static_file_evaluator(scene_path), animation, sink, pacing=pacing, **kw)
+
+
+def render_gpu_animation_with_sink(scene: Union[Scene, SceneGpuData], animation: AnimationConfig, pacing: str,
+                                   sink: FrameSink, **kw) -> None:
+    """A loaded scene's frames into a sink (path_tracer.rs:374-389)."""
+    render_gpu_with_sink(StaticSceneEvaluator(scene), animation, sink, pacing=pacing, **kw)
+
+
+def benchmark_gpu_scene(scene, config: GpuBenchmarkConfig, **kw) -> GpuBenchmarkResult:
+    """Benchmark frames of a scene file or a loaded scene (path_tracer.rs:460-472)."""
+    ev = _static_file_evaluator(scene) if isinstance(scene, (str, Path)) else StaticSceneEvaluator(scene)
+    return benchmark_gpu_evaluator(ev, config, **kw)
