@@ -52,32 +52,42 @@ def host_display_rgba8(hdr: np.ndarray, exposure_stops: float = 0.0) -> np.ndarr
     return out
 
 
-def uneven(count: int = 16, samples: int = 32, max_bounces: int = 8, repeats: int = 3, device: int = 0) -> dict:
-    scenes = configs.uneven_batch(count=count, samples=samples, max_bounces=max_bounces)
+def uneven(count: int = 16, samples: int = 32, max_bounces: int = 8, repeats: int = 3, device: int = 0,
+           min_width: int = 320, max_width: int = 1280) -> dict:
+    """One batched launch over `count` uneven scenes against one launch per scene: device time of
+    the path kernels (CUDA events) and host time of the synchronous calls (each call waits)."""
+    scenes = configs.uneven_batch(count=count, samples=samples, max_bounces=max_bounces, min_width=min_width,
+                                  max_width=max_width)
     rs = [GpuRenderer(device) for _ in scenes]
     try:
         for r, s in zip(rs, scenes):
             r.upload(scene_to_gpu(s))
         paths = sum(s.width * s.height * s.samples for s in scenes)
         render_batch(rs, frame_index=0)  # warm-up
-        batched = []
+        batched, batched_host = [], []
         for k in range(repeats):
+            t0 = time.perf_counter()
             st = render_batch(rs, frame_index=1 + k)
+            batched_host.append((time.perf_counter() - t0) * 1e3)
             batched.append(st["kernel_ms"])
         for r in rs:
             r.render(frame_index=0)
-        single = []
+        single, single_host = [], []
         for k in range(repeats):
             tot = 0.0
+            t0 = time.perf_counter()
             for r in rs:
                 r.render(frame_index=1 + k)
                 tot += r.stats()["kernel_ms"]
+            single_host.append((time.perf_counter() - t0) * 1e3)
             single.append(tot)
         b, u = float(np.median(batched)), float(np.median(single))
+        bh, uh = float(np.median(batched_host)), float(np.median(single_host))
         return {"scenes": count, "triangles": [s.triangle_count for s in scenes],
                 "resolutions": [f"{s.width}x{s.height}" for s in scenes], "spp": samples, "max_bounces": max_bounces,
                 "paths": paths, "batched_ms": b, "unbatched_ms": u, "batched_mpaths_per_s": paths / (b * 1e3),
-                "unbatched_mpaths_per_s": paths / (u * 1e3), "speedup": u / b}
+                "unbatched_mpaths_per_s": paths / (u * 1e3), "speedup": u / b,
+                "batched_host_ms": bh, "unbatched_host_ms": uh, "host_speedup": uh / bh}
     finally:
         for r in rs:
             r.close()
@@ -161,6 +171,7 @@ def main():
     ap.add_argument("--no-guiding", action="store_true")
     args = ap.parse_args()
     print(json.dumps({"uneven": uneven(samples=args.spp)}), flush=True)
+    print(json.dumps({"uneven_small": uneven(samples=4, max_bounces=4, min_width=160, max_width=480)}), flush=True)
     print(json.dumps({"animation": animation(args.frames, args.width, args.height, args.spp,
                                              guiding=not args.no_guiding)}), flush=True)
 

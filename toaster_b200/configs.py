@@ -390,18 +390,18 @@ class BallisticAnimation:
 
 
 def uneven_batch(seed: int = 0, count: int = 16, samples: int = 32, max_bounces: int = 8,
-                 environment: EnvironmentMap | None = None) -> list:
+                 environment: EnvironmentMap | None = None, min_width: int = 320, max_width: int = 1280) -> list:
     """``count`` independent scenes for one batched launch: triangle counts log-uniform in
     [128, 262,144] (seeded random triangles as in random_triangles, scaled to a 4-unit cube, half
     diffuse, a quarter metal, a quarter dielectric, plus a ground sphere) and resolutions
-    log-uniform between 320x180 and 1280x720 (16:9, width a multiple of 16), lit by the mixed
-    scene's sky."""
+    log-uniform between min_width and max_width (16:9, width a multiple of 16; 320x180 to
+    1280x720 by default), lit by the mixed scene's sky."""
     rng = np.random.default_rng(seed + 7000)
     env = environment if environment is not None else sky_environment()
     out = []
     for i in range(count):
         n_tri = int(round(math.exp(rng.uniform(math.log(128), math.log(262144)))))
-        width = int(round(math.exp(rng.uniform(math.log(320), math.log(1280))) / 16)) * 16
+        width = int(round(math.exp(rng.uniform(math.log(min_width), math.log(max_width))) / 16)) * 16
         height = width * 9 // 16
         tris = random_triangles(n_tri, seed=seed * 100 + i) * np.float32(2.0)
         kinds = rng.uniform(0, 1, n_tri)
