@@ -647,3 +647,65 @@ def test_c_abi_arguments_and_error_truncation(tmp_path):
     exposure = ctypes.c_float()
     assert lib.tc_loaded_scene_display(None, ctypes.byref(exposure)) == native.TC_ERR_INVALID
     assert lib.tc_loaded_scene_free(None) == native.TC_OK
+
+
+def test_mutated_files_are_loaded_or_rejected(tmp_path):
+    """Seeded byte mutations of every input kind (scene JSON, glTF JSON, its buffer, GLB, PNG,
+    Radiance): each load must return OK or TC_ERR_INVALID with a message, never crash."""
+    import random
+
+    rng = random.Random(2024)
+    g = Gltf()
+    pos, idx = quad()
+    tex = png_bytes(np.arange(48, dtype=np.uint8).reshape(4, 3, 4) * 5, 6, interlace=True)
+    g.doc["images"] = [{"uri": "t.png"}]
+    g.doc["textures"] = [{"source": 0}]
+    g.doc["materials"] = [{"pbrMetallicRoughness": {"baseColorTexture": {"index": 0}}}]
+    a_pos = g.accessor(pos, 5126, "VEC3", sparse=([1], np.array([[0.5, -1, 0]], np.float32)))
+    a_uv = g.accessor(np.array([[0, 0], [255, 0], [255, 255], [0, 255]], np.uint8), 5121, "VEC2", normalized=True,
+                      stride=4)
+    g.doc["meshes"] = [{"primitives": [{"attributes": {"POSITION": a_pos, "TEXCOORD_0": a_uv},
+                                        "indices": g.accessor(idx, 5123, "SCALAR"), "material": 0}]}]
+    g.doc["nodes"] = [{"mesh": 0, "rotation": [0, 0.2, 0, 0.98], "children": [1]}, {"mesh": 0, "translation": [1, 0, 0]}]
+    g.doc["scenes"] = [{"nodes": [0]}]
+    g.write(tmp_path / "m.gltf", external=True)
+    g.write_glb(tmp_path / "m.glb")
+    rgbe = np.random.default_rng(1).integers(0, 256, (6, 12, 4), dtype=np.uint8)
+    rgbe[..., 3] = 130
+    scene = scene_doc([{"type": "mesh", "path": "m.gltf"}, {"type": "mesh", "path": "m.glb", "material": "white"},
+                       {"type": "sphere", "center": [0, 0, 0], "radius": 1, "material": "light"}],
+                      background={"type": "environment", "path": "e.hdr", "intensity": 2})
+    base = {"m.gltf": (tmp_path / "m.gltf").read_bytes(), "m.bin": (tmp_path / "m.bin").read_bytes(),
+            "m.glb": (tmp_path / "m.glb").read_bytes(), "t.png": tex, "e.hdr": hdr_bytes(rgbe, "rle"),
+            "scene.json": json.dumps(scene).encode()}
+
+    def mutate(b):
+        b = bytearray(b)
+        for _ in range(rng.randint(1, 8)):
+            i = rng.randrange(len(b))
+            op = rng.random()
+            if op < 0.4:
+                b[i] = rng.randrange(256)
+            elif op < 0.6:
+                del b[i:i + rng.randint(1, 16)]
+            elif op < 0.8:
+                b[i:i] = bytes(rng.randrange(256) for _ in range(rng.randint(1, 8)))
+            else:
+                j = rng.randrange(len(b))
+                b[i:i + 4] = b[j:j + 4]
+        return bytes(b) or b"x"
+
+    outcomes = {}
+    for _ in range(300):
+        files = dict(base)
+        target = rng.choice(sorted(files))
+        files[target] = mutate(files[target])
+        for name, data in files.items():
+            (tmp_path / name).write_bytes(data)
+        try:
+            load_scene_gpu(tmp_path / "scene.json")
+            outcomes["ok"] = outcomes.get("ok", 0) + 1
+        except TcError as e:
+            assert e.code == -1 and len(str(e)) > 25
+            outcomes["rejected"] = outcomes.get("rejected", 0) + 1
+    assert outcomes.get("ok", 0) > 0 and outcomes.get("rejected", 0) > 0
