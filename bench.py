@@ -385,7 +385,7 @@ def reference_suite_block(device: int) -> dict:
 def equal_time_block(ref_spp: int, device: int) -> dict:
     """Guided vs plain sampling at equal GPU time on the learned-guiding workload (window room,
     8,192 clutter triangles with 30% metal, 1280x720, 8 bounces): plain accumulates 256 spp in
-    16-spp batches; guided records 16 spp, trains 600 Adam steps on the GPU and accumulates guided
+    16-spp batches; guided records 16 spp, trains the recipe's Adam steps on the GPU and accumulates guided
     batches. RMSE is against a plain FP64 reference of ``ref_spp`` samples per pixel; the trimmed
     RMSE leaves out the 0.1% largest pixel errors."""
     from toaster_b200 import configs, guiding_eval
@@ -393,13 +393,14 @@ def equal_time_block(ref_spp: int, device: int) -> dict:
     scene = configs.room_with_window()
     t0 = time.perf_counter()
     out = guiding_eval.equal_time_comparison(scene, ref_spp=ref_spp, plain_spp=256, batch=16, record_spp=16,
-                                             train_steps=600, train_batch=8192, seed=0, device=device)
+                                             train_steps=guiding_eval.TRAIN_STEPS, train_batch=8192, seed=0,
+                                             device=device)
     keep = ["plain_seconds", "plain_rmse", "guided_seconds_to_plain_rmse", "time_fraction",
             "guided_rmse_at_plain_time", "plain_trimmed_rmse", "time_fraction_trimmed",
             "guided_trimmed_rmse_at_plain_time", "train_seconds", "samples"]
     block = {k: out[k] for k in keep}
     block.update(workload="window room, 8,192 clutter triangles (30% metal), 1280x720, 8 bounces",
-                 reference_spp=ref_spp, plain_spp=256, record_spp=16, train_steps=600,
+                 reference_spp=ref_spp, plain_spp=256, record_spp=16, train_steps=guiding_eval.TRAIN_STEPS,
                  wall_seconds=time.perf_counter() - t0)
     return block
 

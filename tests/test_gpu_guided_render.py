@@ -96,7 +96,7 @@ def test_trained_network_beats_untrained_network(native_lib):
             r.guide_set_params(guiding_eval.initial_params(0), configs.scene_bounds(scene))
             if trained:
                 r.render(samples=32, frame_index=0, guide_record=True)
-                _, n = r.guide_train_recorded(600, 8192, 1e-2, 1)
+                _, n = r.guide_train_recorded(guiding_eval.TRAIN_STEPS, 8192, 1e-2, 1)
                 assert n > 5000
             r.render(samples=128, frame_index=50_000, guiding=True)
             s, _, cnt = r.readback_sums()

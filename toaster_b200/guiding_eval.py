@@ -26,6 +26,13 @@ from . import configs
 from .renderer import GpuRenderer
 from .scene import Scene, scene_to_gpu
 
+# Adam steps of the guiding recipe (batch 8,192, lr 1e-2) on the 16 recorded spp. Training acts as
+# an early stop: on the window room the per-pixel variance of guided sampling is lowest after 100-200
+# steps and rises as the loss keeps falling (the target, a one-sample estimate from 16 spp, rewards
+# lobes that are too narrow).
+TRAIN_STEPS = 200
+
+
 def initial_params(seed: int = 0) -> np.ndarray:
     """He-uniform hidden layers, a 10x smaller output layer, zero biases, zero padded inputs."""
     rng = np.random.default_rng(seed)
@@ -135,10 +142,11 @@ def time_to_reach(points, target: float, col: int = 2):
 
 
 def equal_time_comparison(scene: Scene, ref_spp: int, plain_spp: int = 256, batch: int = 16, record_spp: int = 16,
-                          guided_spp: int | None = None, train_steps: int = 300, train_batch: int = 8192,
+                          guided_spp: int | None = None, train_steps: int | None = None, train_batch: int = 8192,
                           seed: int = 0, device: int = 0, reference: np.ndarray | None = None) -> dict:
     if reference is None:
         reference = reference_image(scene, ref_spp, device=device)
+    train_steps = TRAIN_STEPS if train_steps is None else train_steps
     # Each seed draws its own path samples (frame indices offset by 100,000 per seed).
     plain = timeline_plain(scene, reference, plain_spp, batch, device, frame_offset=100_000 * seed)
     guided, info = timeline_guided(scene, reference, guided_spp or plain_spp, batch, record_spp, train_steps,
@@ -211,7 +219,7 @@ def main():
     ap.add_argument("--plain-spp", type=int, default=256)
     ap.add_argument("--guided-spp", type=int, default=0)
     ap.add_argument("--record-spp", type=int, default=16)
-    ap.add_argument("--train-steps", type=int, default=600)
+    ap.add_argument("--train-steps", type=int, default=0, help=f"Adam steps (default {TRAIN_STEPS}; --kernels: 600)")
     ap.add_argument("--clutter", type=int, default=8192)
     ap.add_argument("--metal", type=float, default=0.3)
     ap.add_argument("--seeds", type=int, default=1)
@@ -220,7 +228,8 @@ def main():
                     help="only time the network kernels (training, inference, one guided batch)")
     args = ap.parse_args()
     if args.kernels:
-        print(json.dumps(kernel_timings(args.width, args.height, args.record_spp, args.train_steps)), flush=True)
+        print(json.dumps(kernel_timings(args.width, args.height, args.record_spp, args.train_steps or 600)),
+              flush=True)
         return
     scene = configs.room_with_window(width=args.width, height=args.height, clutter=args.clutter,
                                      metal_fraction=args.metal)
@@ -229,7 +238,7 @@ def main():
     print(json.dumps({"reference_spp": args.ref_spp, "reference_seconds": time.perf_counter() - t0}), flush=True)
     for seed in range(args.seeds):
         out = equal_time_comparison(scene, args.ref_spp, args.plain_spp, record_spp=args.record_spp,
-                                    guided_spp=args.guided_spp or None, train_steps=args.train_steps, seed=seed,
+                                    guided_spp=args.guided_spp or None, train_steps=args.train_steps or None, seed=seed,
                                     reference=reference)
         if not args.timelines:
             out.pop("plain_timeline")
