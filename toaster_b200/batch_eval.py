@@ -94,7 +94,7 @@ def uneven(count: int = 16, samples: int = 32, max_bounces: int = 8, repeats: in
 
 
 def animation(frames: int = 240, width: int = 1280, height: int = 720, samples: int = 32, max_bounces: int = 8,
-              guiding: bool = True, train_steps: int = 400, device: int = 0) -> dict:
+              guiding: bool = True, train_steps: int = guiding_eval.TRAIN_STEPS, device: int = 0) -> dict:
     anim = configs.BallisticAnimation(width=width, height=height, samples=samples, max_bounces=max_bounces,
                                       frames=frames)
     pack_times = []
