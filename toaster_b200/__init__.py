@@ -24,13 +24,13 @@ __all__ = [
 
 def __getattr__(name):
     # The renderer needs the built CUDA library; import it on first use only.
-    if name in {"GpuRenderer", "render_scene_gpu", "render_gpu_progressive", "benchmark_gpu_scene",
-                "progressive_batch"}:
+    if name in {"GpuRenderer", "render_hdr", "render_batch", "progressive_batch"}:
         from . import renderer
 
         return getattr(renderer, name)
     if name in {"AnimationConfig", "FrameSink", "CompletedFrame", "render_evaluated_gpu_animation",
-                "render_evaluated_gpu_video", "render_gpu_progressive_with_sink", "benchmark_gpu_evaluator"}:
+                "render_evaluated_gpu_video", "render_gpu_progressive_with_sink", "benchmark_gpu_evaluator",
+                "render_scene_gpu", "benchmark_gpu_scene"}:
         from . import frames
 
         return getattr(frames, name)

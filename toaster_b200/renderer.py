@@ -1,16 +1,15 @@
-"""Host-side renderer API over the CUDA library, mirroring the public ``toaster_gpu`` surface.
+"""Host-side renderer API over the CUDA library: one ``GpuRenderer`` per context, one call per C-ABI
+entry point, plus batched launches and animation graphs.
 
-``render_scene_gpu``, ``render_gpu_progressive`` and ``benchmark_gpu_scene`` correspond to
-``render_scene_gpu`` / ``render_gpu_progressive_with_sink`` / ``benchmark_gpu_scene`` in
-crates/toaster-gpu/src/path_tracer.rs (lib.rs:28-37), with the same frame-seed, progressive
-batching and validation rules. Images are linear-HDR float4 (alpha = 1), row-major, y down.
+``progressive_batch`` and ``render_frame_seed`` keep the frame-seed and progressive batching rules
+of crates/toaster-gpu/src/path_tracer.rs:892-923; the reference's public entry points built on
+them (animation, video, progressive and benchmark renders) are in ``frames``. Images are
+linear-HDR float4 (alpha = 1), row-major, y down.
 """
 
 from __future__ import annotations
 
 import ctypes
-import dataclasses
-import time
 from typing import Optional
 
 import numpy as np
@@ -394,62 +393,10 @@ class GpuRenderer:
         return {f: getattr(s, f) for f, _ in native.Stats._fields_}
 
 
-def render_scene_gpu(scene: Scene, device: int = 0, frame_index: int = 0) -> np.ndarray:
-    """Renders one frame of ``scene`` at its own settings and returns the HDR image."""
+def render_hdr(scene: Scene, device: int = 0, frame_index: int = 0) -> np.ndarray:
+    """Renders one frame of ``scene`` at its own settings and returns the linear-HDR image
+    (height, width, 4) float32. The reference's file-based entry points are in ``frames``."""
     with GpuRenderer(device) as r:
         r.upload(scene_to_gpu(scene))
         r.render(frame_index=frame_index)
         return r.readback()
-
-
-def render_gpu_progressive(scene: Scene, target_samples: int, batch_samples: Optional[int] = None,
-                           device: int = 0, callback=None) -> np.ndarray:
-    """Progressive accumulation to exactly ``target_samples`` (path_tracer.rs:428-458)."""
-    batch_samples = batch_samples or scene.samples
-    with GpuRenderer(device) as r:
-        r.upload(scene_to_gpu(scene))
-        frame = 0
-        while True:
-            n = progressive_batch(batch_samples, r.accumulated, target_samples)
-            if n is None:
-                break
-            r.render(samples=n, frame_index=render_frame_seed(frame, False), accumulate=frame > 0)
-            if callback is not None:
-                callback(frame, r)
-            frame += 1
-        return r.readback()
-
-
-@dataclasses.dataclass
-class GpuBenchmarkResult:
-    setup_time_s: float
-    frames: list  # per measured frame: dict of stage timings (ms)
-    final_image: np.ndarray
-
-
-def benchmark_gpu_scene(scene: Scene, warmup_frames: int, measured_frames: int, device: int = 0) -> GpuBenchmarkResult:
-    """Static independent frames at time 0 and seed 0 (path_tracer.rs:476-515)."""
-    if measured_frames <= 0:
-        raise ValueError("benchmark measured frame count must be greater than zero")
-    t0 = time.perf_counter()
-    r = GpuRenderer(device)
-    data = scene_to_gpu(scene)
-    r.upload(data)
-    setup = time.perf_counter() - t0
-    frames = []
-    image = None
-    try:
-        for frame in range(warmup_frames + measured_frames):
-            f0 = time.perf_counter()
-            r.render(frame_index=render_frame_seed(frame, True))
-            f1 = time.perf_counter()
-            image = r.readback()
-            f2 = time.perf_counter()
-            st = r.stats()
-            if frame >= warmup_frames:
-                frames.append({"dispatch_wait_ms": (f1 - f0) * 1e3, "readback_ms": (f2 - f1) * 1e3,
-                               "kernel_ms": st["kernel_ms"], "total_ms": (f2 - f0) * 1e3, "rays": st["rays"],
-                               "paths": st["paths"]})
-    finally:
-        r.close()
-    return GpuBenchmarkResult(setup, frames, image)
