@@ -753,7 +753,11 @@ static int enqueue_render(tc_context* ctx, const tc_gpu_render_params* p, const 
   const int mode = o.guiding ? tcb::kModeGuided : (o.guide_record ? tcb::kModeRecord : tcb::kModePlain);
   int per_sm = tcb::render_max_blocks_per_sm(block, moments, mode, L.short_stack, L.min_active);
   if (per_sm <= 0) return fail(ctx, TC_ERR_CUDA, "render kernel cannot be resident with this block size");
-  const int grid = per_sm * ctx->sm_count;
+  // The persistent grid fills every SM; a frame with fewer work items than that needs fewer blocks
+  // (guided rounds size their work on the device, so they keep the full grid).
+  int grid = per_sm * ctx->sm_count;
+  if (mode != tcb::kModeGuided)
+    grid = int(std::max<uint64_t>(1, std::min<uint64_t>(uint64_t(grid), (L.total_items + block - 1) / block)));
   if (mode == tcb::kModeRecord) {
     // One record per diffuse scatter and per unoccluded environment shadow ray (capped), and the
     // final radiance of every path of the batch.

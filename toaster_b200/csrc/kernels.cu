@@ -613,10 +613,12 @@ __global__ void __launch_bounds__(256) render_kernel(const RenderLaunch L) {
   // The root record lives in device memory (a geometry refit rewrites it between launches);
   // single-frame launches stage it in shared memory once.
   __shared__ ChildRec root;
+  __shared__ unsigned long long s_count[3];  // this block's share of the launch counters
+  if (threadIdx.x < 3) s_count[threadIdx.x] = 0ull;
   if constexpr (!kBatch) {
     if (threadIdx.x == 0) root = *L.f.scene.root;
-    __syncthreads();
   }
+  __syncthreads();
   extern __shared__ uint2 s_stack[];  // L.short_stack entries per thread, blockDim.x apart
   uint2* const my_stack = s_stack + threadIdx.x;
   const unsigned lane = threadIdx.x & 31u;
@@ -854,15 +856,18 @@ __global__ void __launch_bounds__(256) render_kernel(const RenderLaunch L) {
     }
   }
 
-  // Per-launch counters: one atomic per warp.
+  // Per-launch counters: summed per warp, then per block in shared memory, then one global atomic
+  // per block and counter.
   const unsigned long long tp = __reduce_add_sync(0xffffffffu, n_paths);
   const unsigned long long te = __reduce_add_sync(0xffffffffu, n_ext);
   const unsigned long long ts = __reduce_add_sync(0xffffffffu, n_shadow);
   if (lane == 0) {
-    atomicAdd(L.counters + 0, tp);
-    atomicAdd(L.counters + 1, te);
-    atomicAdd(L.counters + 2, ts);
+    atomicAdd(&s_count[0], tp);
+    atomicAdd(&s_count[1], te);
+    atomicAdd(&s_count[2], ts);
   }
+  __syncthreads();
+  if (threadIdx.x < 3 && s_count[threadIdx.x] != 0ull) atomicAdd(L.counters + threadIdx.x, s_count[threadIdx.x]);
 }
 
 static size_t stack_smem(int short_stack, int block_size) {
