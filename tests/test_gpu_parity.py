@@ -192,6 +192,17 @@ def test_image_statistical_parity_sky_dielectric_metal(renderer):
     statistical_parity(renderer, s)
 
 
+def test_image_statistical_parity_window_room(renderer):
+    # The learned-guiding workload's plain estimator: a closed room lit only through a small window,
+    # diffuse and metal clutter (long paths, environment NEE through an opening). The sky has no
+    # sun here: with it, a 256-spp mean of this room moves by 3% between seeds and by 19% between
+    # 256 and 4,096 spp (rare sun paths), which no mean comparison at these counts can bound. The
+    # oracle takes 1,024 spp, so its image mean varies about 1%.
+    env = configs.sky_environment(width=256, height=128, sun_radiance=0.0)
+    s = configs.room_with_window(width=48, height=27, samples=64, clutter=1024, environment=env)
+    statistical_parity(renderer, s, cpu_spp=1024)
+
+
 def test_progressive_accumulation_contract(renderer):
     s = configs.mixed(width=32, height=18, samples=8)
     renderer.upload(scene_to_gpu(s))
