@@ -11,7 +11,8 @@
  *     the message. The same checks that toaster-gpu performs with anyhow::ensure! are made here
  *     and reported as TC_ERR_INVALID.
  *   - Host pointers are copied; the library owns every device buffer and one CUDA stream per
- *     context. Calls are synchronous unless their name ends in _async. One context per thread.
+ *     context. Calls are synchronous unless their name ends in _async, and except
+ *     tc_render_no_alloc, which only enqueues its work. One context per thread.
  *   - There is no CPU fallback: without a usable sm_100 GPU, tc_create fails.
  */
 #ifndef TOASTER_CUDA_H
@@ -306,22 +307,30 @@ int tc_encode_jpeg(tc_context* ctx, uint32_t quality, float exposure_stops, uint
  * consume frames on the device. No reference counterpart. */
 int tc_display_rgba8_async(tc_context* ctx, float exposure_stops, void* d_rgba, size_t n_bytes, void* stream);
 
-/* Same traversal and estimator as tc_render, for callers that cannot allocate device memory at
- * render time: hosts whose device memory belongs to their own pool or framework allocator (a
- * cudaMalloc beside it is invisible to that allocator's accounting and can fail once the pool
- * has reserved the rest of HBM), and embedders running under a fixed device-memory budget that
- * must be known before the first frame. No reference counterpart (toaster-gpu allocates all its
- * buffers through wgpu).
- * It allocates nothing. The scene comes from an earlier tc_upload_scene; the caller supplies the
- * FP64 per-pixel sums: `sums` is device memory of at least 3*width*height doubles (n_doubles).
- * accumulated_samples == 0 clears it first, otherwise the batch is added to it. The image is
- * sums / (total samples), which the caller tracks. The kernel's scratch (work counter and
- * counters) is a 256-byte static device array holding at most 32 words; this call uses 4, at any
- * image size. It is shared by every call: calls whose work overlaps on the GPU race, so
- * serialise them (one stream, or wait between calls). The first call on a device looks up that
- * array's address once (cudaGetSymbolAddress). The work is enqueued on `stream` (NULL = the
- * context's stream) and not synchronised. Rejects frames above 2^31 pixels and sums buffers
- * smaller than 3*width*height doubles. */
+/* Same traversal and estimator as tc_render, for callers that must not have the library allocate
+ * device memory at render time: hosts whose device memory all belongs to their own pool or
+ * framework allocator (a cudaMalloc beside the pool is invisible to its accounting and fails once
+ * the pool has reserved the rest of HBM), and embedders that run under a fixed device-memory
+ * budget which has to be known before the first frame. No reference counterpart (toaster-gpu
+ * allocates all its buffers through wgpu).
+ * It calls no cudaMalloc, cudaFree or other allocating routine. The scene comes from an earlier
+ * tc_upload_scene; the caller supplies the FP64 per-pixel sums: `sums` is device memory of at
+ * least 3*width*height doubles (n_doubles). accumulated_samples == 0 clears it first, otherwise
+ * the batch is added to it. The image is sums / (total samples), which the caller tracks.
+ * Scratch: the path kernel's work counter and ray counters live in one 256-byte static device
+ * array of the library (at most 32 64-bit words; this call uses 4 at any image size), which
+ * every GPU that loads the library holds until the process exits. All calls share it and it
+ * keeps the last call's values: each call clears the words it uses before its kernel, and calls
+ * whose work overlaps on the GPU race on it, so serialise them (one stream, or wait between
+ * calls). Set-up: the first call on each context looks up the array's device address in that
+ * context's CUDA context (cudaGetSymbolAddress, with the context's device current) and keeps it
+ * with the context; make that first call before any stream capture. A context does not survive
+ * a cudaDeviceReset (none of its buffers do); create a new one afterwards.
+ * Ordering: the work is enqueued on `stream` (NULL = the context's stream) and not
+ * synchronised, and it reads the context's scene buffers. Synchronise `stream` before the next
+ * call that changes the context (tc_upload_scene, tc_update_geometry, tc_set_camera,
+ * tc_destroy and the like) or reads `sums` on the host.
+ * Rejects frames above 2^31 pixels and sums buffers smaller than 3*width*height doubles. */
 int tc_render_no_alloc(tc_context* ctx, const tc_gpu_render_params* params, double* sums, size_t n_doubles,
                        void* stream);
 
@@ -390,6 +399,15 @@ int tc_guide_recorded_samples(tc_context* ctx, float* out, size_t n_floats, uint
  * (mn_major = 0) or MN-major (1) operands, FP32 accumulation in tensor memory. d receives
  * 128 x n floats. 16 <= n <= 128 and 16 <= k <= 80, both multiples of 16. */
 int tc_umma_selftest(const uint16_t* a, const uint16_t* b, float* d, int n, int k, int a_mn_major, int b_mn_major);
+
+/* Cache read-bandwidth probe (no reference counterpart; measurement only): every SM streams a
+ * zero-filled device buffer of `bytes` (>= 1 MiB, allocated and freed by the call) `passes` times
+ * with 16-byte loads that bypass L1, after one untimed pass. A buffer smaller than L2 (126 MB on
+ * B200) gives the L2 read bandwidth, a larger one HBM. *gb_per_s receives the rate (CUDA events).
+ * The path kernel's roofline on L2-resident scenes is quoted against this figure. Errors are
+ * reported by tc_probe_last_error. */
+int tc_probe_cache_read(int device_ordinal, size_t bytes, int passes, double* gb_per_s);
+const char* tc_probe_last_error(void);
 
 /* Host-only helpers (no GPU needed) -------------------------------------------------------- */
 

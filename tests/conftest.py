@@ -9,6 +9,14 @@ if str(ROOT) not in sys.path:
     sys.path.insert(0, str(ROOT))
 
 
+def reference_checkout():
+    """The reference's checkout, for the CPU tests that compare against its scene files: the
+    directory named by TOASTER_REFERENCE, else a `reference` directory beside this repository.
+    The tests that use it skip when neither exists."""
+    env = os.environ.get("TOASTER_REFERENCE")
+    return Path(env) if env else ROOT.parent / "reference"
+
+
 def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a B200 (sm_100) GPU and the built CUDA library")
 

@@ -5,15 +5,13 @@ present, and they load through the native loader with the geometry counts the re
 test expects (crates/toaster-scene/src/loader.rs:1891-1916).
 """
 
-import os
-from pathlib import Path
-
 import pytest
+from conftest import reference_checkout
 
 from toaster_b200.bench_fixtures import SCENES, write_suite
 from toaster_b200.scene import load_scene_gpu
 
-REFERENCE = Path(os.environ.get("TOASTER_REFERENCE", "/root/reference"))
+REFERENCE = reference_checkout()
 COUNTS = [(128, 1, False), (2048, 1, False), (8192, 1, False), (2, 65, False), (2, 513, False), (2048, 129, False),
           (0, 4, True)]
 

@@ -19,6 +19,7 @@ from pathlib import Path
 
 import numpy as np
 import pytest
+from conftest import reference_checkout
 
 from toaster_b200 import gpu_types as gt
 from toaster_b200.native import TcError
@@ -26,7 +27,7 @@ from toaster_b200.scene import load_scene, load_scene_gpu, scene_to_gpu
 
 FIELDS = ["params", "camera", "spheres", "triangles", "triangle_attributes", "materials", "lights",
           "environment_pixels", "texture_pixels"]
-REFERENCE_SCENES = Path(os.environ.get("TOASTER_REFERENCE", "/root/reference")) / "scenes"
+REFERENCE_SCENES = reference_checkout() / "scenes"
 
 
 def both(path):

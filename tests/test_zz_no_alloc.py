@@ -1,10 +1,11 @@
-"""tc_render_no_alloc: the render entry point for callers that cannot allocate device memory.
+"""tc_render_no_alloc: the render entry point for callers that cannot let the library allocate.
 
-Such callers (code inside CUDA stream capture, hosts whose device memory belongs to their own
-pool or framework allocator) pass the output buffer themselves; the library's scratch lives in a
-static device array. The sums it produces must equal those of tc_render + tc_readback_sums for
-the same scene, parameters and seeds, on two consecutive calls (the second call proves the shared
-scratch is cleared between calls).
+Hosts whose device memory all belongs to their own pool or framework allocator, or that run under
+a fixed device-memory budget, cannot have a cudaMalloc made behind their allocator's back at render
+time. They pass the output buffer themselves; the library's scratch lives in a static device
+array. The sums it produces must equal those of tc_render + tc_readback_sums for the same scene,
+parameters and seeds, on two consecutive calls (the second call shows that the shared scratch,
+which keeps the first call's counters, is cleared between calls).
 """
 
 import ctypes

@@ -3,8 +3,8 @@
     python -m toaster_b200.build
 
 produces ``toaster_b200/lib/libtoaster_cuda.so`` (loaded through ctypes) and
-``toaster_b200/lib/libtoaster_cuda.a`` (for a native host such as the Rust crate described in
-INTEGRATION.md). Host C++ is compiled with -ffp-contract=off: the hierarchy bounds must round
+``toaster_b200/lib/libtoaster_cuda.a`` (for a native host such as the Rust crate
+``toaster-cuda``). Host C++ is compiled with -ffp-contract=off: the hierarchy bounds must round
 exactly like the reference's f32 arithmetic.
 """
 
@@ -20,6 +20,7 @@ PKG = Path(__file__).resolve().parent
 CSRC = PKG / "csrc"
 LIB = PKG / "lib"
 SOURCES = ["api.cu", "kernels.cu", "guide.cu", "umma_selftest.cu", "display.cu", "refit.cu", "bvh_device.cu",
+           "probe.cu",
            "bvh_build.cpp", "scene_loader.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

@@ -125,6 +125,10 @@ struct tc_context {
   bool has_records = false;
 
   tc_stats stats{};
+
+  // tc_render_no_alloc: device address of the library's static scratch array in this context's
+  // CUDA context, looked up by the first such call on the context.
+  unsigned long long* static_scratch = nullptr;
 };
 
 namespace {
@@ -1260,8 +1264,8 @@ int tc_render_no_alloc(tc_context* ctx, const tc_gpu_render_params* p, double* s
     return fail(ctx, TC_ERR_INVALID, "sums buffer holds " + std::to_string(n_doubles) + " doubles; " +
                                          std::to_string(3 * npix) + " (3 per pixel) are needed");
   TC_CUDA(ctx, cudaSetDevice(ctx->device));
-  unsigned long long* scratch = nullptr;
-  TC_CUDA(ctx, tcb::render_static_scratch(ctx->device, &scratch));
+  if (!ctx->static_scratch) TC_CUDA(ctx, tcb::render_static_scratch(ctx->device, &ctx->static_scratch));
+  unsigned long long* scratch = ctx->static_scratch;
   static_assert(tcb::kStaticScratchWords >= 4, "the render scratch needs 4 words");
   cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : ctx->stream;
   if (p->accumulated_samples == 0) TC_CUDA(ctx, cudaMemsetAsync(sums, 0, sizeof(double) * 3 * npix, st));
@@ -1285,7 +1289,10 @@ int tc_render_no_alloc(tc_context* ctx, const tc_gpu_render_params* p, double* s
   const int block = 128;
   const int per_sm = tcb::render_max_blocks_per_sm(block, false);
   if (per_sm <= 0) return fail(ctx, TC_ERR_CUDA, "render kernel cannot be resident with this block size");
-  TC_CUDA(ctx, tcb::launch_render(L, block, per_sm * ctx->sm_count, false, st));
+  // Like tc_render: a frame with fewer work items than the resident grid needs fewer blocks.
+  const uint64_t grid = std::max<uint64_t>(
+      1, std::min<uint64_t>(uint64_t(per_sm) * ctx->sm_count, (L.total_items + block - 1) / block));
+  TC_CUDA(ctx, tcb::launch_render(L, block, int(grid), false, st));
   return TC_OK;
 }
 

@@ -109,8 +109,9 @@ int render_batch_max_blocks_per_sm(int block_size, int short_stack = 0);
 cudaError_t launch_guide_samples(const float4* records, const uint32_t* record_count, uint32_t capacity,
                                  const float4* path_radiance, float4* samples, uint32_t* sample_count,
                                  float* weight_sum, cudaStream_t stream);
-// Device address of the library's static render scratch (kStaticScratchWords 64-bit words) on
-// `device`, which must be the current device; looked up once per device.
+// Device address of the library's static render scratch (kStaticScratchWords 64-bit words) in
+// the CUDA context current on `device`, which must be the current device. The caller keeps it
+// with the other resources of that context.
 constexpr int kStaticScratchWords = 32;
 cudaError_t render_static_scratch(int device, unsigned long long** out);
 cudaError_t launch_resolve(const double* accum, uint32_t pixels, double inv_samples, float4* out,

@@ -17,8 +17,6 @@
 #include <math_constants.h>
 #include <stdint.h>
 
-#include <mutex>
-
 #include "device_scene.h"
 #include "traverse.cuh"
 
@@ -999,24 +997,19 @@ cudaError_t launch_guide_samples(const float4* records, const uint32_t* record_c
 static __device__ __align__(256) unsigned long long g_render_scratch[kStaticScratchWords];
 
 cudaError_t render_static_scratch(int device, unsigned long long** out) {
-  // The symbol's device address is looked up once per device, with that device current (host
-  // code must never hand the array's name itself to a kernel: it is only a host-side stand-in).
-  constexpr int kMaxDevices = 64;
-  static std::mutex lock;
-  static unsigned long long* cache[kMaxDevices] = {};
-  if (device < 0 || device >= kMaxDevices) return cudaErrorInvalidDevice;
-  std::lock_guard<std::mutex> guard(lock);
-  if (!cache[device]) {
-    int current = 0;
-    cudaError_t e = cudaGetDevice(&current);
-    if (e != cudaSuccess) return e;
-    if (current != device) return cudaErrorInvalidDevice;
-    void* ptr = nullptr;
-    e = cudaGetSymbolAddress(&ptr, g_render_scratch);
-    if (e != cudaSuccess) return e;
-    cache[device] = static_cast<unsigned long long*>(ptr);
-  }
-  *out = cache[device];
+  // Host code must never hand the array's name itself to a kernel: it is only a host-side
+  // stand-in. The device address belongs to the CUDA context current now (the one the library
+  // module was loaded into), so it is looked up with `device` current and kept by the caller
+  // beside the other resources of that context rather than in a process-wide table, which a
+  // cudaDeviceReset or a host's own driver context would leave pointing at freed memory.
+  int current = 0;
+  cudaError_t e = cudaGetDevice(&current);
+  if (e != cudaSuccess) return e;
+  if (current != device) return cudaErrorInvalidDevice;
+  void* ptr = nullptr;
+  e = cudaGetSymbolAddress(&ptr, g_render_scratch);
+  if (e != cudaSuccess) return e;
+  *out = static_cast<unsigned long long*>(ptr);
   return cudaSuccess;
 }
 

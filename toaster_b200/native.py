@@ -45,6 +45,8 @@ EXPORTED_SYMBOLS = (
     "tc_build_bvh_host",
     "tc_record_sizes",
     "tc_umma_selftest",
+    "tc_probe_cache_read",
+    "tc_probe_last_error",
     "tc_guide_set_params",
     "tc_guide_get_params",
     "tc_guide_infer",
@@ -176,6 +178,8 @@ def load_library(path: os.PathLike | None = None) -> ctypes.CDLL:
     lib.tc_build_bvh_host.restype = ctypes.c_long
     lib.tc_record_sizes.argtypes = [ctypes.POINTER(u32), sz]
     lib.tc_umma_selftest.argtypes = [vp, vp, vp, i32, i32, i32, i32]
+    lib.tc_probe_cache_read.argtypes = [i32, sz, i32, ctypes.POINTER(ctypes.c_double)]
+    lib.tc_probe_last_error.restype = ctypes.c_char_p
     lib.tc_guide_set_params.argtypes = [vp, vp, vp]
     lib.tc_guide_get_params.argtypes = [vp, vp]
     lib.tc_guide_infer.argtypes = [vp, vp, sz, vp]
@@ -244,6 +248,17 @@ def umma_selftest(a: np.ndarray, b: np.ndarray, a_mn_major: bool = False, b_mn_m
     check(lib, None, lib.tc_umma_selftest(a.ctypes.data, b.ctypes.data, d.ctypes.data, n, k, int(a_mn_major),
                                           int(b_mn_major)))
     return d
+
+
+def probe_cache_read(device: int = 0, nbytes: int = 64 << 20, passes: int = 50) -> float:
+    """Read bandwidth in GB/s of a device buffer of `nbytes` streamed by every SM with loads that
+    bypass L1: L2 bandwidth for buffers smaller than L2, HBM for larger ones."""
+    lib = load_library()
+    out = ctypes.c_double(0.0)
+    code = lib.tc_probe_cache_read(device, nbytes, passes, ctypes.byref(out))
+    if code != 0:
+        raise TcError(code, lib.tc_probe_last_error().decode())
+    return out.value
 
 
 class LoadedScene:
