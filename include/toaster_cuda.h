@@ -143,7 +143,8 @@ typedef struct tc_render_options {
   uint32_t guide_record;     /* 1: record (position, normal, direction, incident radiance) training
                                 samples at every diffuse scatter of this batch and at every
                                 environment shadow ray that reaches the sky (plain sampling) */
-  uint32_t wave_paths;       /* guided wavefront width: paths in flight per wave; 0 = 2^23 */
+  uint32_t wave_paths;       /* paths in flight: guided wavefront (0 = 2^23) or plain wavefront
+                                schedule (0 = 2^21) */
   uint32_t short_stack;      /* traversal stack entries per thread held in shared memory (0..16;
                                 deeper entries live in local memory); 0 = none */
   uint32_t refill_lanes;     /* a warp pauses traversal to refill finished lanes once fewer than
@@ -154,7 +155,17 @@ typedef struct tc_render_options {
   float guide_fraction;      /* guided renders: probability of sampling the network's mixture at a
                                 diffuse vertex (one-sample MIS with cosine sampling, the mixture pdf
                                 (1 - f) cos/pi + f q); in [0, 1), 0 = default 0.5 */
+  uint32_t schedule;         /* plain renders: TC_SCHEDULE_AUTO (0) = the wavefront for tc_render and
+                                tc_autotune calls of at least 2^20 paths and 1 or more bounces, the
+                                megakernel otherwise; TC_SCHEDULE_MEGAKERNEL (1) = one persistent
+                                path kernel; TC_SCHEDULE_WAVEFRONT (2) = per-path state in device
+                                memory and three launches per bounce (logic, material-sorted
+                                shading, tracing with one ray kind per warp), wave_paths slots
+                                (0 = 2^21). Captured animation frames use the megakernel. */
 } tc_render_options;
+#define TC_SCHEDULE_AUTO 0u
+#define TC_SCHEDULE_MEGAKERNEL 1u
+#define TC_SCHEDULE_WAVEFRONT 2u
 
 /* Counters of the most recent tc_render / tc_trace_* call. */
 typedef struct tc_stats {
@@ -187,6 +198,21 @@ int tc_set_stream(tc_context* ctx, void* stream);
 /* Replaces create_scene_gpu_buffers + the queue.write_buffer uploads
  * (crates/toaster-gpu/src/buffers.rs:117-271, path_tracer.rs:676-721). */
 int tc_upload_scene(tc_context* ctx, const tc_scene_data* scene);
+
+/* Triangle test of the scenes uploaded after this call (no reference counterpart: the reference
+ * uses Moller-Trumbore only, crates/toaster-cpu/src/intersect.rs:87-120):
+ *   TC_TRIANGLE_MOLLER_TRUMBORE (0, default)  the reference's test, operation for operation: the
+ *                                             parity mode, bit-exact closest hits;
+ *   TC_TRIANGLE_WATERTIGHT (1)                the FP32 watertight test of Woop, Benthin and Wald
+ *                                             (JCGT 2013): no ray slips between triangles that share
+ *                                             an edge; hit distances round differently, so ties and
+ *                                             near-ties may pick another primitive than the reference.
+ * The watertight test keeps a second copy of the triangle vertices in leaf order (48 B per
+ * primitive) and is traced by tc_trace_closest and by plain renders on the wavefront schedule;
+ * other render calls on such a scene fail with TC_ERR_INVALID. */
+#define TC_TRIANGLE_MOLLER_TRUMBORE 0
+#define TC_TRIANGLE_WATERTIGHT 1
+int tc_set_triangle_test(tc_context* ctx, int test);
 
 /* Where tc_upload_scene builds the median-split hierarchy when the scene brings none: 0 = on the
  * device for scenes of at least 4,096 primitives, on the host below (default); 1 = always on the

@@ -36,6 +36,13 @@ namespace {
 
 // Default dynamic-fetch threshold of the path kernel (tc_render_options.refill_lanes).
 constexpr int kDefaultRefillLanes = 1;
+// Plain wavefront schedule: default path slots, and the smallest frame (in paths) that the
+// automatic schedule gives it (smaller frames run in less time than its per-bounce launches cost).
+constexpr uint32_t kWavefrontSlots = 1u << 21;
+constexpr uint64_t kWavefrontMinPaths = 1ull << 20;
+// Iterations the host runs ahead of the live-slot count it waits for (kWfRing = kWfLag + 1).
+constexpr int kWfLag = 4;
+constexpr int kWfRing = kWfLag + 1;
 // Scenes with at least this many primitives build their hierarchy on the device by default.
 constexpr size_t kDeviceBuildMin = 4096;
 
@@ -118,7 +125,7 @@ struct tc_context {
   tcb::GuideDevice guide;
   DevBuf g_params, g_m, g_v, g_grad, g_images, g_biases, g_status, g_in, g_out;
   // Guided wavefront buffers (two state buffers, queries, decoded mixtures, round counters).
-  DevBuf w_state_a, w_state_b, w_query, w_mix, w_counts;
+  DevBuf w_state_a, w_state_b, w_query, w_mix, w_counts, w_prefix;
   // Recorded training data of the last guide_record batch.
   DevBuf rec_records, rec_count, rec_path_rad, rec_samples, rec_wsum;
   uint32_t rec_capacity = 0;
@@ -129,6 +136,18 @@ struct tc_context {
   // tc_render_no_alloc: device address of the library's static scratch array in this context's
   // CUDA context, looked up by the first such call on the context.
   unsigned long long* static_scratch = nullptr;
+
+  // Plain wavefront schedule: per-path state and queues for wf_capacity slots, and a pinned
+  // ring of live-slot counts with one event per entry (the host's drain check).
+  uint32_t wf_capacity = 0;
+  DevBuf wf_state, wf_ray_o, wf_ray_d, wf_thr, wf_rad, wf_rng, wf_hit, wf_nee, wf_shadow_q, wf_ext_q, wf_mat_q, wf_q;
+  uint32_t* wf_live_host = nullptr;
+  cudaEvent_t wf_events[kWfRing] = {};
+
+  // Triangle test of the next upload (tc_set_triangle_test) and, for the watertight test, the
+  // vertex records of the uploaded scene in leaf order.
+  int triangle_test = TC_TRIANGLE_MOLLER_TRUMBORE;
+  DevBuf tri_verts;
 };
 
 namespace {
@@ -424,6 +443,9 @@ int tc_destroy(tc_context* ctx) {
   if (ctx->ev_kernel0) cudaEventDestroy(ctx->ev_kernel0);
   if (ctx->ev_kernel1) cudaEventDestroy(ctx->ev_kernel1);
   if (ctx->ev_end) cudaEventDestroy(ctx->ev_end);
+  for (cudaEvent_t e : ctx->wf_events)
+    if (e) cudaEventDestroy(e);
+  if (ctx->wf_live_host) cudaFreeHost(ctx->wf_live_host);
   if (ctx->jpeg_params) nvjpegEncoderParamsDestroy(ctx->jpeg_params);
   if (ctx->jpeg_state) nvjpegEncoderStateDestroy(ctx->jpeg_state);
   if (ctx->jpeg) nvjpegDestroy(ctx->jpeg);
@@ -621,6 +643,15 @@ int tc_upload_scene(tc_context* ctx, const tc_scene_data* sd) {
     s.cam_horizontal[c] = sd->camera.horizontal[c];
     s.cam_vertical[c] = sd->camera.vertical[c];
   }
+  const bool raw_tris_on_device = built && on_device;
+  if (ctx->triangle_test == TC_TRIANGLE_WATERTIGHT && sd->triangle_count) {
+    // Vertex records for the watertight test, gathered in leaf order from the scene's triangles.
+    if (!raw_tris_on_device) TC_CUDA(ctx, upload(ctx->raw_triangles, sd->triangles, sd->triangle_count, st));
+    TC_CUDA(ctx, ctx->tri_verts.reserve(3 * sizeof(float4) * size_t(prim_count)));
+    TC_CUDA(ctx, tcb::launch_triangle_vertices(ctx->prims.as<tcb::PrimRecord>(), prim_count, ctx->raw_triangles.ptr,
+                                               ctx->tri_verts.as<float4>(), st));
+    s.tri_verts = ctx->tri_verts.as<float4>();
+  }
   TC_CUDA(ctx, cudaStreamSynchronize(st));
   ctx->has_scene = true;
   ctx->sphere_count = uint32_t(sd->sphere_count);
@@ -633,7 +664,16 @@ int tc_upload_scene(tc_context* ctx, const tc_scene_data* sd) {
   ctx->any_attr = any_attr;
   ctx->pair_count = pair_count;
   ctx->device_built = built && on_device;
-  ctx->raw_spheres_valid = ctx->raw_triangles_valid = ctx->device_built;
+  ctx->raw_spheres_valid = ctx->device_built;
+  ctx->raw_triangles_valid = ctx->device_built || ctx->scene.tri_verts != nullptr;
+  return TC_OK;
+}
+
+int tc_set_triangle_test(tc_context* ctx, int test) {
+  if (!ctx) return fail(nullptr, TC_ERR_INVALID, "context is null");
+  if (test != TC_TRIANGLE_MOLLER_TRUMBORE && test != TC_TRIANGLE_WATERTIGHT)
+    return fail(ctx, TC_ERR_INVALID, "triangle test must be 0 (Moller-Trumbore) or 1 (watertight)");
+  ctx->triangle_test = test;
   return TC_OK;
 }
 
@@ -682,6 +722,9 @@ int tc_update_geometry(tc_context* ctx, const tc_scene_data* sd, const tc_scene_
     TC_CUDA(ctx, tcb::launch_refit(plan, ctx->pairs.as<tcb::PairNode>(), ctx->root_buf.as<tcb::ChildRec>(),
                                    ctx->prims.as<tcb::PrimRecord>(), ctx->bvh_prims,
                                    ctx->raw_spheres.as<tc_gpu_sphere>(), ctx->raw_triangles.as<tc_gpu_triangle>(), st));
+    if (ctx->scene.tri_verts && changes->triangles)
+      TC_CUDA(ctx, tcb::launch_triangle_vertices(ctx->prims.as<tcb::PrimRecord>(), ctx->bvh_prims,
+                                                 ctx->raw_triangles.ptr, ctx->tri_verts.as<float4>(), st));
   }
   if (changes->emissive_geometry && !lights.empty())
     TC_CUDA(ctx, upload(ctx->lights, lights.data(), lights.size(), st));
@@ -707,6 +750,73 @@ int tc_set_camera(tc_context* ctx, const tc_gpu_camera* cam) {
     ctx->scene.cam_lower_left[c] = cam->lower_left_corner[c];
     ctx->scene.cam_horizontal[c] = cam->horizontal[c];
     ctx->scene.cam_vertical[c] = cam->vertical[c];
+  }
+  return TC_OK;
+}
+
+// Plain render as a wavefront (tcb::WavefrontLaunch): iterations of logic, shade and trace
+// launches until no slot holds a path and no work is left. The host waits, kWfLag iterations
+// behind the last one it enqueued, for the live-slot count of an earlier iteration, so the GPU
+// always has queued work; the iterations launched after the last path finished find nothing to do.
+static int run_wavefront(tc_context* ctx, const tcb::RenderLaunch& L, uint32_t slots, uint32_t max_bounces,
+                         int refill_lanes, bool moments, cudaStream_t st) {
+  const uint64_t items = L.total_items;
+  const uint32_t cap = uint32_t(std::max<uint64_t>(32, std::min<uint64_t>(slots, items)));
+  if (cap != ctx->wf_capacity) {
+    ctx->wf_capacity = 0;
+    const size_t n = cap;
+    TC_CUDA(ctx, ctx->wf_state.reserve(sizeof(uint32_t) * n));
+    TC_CUDA(ctx, ctx->wf_ray_o.reserve(sizeof(float4) * n));
+    TC_CUDA(ctx, ctx->wf_ray_d.reserve(sizeof(float4) * n));
+    TC_CUDA(ctx, ctx->wf_thr.reserve(sizeof(float4) * n));
+    TC_CUDA(ctx, ctx->wf_rad.reserve(sizeof(float4) * n));
+    TC_CUDA(ctx, ctx->wf_rng.reserve(sizeof(uint4) * n));
+    TC_CUDA(ctx, ctx->wf_hit.reserve(sizeof(uint4) * n));
+    TC_CUDA(ctx, ctx->wf_nee.reserve(2 * sizeof(float4) * n));
+    TC_CUDA(ctx, ctx->wf_shadow_q.reserve(4 * sizeof(float4) * n));  // two shadow rays per slot
+    TC_CUDA(ctx, ctx->wf_ext_q.reserve(sizeof(uint32_t) * n));
+    TC_CUDA(ctx, ctx->wf_mat_q.reserve(3 * sizeof(uint32_t) * n));
+    TC_CUDA(ctx, ctx->wf_q.reserve(sizeof(uint32_t) * tcb::kWfCounters));
+    ctx->wf_capacity = cap;
+  }
+  if (!ctx->wf_live_host) {
+    TC_CUDA(ctx, cudaHostAlloc(reinterpret_cast<void**>(&ctx->wf_live_host), sizeof(uint32_t) * kWfRing,
+                               cudaHostAllocDefault));
+    for (cudaEvent_t& e : ctx->wf_events) TC_CUDA(ctx, cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  }
+  tcb::WavefrontLaunch w{};
+  w.r = L;
+  w.capacity = cap;
+  w.state = ctx->wf_state.as<uint32_t>();
+  w.ray_o = ctx->wf_ray_o.as<float4>();
+  w.ray_d = ctx->wf_ray_d.as<float4>();
+  w.thr = ctx->wf_thr.as<float4>();
+  w.rad = ctx->wf_rad.as<float4>();
+  w.rng = ctx->wf_rng.as<uint4>();
+  w.hit = ctx->wf_hit.as<uint4>();
+  w.nee = ctx->wf_nee.as<float4>();
+  w.shadow_q = ctx->wf_shadow_q.as<float4>();
+  w.ext_q = ctx->wf_ext_q.as<uint32_t>();
+  w.mat_q = ctx->wf_mat_q.as<uint32_t>();
+  w.q = ctx->wf_q.as<uint32_t>();
+  w.refill_lanes = refill_lanes;
+  TC_CUDA(ctx, cudaMemsetAsync(w.state, 0, sizeof(uint32_t) * cap, st));
+  // Every iteration advances each live path by one vertex and refills every free slot, so the
+  // frame drains in at most (waves + 1) x (bounces + 2) iterations; the bound only guards the loop.
+  const uint64_t bound = 2 * ((items + cap - 1) / cap + 1) * (uint64_t(max_bounces) + 2) + 2 * kWfRing;
+  for (uint64_t it = 0;; ++it) {
+    if (it > bound) return fail(ctx, TC_ERR_DEVICE_STATUS, "wavefront render did not drain its paths");
+    TC_CUDA(ctx, cudaMemsetAsync(w.q, 0, sizeof(uint32_t) * tcb::kWfCounters, st));
+    TC_CUDA(ctx, tcb::launch_wavefront_iteration(w, moments, ctx->sm_count, st));
+    const int k = int(it % kWfRing);
+    TC_CUDA(ctx, cudaMemcpyAsync(ctx->wf_live_host + k, w.q + tcb::kWfLive, sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                                 st));
+    TC_CUDA(ctx, cudaEventRecord(ctx->wf_events[k], st));
+    if (it >= uint64_t(kWfLag)) {
+      const int j = int((it - kWfLag) % kWfRing);
+      TC_CUDA(ctx, cudaEventSynchronize(ctx->wf_events[j]));
+      if (ctx->wf_live_host[j] == 0) break;
+    }
   }
   return TC_OK;
 }
@@ -777,8 +887,25 @@ static int enqueue_render(tc_context* ctx, const tc_gpu_render_params* p, const 
     L.g.record_capacity = ctx->rec_capacity;
     L.g.path_radiance = ctx->rec_path_rad.as<float4>();
   }
+  // Plain renders called directly (not captured into a graph) may run as a wavefront.
+  const bool direct = !camera_dev && !frame_index_dev;
+  if (o.schedule > TC_SCHEDULE_WAVEFRONT) return fail(ctx, TC_ERR_INVALID, "schedule must be 0 (auto), 1 or 2");
+  if (o.schedule == TC_SCHEDULE_WAVEFRONT && mode == tcb::kModePlain && !direct)
+    return fail(ctx, TC_ERR_INVALID, "the wavefront schedule renders direct calls only, not captured frames");
+  const bool wavefront =
+      mode == tcb::kModePlain && direct && p->max_bounces > 0 && p->max_bounces <= tcb::kWfDepthMask &&
+      (o.schedule == TC_SCHEDULE_WAVEFRONT ||
+       (o.schedule == TC_SCHEDULE_AUTO && uint64_t(npix) * p->samples >= kWavefrontMinPaths));
+  if (ctx->scene.tri_verts && !wavefront)
+    return fail(ctx, TC_ERR_INVALID,
+                "the watertight triangle test is traced by tc_trace_closest and by plain wavefront renders only");
   if (timing) TC_CUDA(ctx, cudaEventRecord(ctx->ev_kernel0, st));
-  if (mode != tcb::kModeGuided) {
+  if (wavefront) {
+    L.total_items = uint64_t(npix) * p->samples;  // one path per work item
+    if (int rc = run_wavefront(ctx, L, o.wave_paths ? o.wave_paths : kWavefrontSlots, p->max_bounces,
+                               int(o.refill_lanes), moments, st))
+      return rc;
+  } else if (mode != tcb::kModeGuided) {
     TC_CUDA(ctx, tcb::launch_render(L, block, grid, moments, st, mode));
   } else {
     // Wavefront: waves of whole samples per pixel; within a wave, rounds of (path kernel ->
@@ -872,8 +999,10 @@ int tc_render_batch(tc_context* const* contexts, const tc_gpu_render_params* par
   if (!lead) return fail(nullptr, TC_ERR_INVALID, "context 0 of the batch is null");
   tc_render_options o{};
   if (opt) o = *opt;
-  if (o.keep_moments || o.guiding || o.guide_record)
-    return fail(lead, TC_ERR_INVALID, "batched frames are plain renders (no moments, guiding or recording)");
+  if (o.keep_moments || o.guide_record)
+    return fail(lead, TC_ERR_INVALID, "batched frames do not keep moments or record training samples");
+  if (o.guiding && !(o.guide_fraction >= 0.0f && o.guide_fraction < 1.0f))
+    return fail(lead, TC_ERR_INVALID, "guide_fraction must be in [0, 1)");
   const int block = o.block_size ? int(o.block_size) : 128;
   if (block % 32 != 0 || block < 32 || block > 256)
     return fail(lead, TC_ERR_INVALID, "block_size must be a multiple of 32 in [32, 256]");
@@ -883,12 +1012,18 @@ int tc_render_batch(tc_context* const* contexts, const tc_gpu_render_params* par
     tc_context* c = contexts[i];
     if (!c) return fail(lead, TC_ERR_INVALID, "context " + std::to_string(i) + " of the batch is null");
     if (c->device != lead->device) return fail(lead, TC_ERR_INVALID, "batched contexts must share one device");
+    if (c->scene.tri_verts)
+      return fail(lead, TC_ERR_INVALID, "batched frames use the Moller-Trumbore triangle test");
     for (size_t j = 0; j < i; ++j)
       if (contexts[j] == c) return fail(lead, TC_ERR_INVALID, "a context appears twice in the batch");
     if (int rc = check_render_params(c, &params[i])) {
       lead->error = "frame " + std::to_string(i) + ": " + c->error;
       return rc;
     }
+    if (o.guiding && !c->has_guide)
+      return fail(lead, TC_ERR_STATE, "frame " + std::to_string(i) + ": guided rendering needs tc_guide_set_params first");
+    if (o.guiding && params[i].samples != params[0].samples)
+      return fail(lead, TC_ERR_INVALID, "guided batched frames must share one sample count");
   }
   TC_CUDA(lead, cudaSetDevice(lead->device));
   cudaStream_t st = lead->stream;
@@ -923,6 +1058,24 @@ int tc_render_batch(tc_context* const* contexts, const tc_gpu_render_params* par
     items += uint64_t(p->width) * p->height * J.items_per_pixel;
     paths += uint64_t(p->width) * p->height * p->samples;
   }
+  // Guided: waves of whole samples per pixel over all frames; frame i owns the region
+  // [ws * pix_begin_i, ws * (pix_begin_i + pixels_i)) of the wave's suspended-path buffers.
+  uint64_t total_pix = 0;
+  for (size_t i = 0; i < n; ++i) {
+    jobs[i].pix_begin = uint32_t(total_pix);
+    total_pix += uint64_t(params[i].width) * params[i].height;
+  }
+  uint32_t ws = 0, rounds = 0;
+  if (o.guiding) {
+    const uint32_t wave_cap = o.wave_paths ? o.wave_paths : (1u << 23);
+    ws = uint32_t(std::max<uint64_t>(1, std::min<uint64_t>(params[0].samples, wave_cap / total_pix)));
+    if (uint64_t(ws) * total_pix > (1ull << 31)) return fail(lead, TC_ERR_INVALID, "batched guided frames are too large");
+    for (size_t i = 0; i < n; ++i) {
+      jobs[i].wave_offset = ws * jobs[i].pix_begin;
+      jobs[i].wave_capacity = ws * params[i].width * params[i].height;
+      rounds = std::max(rounds, params[i].max_bounces > 1 ? params[i].max_bounces - 1 : 0u);
+    }
+  }
   TC_CUDA(lead, upload(lead->batch_jobs, jobs.data(), jobs.size(), st));
   tcb::RenderLaunch L{};
   L.jobs = lead->batch_jobs.as<tcb::FrameJob>();
@@ -934,10 +1087,63 @@ int tc_render_batch(tc_context* const* contexts, const tc_gpu_render_params* par
   L.min_active = int(o.refill_lanes ? o.refill_lanes : kDefaultRefillLanes);
   TC_CUDA(lead, cudaMemsetAsync(lead->work_counter.ptr, 0, sizeof(unsigned long long), st));
   TC_CUDA(lead, cudaMemsetAsync(lead->counters.ptr, 0, 4 * sizeof(unsigned long long), st));
-  const int per_sm = tcb::render_batch_max_blocks_per_sm(block, L.short_stack);
+  const int per_sm = tcb::render_batch_max_blocks_per_sm(block, o.guiding != 0);
   if (per_sm <= 0) return fail(lead, TC_ERR_CUDA, "batched render kernel cannot be resident with this block size");
+  const int grid = per_sm * lead->sm_count;
   TC_CUDA(lead, cudaEventRecord(lead->ev_kernel0, st));
-  TC_CUDA(lead, tcb::launch_render_batch(L, block, per_sm * lead->sm_count, st));
+  if (!o.guiding) {
+    TC_CUDA(lead, tcb::launch_render_batch(L, block, grid, st));
+  } else {
+    // Rounds of (batched path kernel -> each frame's network infers its frame's queries -> prefix
+    // of the per-frame counts -> batched resume), as the single-frame guided wavefront does.
+    const size_t cap = size_t(ws) * total_pix;
+    TC_CUDA(lead, lead->w_state_a.reserve(sizeof(float4) * 6 * cap));
+    TC_CUDA(lead, lead->w_state_b.reserve(sizeof(float4) * 6 * cap));
+    TC_CUDA(lead, lead->w_query.reserve(sizeof(float4) * 2 * cap));
+    TC_CUDA(lead, lead->w_mix.reserve(sizeof(float4) * tcb::kGuideDecodedF4 * cap));
+    TC_CUDA(lead, lead->w_counts.reserve(sizeof(uint32_t) * (rounds + 1) * n));
+    TC_CUDA(lead, lead->w_prefix.reserve(sizeof(uint32_t) * std::max<size_t>(rounds, 1) * (n + 1)));
+    float4* state_in = lead->w_state_a.as<float4>();
+    float4* state_out = lead->w_state_b.as<float4>();
+    uint32_t* counts = lead->w_counts.as<uint32_t>();
+    uint32_t* prefix = lead->w_prefix.as<uint32_t>();
+    float4* query = lead->w_query.as<float4>();
+    float4* mix = lead->w_mix.as<float4>();
+    L.g.guide_fraction = o.guide_fraction > 0.0f ? o.guide_fraction : 0.5f;
+    L.g.capacity = uint32_t(cap);
+    L.g.out_query = query;
+    for (uint32_t first = 0; first < params[0].samples; first += ws) {
+      const uint32_t wsz = std::min(ws, params[0].samples - first);
+      TC_CUDA(lead, cudaMemsetAsync(counts, 0, sizeof(uint32_t) * (rounds + 1) * n, st));
+      tcb::RenderLaunch R = L;
+      R.total_items = uint64_t(wsz) * total_pix;
+      R.g.wave_first_sample = first;
+      R.g.wave_spp = wsz;
+      R.g.resume = 0;
+      R.g.out_state = state_out;
+      R.g.job_out_count = counts;
+      TC_CUDA(lead, cudaMemsetAsync(lead->work_counter.ptr, 0, sizeof(unsigned long long), st));
+      TC_CUDA(lead, tcb::launch_render_batch(R, block, grid, st, true));
+      for (uint32_t r = 0; r < rounds; ++r) {
+        std::swap(state_in, state_out);
+        for (size_t i = 0; i < n; ++i)
+          TC_CUDA(lead, tcb::guide_launch_infer(contexts[i]->guide, query + 2 * size_t(jobs[i].wave_offset),
+                                                jobs[i].wave_capacity,
+                                                mix + size_t(tcb::kGuideDecodedF4) * jobs[i].wave_offset,
+                                                lead->sm_count, st, counts + size_t(r) * n + i));
+        uint32_t* pre = prefix + size_t(r) * (n + 1);
+        TC_CUDA(lead, tcb::launch_job_prefix(counts + size_t(r) * n, L.jobs, uint32_t(n), pre, st));
+        R.g.resume = 1;
+        R.g.in_state = state_in;
+        R.g.in_job_prefix = pre;
+        R.g.in_mix = mix;
+        R.g.out_state = state_out;
+        R.g.job_out_count = counts + size_t(r + 1) * n;
+        TC_CUDA(lead, cudaMemsetAsync(lead->work_counter.ptr, 0, sizeof(unsigned long long), st));
+        TC_CUDA(lead, tcb::launch_render_batch(R, block, grid, st, true));
+      }
+    }
+  }
   TC_CUDA(lead, cudaEventRecord(lead->ev_kernel1, st));
   unsigned long long counters[4] = {0, 0, 0, 0};
   TC_CUDA(lead, cudaMemcpyAsync(counters, lead->counters.ptr, sizeof(counters), cudaMemcpyDeviceToHost, st));
@@ -1256,6 +1462,7 @@ int tc_render_no_alloc(tc_context* ctx, const tc_gpu_render_params* p, double* s
   if (!ctx) return fail(nullptr, TC_ERR_INVALID, "context is null");
   if (!p || !sums) return fail(ctx, TC_ERR_INVALID, "render params or sums buffer is null");
   if (!ctx->has_scene) return fail(ctx, TC_ERR_STATE, "tc_render_no_alloc before tc_upload_scene");
+  if (ctx->scene.tri_verts) return fail(ctx, TC_ERR_INVALID, "tc_render_no_alloc uses the Moller-Trumbore triangle test");
   if (p->width == 0 || p->height == 0) return fail(ctx, TC_ERR_INVALID, "render dimensions must be nonzero");
   if (p->samples == 0) return fail(ctx, TC_ERR_INVALID, "sample batch must be greater than zero");
   const uint64_t npix = uint64_t(p->width) * p->height;

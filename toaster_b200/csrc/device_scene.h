@@ -33,6 +33,9 @@ struct DevScene {
   uint32_t env_sampleable;   // 1 when the importance distribution has positive mass
   uint32_t background;       // 0 sky, 1 black, 2 environment
   float cam_origin[3], cam_lower_left[3], cam_horizontal[3], cam_vertical[3];
+  // Watertight triangle test (tc_set_triangle_test): the vertices of every leaf-order primitive
+  // record (3 float4, triangles only), or null for the reference's Moller-Trumbore test.
+  const float4* tri_verts;
 };
 
 // Training-data recording and guided wavefront rounds (render modes kRecord / kGuided).
@@ -56,6 +59,10 @@ struct GuideLaunch {
   uint32_t wave_first_sample;
   uint32_t wave_spp;
   float guide_fraction;    // probability of sampling the guide's mixture at a diffuse vertex
+  // Batched guided rounds: suspended paths per frame (n counters) and, when resuming, the
+  // exclusive prefix of the previous round's per-frame counts (n + 1 entries, the total last).
+  uint32_t* job_out_count;
+  const uint32_t* in_job_prefix;
 };
 
 // Path kernel modes.
@@ -78,6 +85,10 @@ struct FrameJob {
   // of the values above, so one captured launch serves every frame.
   const uint32_t* frame_index_dev;
   const float* camera_dev;
+  // Batched guided launches: first pixel of this frame in the concatenation of all frames' pixels,
+  // and the frame's region (offset, capacity) in the wave's suspended-path buffers.
+  uint32_t pix_begin;
+  uint32_t wave_offset, wave_capacity;
 };
 
 struct RenderLaunch {
@@ -92,6 +103,52 @@ struct RenderLaunch {
   GuideLaunch g;
 };
 
+// Wavefront schedule of plain renders: every path in flight owns a slot of per-path state in
+// device memory, and each iteration runs three launches over it:
+//   logic   per slot: adds the shadow-ray results of the last vertex, consumes the last
+//           extension hit (miss -> environment, emissive -> emission, else the slot joins the
+//           queue of its material), finishes paths into the FP64 image sums and starts new
+//           camera paths in free slots (their rays join the extension queue);
+//   shade   per material queue (diffuse, then metal, then dielectric, so a warp shades one
+//           material): next-event shadow rays and the scattered extension ray;
+//   trace   extension rays (closest hit) then shadow rays (first hit), 32 rays of one kind per
+//           warp; a shadow ray that hits something zeroes its contribution.
+// State word per slot: bits 0-23 remaining depth, then the flags below.
+constexpr uint32_t kWfDepthMask = 0x00FFFFFFu;
+constexpr uint32_t kWfAlive = 1u << 24;          // the slot holds a path
+constexpr uint32_t kWfExtPending = 1u << 25;     // its extension ray is queued / traced
+constexpr uint32_t kWfNeePending = 1u << 26;     // its two shadow-ray contributions are to be added
+constexpr uint32_t kWfTerminate = 1u << 27;      // the path ends once its contributions are added
+constexpr uint32_t kWfEmission = 1u << 28;       // emission seen by the extension ray counts
+// Queue counters (uint32 each), cleared before every iteration.
+enum WfCounter : int {
+  kWfExtCount = 0, kWfShadowCount = 1, kWfMatCount = 2,  // [2..4]: diffuse, metal, dielectric
+  kWfLive = 5, kWfTraceCursor = 6, kWfCounters = 8
+};
+
+struct WavefrontLaunch {
+  RenderLaunch r;        // frame (r.f), work counter and launch counters; r.g is unused
+  uint32_t capacity;     // path slots
+  uint32_t* state;       // state word
+  float4* ray_o;         // (ray origin.xyz, solid-angle pdf of the last diffuse bounce or -1)
+  float4* ray_d;         // (ray direction.xyz, -)
+  float4* thr;           // (throughput.xyz, pixel)
+  float4* rad;           // (radiance.xyz, -)
+  uint4* rng;            // PCG32 state and increment
+  uint4* hit;            // (t bits, primitive record or kNoNode, tag, -) of the extension ray
+  float4* nee;           // 2 per slot: light and environment shadow-ray contributions
+  float4* shadow_q;      // 2 per entry: (origin.xyz, tmax), (direction.xyz, target nee index)
+  uint32_t* ext_q;       // slots whose extension ray is to be traced
+  uint32_t* mat_q;       // 3 x capacity: slots to shade, per material kind
+  uint32_t* q;           // kWfCounters counters
+  int refill_lanes;      // > 1: trace lanes refill once fewer than this many of a warp still traverse
+};
+
+// Vertices of every triangle record in leaf order (verts[3k..3k+2]) gathered from the scene-order
+// triangles (tc_gpu_triangle records) through the records' tags.
+cudaError_t launch_triangle_vertices(const PrimRecord* prims, uint32_t n, const void* triangles, float4* verts,
+                                     cudaStream_t stream);
+
 // Launchers implemented in kernels.cu. All enqueue on `stream` and return the launch error.
 cudaError_t launch_trace_closest(const DevScene& s, const float* rays, uint64_t n, float tmin, uint32_t* prim,
                                  float* t, cudaStream_t stream);
@@ -99,9 +156,16 @@ cudaError_t launch_render(const RenderLaunch& r, int block_size, int grid_size, 
                           int mode = kModePlain);
 int render_max_blocks_per_sm(int block_size, bool moments, int mode = kModePlain, int short_stack = 0,
                              int min_active = 1);
-// Batched plain launch over r.jobs (r.job_count frames, items concatenated in job order).
-cudaError_t launch_render_batch(const RenderLaunch& r, int block_size, int grid_size, cudaStream_t stream);
-int render_batch_max_blocks_per_sm(int block_size, int short_stack = 0);
+// One wavefront iteration (logic, shade, trace) on `stream`; the caller clears w.q first.
+cudaError_t launch_wavefront_iteration(const WavefrontLaunch& w, bool moments, int sm_count, cudaStream_t stream);
+// Batched launch over r.jobs (r.job_count frames, items concatenated in job order): plain, or one
+// round of the guided wavefront (r.g, with per-frame regions of the wave buffers).
+cudaError_t launch_render_batch(const RenderLaunch& r, int block_size, int grid_size, cudaStream_t stream,
+                                bool guided = false);
+int render_batch_max_blocks_per_sm(int block_size, bool guided = false);
+// prefix[0..n) = exclusive prefix of min(counts[i], jobs[i].wave_capacity); prefix[n] = total.
+cudaError_t launch_job_prefix(const uint32_t* counts, const FrameJob* jobs, uint32_t n, uint32_t* prefix,
+                              cudaStream_t stream);
 // Training samples (3 float4 each: position + weight, normal, direction) from recorded diffuse
 // scatters: weight = luminance of the radiance that arrived along the scattered direction. Only
 // positive-weight samples are written (compacted, order unspecified); *sample_count (zeroed by

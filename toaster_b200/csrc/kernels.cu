@@ -17,6 +17,8 @@
 #include <math_constants.h>
 #include <stdint.h>
 
+#include <algorithm>
+
 #include "device_scene.h"
 #include "traverse.cuh"
 
@@ -225,9 +227,30 @@ __global__ void trace_closest_kernel(const DevScene s, const float* __restrict__
   const RayQ q = make_ray(r[0], r[1], r[2], r[3], r[4], r[5]);
   TraceResult tr;
   uint32_t visits = 0;
-  const bool hit = trace_ray(s.pairs, s.prims, root, q, tmin, CUDART_INF_F, false, tr, visits);
+  const bool hit = s.tri_verts
+                       ? trace_ray<true>(s.pairs, s.prims, root, q, tmin, CUDART_INF_F, false, tr, visits, s.tri_verts)
+                       : trace_ray(s.pairs, s.prims, root, q, tmin, CUDART_INF_F, false, tr, visits);
   prim[i] = hit ? (tr.tag & ~kTagLast) : 0xFFFFFFFFu;
   tout[i] = hit ? tr.t : CUDART_INF_F;
+}
+
+__global__ void triangle_vertices_kernel(const PrimRecord* __restrict__ prims, uint32_t n,
+                                         const float4* __restrict__ tris, float4* __restrict__ verts) {
+  const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  const uint32_t tag = __float_as_uint(prims[k].a[3]);
+  if (!(tag & kTagTriangle)) return;
+  const float4* t = tris + 4 * size_t(tag & kTagIndexMask);  // tc_gpu_triangle: v0, v1, v2, material
+  verts[3 * size_t(k)] = t[0];
+  verts[3 * size_t(k) + 1] = t[1];
+  verts[3 * size_t(k) + 2] = t[2];
+}
+
+cudaError_t launch_triangle_vertices(const PrimRecord* prims, uint32_t n, const void* triangles, float4* verts,
+                                     cudaStream_t stream) {
+  if (n == 0) return cudaSuccess;
+  triangle_vertices_kernel<<<(n + 255) / 256, 256, 0, stream>>>(prims, n, static_cast<const float4*>(triangles), verts);
+  return cudaGetLastError();
 }
 
 cudaError_t launch_trace_closest(const DevScene& s, const float* rays, uint64_t n, float tmin, uint32_t* prim,
@@ -467,9 +490,26 @@ __device__ __forceinline__ V3 background(const DevScene& s, V3 d, float bsdf_pdf
 }
 
 // Writes a path suspended at a diffuse vertex (guided mode) and the query for its mixture.
+// Batched launches keep one region of the wave buffers per frame (FrameJob::wave_offset), so the
+// frame's own network infers its queries; the frame index travels with the path.
+template <bool kBatch>
 __device__ __forceinline__ void suspend_path(const RenderLaunch& L, const Lane& ln) {
-  const uint32_t slot = aggregated_increment(L.g.out_count);
-  if (slot >= L.g.capacity) return;  // cannot happen: capacity covers every path of the wave
+  uint32_t slot;
+  if constexpr (kBatch) {
+    // One atomic per group of lanes of the same frame.
+    const unsigned group = __match_any_sync(__activemask(), ln.job);
+    const int leader = __ffs(group) - 1;
+    uint32_t base = 0;
+    if (int(threadIdx.x & 31u) == leader) base = atomicAdd(L.g.job_out_count + ln.job, uint32_t(__popc(group)));
+    base = __shfl_sync(group, base, leader);
+    const uint32_t local = base + uint32_t(__popc(group & ((1u << (threadIdx.x & 31u)) - 1u)));
+    const FrameJob& J = L.jobs[ln.job];
+    if (local >= J.wave_capacity) return;  // cannot happen: the region covers every path of the frame's wave
+    slot = J.wave_offset + local;
+  } else {
+    slot = aggregated_increment(L.g.out_count);
+    if (slot >= L.g.capacity) return;  // cannot happen: capacity covers every path of the wave
+  }
   float4* st = L.g.out_state + 6 * size_t(slot);
   st[0] = make_float4(ln.hp.x, ln.hp.y, ln.hp.z, ln.hn.x);
   st[1] = make_float4(ln.hn.y, ln.hn.z, ln.alb.x, ln.alb.y);
@@ -477,7 +517,7 @@ __device__ __forceinline__ void suspend_path(const RenderLaunch& L, const Lane& 
   st[3] = make_float4(ln.rad.x, ln.rad.y, ln.rad.z, __int_as_float(ln.depth));
   st[4] = make_float4(__uint_as_float(ln.pixel), __uint_as_float(uint32_t(ln.rng.state)),
                       __uint_as_float(uint32_t(ln.rng.state >> 32)), __uint_as_float(uint32_t(ln.rng.inc)));
-  st[5] = make_float4(__uint_as_float(uint32_t(ln.rng.inc >> 32)), 0.0f, 0.0f, 0.0f);
+  st[5] = make_float4(__uint_as_float(uint32_t(ln.rng.inc >> 32)), __uint_as_float(ln.job), 0.0f, 0.0f);
   float4* q = L.g.out_query + 2 * size_t(slot);
   q[0] = make_float4(ln.hp.x, ln.hp.y, ln.hp.z, 0.0f);
   q[1] = make_float4(ln.hn.x, ln.hn.y, ln.hn.z, 0.0f);
@@ -495,6 +535,7 @@ __device__ __forceinline__ void resume_path(const RenderLaunch& L, Lane& ln, uin
   ln.pixel = __float_as_uint(e.x);
   ln.rng.state = uint64_t(__float_as_uint(e.y)) | (uint64_t(__float_as_uint(e.z)) << 32);
   ln.rng.inc = uint64_t(__float_as_uint(e.w)) | (uint64_t(__float_as_uint(f.x)) << 32);
+  ln.job = __float_as_uint(f.y);
   ln.include_emission = false;
   ln.bsdf_pdf = -1.0f;
   ln.mix_slot = int(slot);
@@ -505,32 +546,37 @@ __device__ __forceinline__ void resume_path(const RenderLaunch& L, Lane& ln, uin
   ln.phase = kShadowLight;
 }
 
-template <int kMode, bool kMoments>
-__device__ __forceinline__ void shade_hit(const RenderLaunch& L, const FrameJob& J, Lane& ln, const TraceResult& tr,
-                                          uint32_t& n_paths) {
-  const DevScene& s = J.scene;
-  const float4* p = reinterpret_cast<const float4*>(s.prims + tr.rec);
-  const float4 A = __ldg(p), B = __ldg(p + 1);
-  const V3 hp = ln.ro + ln.rd * tr.t;
-  V3 nrm;
-  float tu = 0.0f, tv = 0.0f;
+// Surface seen by a ray at its closest hit: point, shading normal facing the ray, texture
+// coordinates and material (intersect.rs:57-68, :122-148).
+struct Surface {
+  V3 hp, nrm;
+  float tu, tv;
   bool front;
   uint32_t mat;
+};
+
+__device__ __forceinline__ Surface surface_at(const DevScene& s, V3 ro, V3 rd, const TraceResult& tr) {
+  Surface f;
+  const float4* p = reinterpret_cast<const float4*>(s.prims + tr.rec);
+  const float4 A = __ldg(p), B = __ldg(p + 1);
+  f.hp = ro + rd * tr.t;
+  f.tu = 0.0f;
+  f.tv = 0.0f;
   if (tr.tag & kTagTriangle) {
     const float4 C = __ldg(p + 2);
     const V3 e1 = mk(B.x, B.y, B.z), e2 = mk(C.x, C.y, C.z);
     const V3 gn = normalize(cross(e1, e2));
-    front = dot(ln.rd, gn) < 0.0f;
+    f.front = dot(rd, gn) < 0.0f;
     V3 outward = gn;
     const uint32_t flags = __float_as_uint(C.w);
     if (flags != 0u && s.attributes != nullptr) {
       // Barycentrics for attribute interpolation (intersect.rs:124-135).
-      const V3 sv = ln.ro - mk(A.x, A.y, A.z);
-      const V3 pv = cross(ln.rd, e2);
+      const V3 sv = ro - mk(A.x, A.y, A.z);
+      const V3 pv = cross(rd, e2);
       const float inv = 1.0f / dot(e1, pv);
       const float u = dot(sv, pv) * inv;
       const V3 qv = cross(sv, e1);
-      const float v = dot(ln.rd, qv) * inv;
+      const float v = dot(rd, qv) * inv;
       const float w0 = 1.0f - u - v;
       const float4* at = s.attributes + size_t(5) * (tr.tag & kTagIndexMask);
       if (flags & 1u) {
@@ -540,61 +586,96 @@ __device__ __forceinline__ void shade_hit(const RenderLaunch& L, const FrameJob&
       }
       if (flags & 2u) {
         const float4 uv01 = __ldg(at + 3), uv2 = __ldg(at + 4);
-        tu = w0 * uv01.x + u * uv01.z + v * uv2.x;
-        tv = w0 * uv01.y + u * uv01.w + v * uv2.y;
+        f.tu = w0 * uv01.x + u * uv01.z + v * uv2.x;
+        f.tv = w0 * uv01.y + u * uv01.w + v * uv2.y;
       }
     }
-    nrm = front ? outward : -outward;
-    mat = __float_as_uint(B.w);
+    f.nrm = f.front ? outward : -outward;
   } else {
-    const V3 outward = (hp - mk(A.x, A.y, A.z)) * (1.0f / B.x);
-    front = dot(ln.rd, outward) < 0.0f;
-    nrm = front ? outward : -outward;
-    mat = __float_as_uint(B.w);
+    const V3 outward = (f.hp - mk(A.x, A.y, A.z)) * (1.0f / B.x);
+    f.front = dot(rd, outward) < 0.0f;
+    f.nrm = f.front ? outward : -outward;
   }
-  const DevMaterial m = s.materials[mat];
+  f.mat = __float_as_uint(B.w);
+  return f;
+}
+
+// Fuzzy metal reflection (integrator.rs:303-313): false when the ray is absorbed (it points into
+// the surface). On success the lane holds the reflected ray.
+__device__ __forceinline__ bool bounce_metal(Lane& ln, const DevMaterial& m, const Surface& f) {
+  const V3 refl = reflect(normalize(ln.rd), f.nrm);
+  const V3 ball = uniform_ball(ln.rng.uniform(), ln.rng.uniform(), ln.rng.uniform());
+  const V3 dir = refl + ball * m.roughness;
+  if (dot(dir, f.nrm) <= 0.0f) return false;
+  ln.ro = f.hp;
+  ln.rd = normalize(dir);
+  ln.thr = ln.thr * mk(m.albedo[0], m.albedo[1], m.albedo[2]);
+  return true;
+}
+
+// Dielectric (integrator.rs:315-334): Schlick reflection or Snell refraction.
+__device__ __forceinline__ void bounce_dielectric(Lane& ln, const DevMaterial& m, const Surface& f) {
+  const float ratio = f.front ? 1.0f / m.ior : m.ior;
+  const V3 unit = normalize(ln.rd);
+  const float ct = fminf(dot(-unit, f.nrm), 1.0f);
+  const float st = sqrtf(1.0f - ct * ct);
+  const bool cannot = ratio * st > 1.0f;
+  V3 dir;
+  if (cannot || schlick(ct, ratio) > ln.rng.uniform()) dir = reflect(unit, f.nrm);
+  else dir = refract(unit, f.nrm, ratio);
+  ln.ro = f.hp;
+  ln.rd = normalize(dir);
+}
+
+// Cosine-weighted diffuse direction about the lane's shading normal (integrator.rs:277-301).
+__device__ __forceinline__ V3 cosine_direction(Lane& ln) {
+  V3 dir = ln.hn + uniform_sphere(ln.rng.uniform(), ln.rng.uniform());
+  if (dot(dir, dir) < 1e-8f) dir = ln.hn;
+  return normalize(dir);
+}
+
+// The lane continues from its diffuse vertex along `dir` (drawn by cosine_direction).
+__device__ __forceinline__ void take_diffuse_bounce(Lane& ln, V3 dir) {
+  ln.ro = ln.hp;
+  ln.rd = dir;
+  ln.thr = ln.thr * ln.alb;
+  ln.include_emission = false;
+  ln.bsdf_pdf = fmaxf(dot(ln.hn, dir), 0.0f) / kPiF;
+}
+
+template <int kMode, bool kMoments, bool kBatch>
+__device__ __forceinline__ void shade_hit(const RenderLaunch& L, const FrameJob& J, Lane& ln, const TraceResult& tr,
+                                          uint32_t& n_paths) {
+  const DevScene& s = J.scene;
+  const Surface f = surface_at(s, ln.ro, ln.rd, tr);
+  const DevMaterial m = s.materials[f.mat];
   if (m.kind == kEmissive) {
     if (ln.include_emission) ln.rad = ln.rad + ln.thr * mk(m.emission[0], m.emission[1], m.emission[2]);
     finish_sample<kMode, kMoments>(L, J, ln, n_paths);
     return;
   }
   if (m.kind == kDiffuse) {
-    ln.hp = hp;
-    ln.hn = nrm;
-    ln.alb = base_color(s, m, tu, tv);
+    ln.hp = f.hp;
+    ln.hn = f.nrm;
+    ln.alb = base_color(s, m, f.tu, f.tv);
     ln.mix_slot = -1;
     ln.phase = kShadowLight;
     if constexpr (kMode == kModeGuided) {
       // A vertex that will scatter waits for the network's mixture; the last vertex only does NEE.
       if (ln.depth > 1) {
-        suspend_path(L, ln);
+        suspend_path<kBatch>(L, ln);
         ln.phase = kIdle;
       }
     }
     return;
   }
   if (m.kind == kMetal) {
-    const V3 refl = reflect(normalize(ln.rd), nrm);
-    const V3 ball = uniform_ball(ln.rng.uniform(), ln.rng.uniform(), ln.rng.uniform());
-    const V3 dir = refl + ball * m.roughness;
-    if (dot(dir, nrm) <= 0.0f) {
+    if (!bounce_metal(ln, m, f)) {
       finish_sample<kMode, kMoments>(L, J, ln, n_paths);
       return;
     }
-    ln.ro = hp;
-    ln.rd = normalize(dir);
-    ln.thr = ln.thr * mk(m.albedo[0], m.albedo[1], m.albedo[2]);
-  } else {  // dielectric (integrator.rs:315-334)
-    const float ratio = front ? 1.0f / m.ior : m.ior;
-    const V3 unit = normalize(ln.rd);
-    const float ct = fminf(dot(-unit, nrm), 1.0f);
-    const float st = sqrtf(1.0f - ct * ct);
-    const bool cannot = ratio * st > 1.0f;
-    V3 dir;
-    if (cannot || schlick(ct, ratio) > ln.rng.uniform()) dir = reflect(unit, nrm);
-    else dir = refract(unit, nrm, ratio);
-    ln.ro = hp;
-    ln.rd = normalize(dir);
+  } else {
+    bounce_dielectric(ln, m, f);
   }
   ln.include_emission = true;
   ln.bsdf_pdf = -1.0f;
@@ -607,7 +688,7 @@ __device__ __forceinline__ void shade_hit(const RenderLaunch& L, const FrameJob&
 // L.min_active) with an optional shared-memory short stack (L.short_stack).
 template <int kMode, bool kMoments, bool kBatch, bool kPause>
 __global__ void __launch_bounds__(256) render_kernel(const RenderLaunch L) {
-  static_assert(!kBatch || kMode == kModePlain, "batched launches trace plain paths");
+  static_assert(!kBatch || kMode != kModeRecord, "batched launches do not record training samples");
   // The root record lives in device memory (a geometry refit rewrites it between launches);
   // single-frame launches stage it in shared memory once.
   __shared__ ChildRec root;
@@ -636,7 +717,10 @@ __global__ void __launch_bounds__(256) render_kernel(const RenderLaunch L) {
   uint32_t n_paths = 0, n_ext = 0, n_shadow = 0, node_visits = 0;
   uint64_t total_items = L.total_items;
   if constexpr (kMode == kModeGuided) {
-    if (L.g.resume) total_items = *L.g.in_count < L.g.capacity ? *L.g.in_count : L.g.capacity;
+    if (L.g.resume) {
+      if constexpr (kBatch) total_items = L.g.in_job_prefix[L.job_count];
+      else total_items = *L.g.in_count < L.g.capacity ? *L.g.in_count : L.g.capacity;
+    }
   }
 
   for (;;) {
@@ -653,7 +737,39 @@ __global__ void __launch_bounds__(256) render_kernel(const RenderLaunch L) {
         if (item >= total_items) {
           finished = true;
         } else if (kMode == kModeGuided && L.g.resume) {
-          resume_path(L, ln, uint32_t(item));
+          if constexpr (kBatch) {
+            // The frame whose share of this round's suspended paths holds the item.
+            uint32_t lo = 0, hi = L.job_count - 1;
+            while (lo < hi) {
+              const uint32_t mid = (lo + hi + 1) >> 1;
+              if (L.g.in_job_prefix[mid] <= item) lo = mid;
+              else hi = mid - 1;
+            }
+            resume_path(L, ln, L.jobs[lo].wave_offset + uint32_t(item - L.g.in_job_prefix[lo]));
+          } else {
+            resume_path(L, ln, uint32_t(item));
+          }
+        } else if (kMode == kModeGuided && kBatch) {
+          // One path per item; a frame's items are its wave's samples, pixel-major within each.
+          const uint64_t ws = L.g.wave_spp;
+          uint32_t lo = 0, hi = L.job_count - 1;
+          while (lo < hi) {
+            const uint32_t mid = (lo + hi + 1) >> 1;
+            if (uint64_t(L.jobs[mid].pix_begin) * ws <= item) lo = mid;
+            else hi = mid - 1;
+          }
+          ln.job = lo;
+          const FrameJob& J = L.jobs[lo];
+          const uint32_t fpix = J.width * J.height;
+          const uint64_t local = item - uint64_t(J.pix_begin) * ws;
+          const uint32_t k = uint32_t(local / fpix);
+          ln.pixel = uint32_t(local - uint64_t(k) * fpix);
+          ln.item_samples = 1;
+          ln.item_done = 0;
+          ln.sample = J.sample_base + L.g.wave_first_sample + k;
+          ln.acc = mk(0.f, 0.f, 0.f);
+          if (kMoments) ln.acc2 = mk(0.f, 0.f, 0.f);
+          start_sample(J, ln);
         } else if (kMode == kModeGuided) {
           // One path per item: pixel-major within each sample of the wave.
           const uint32_t k = uint32_t(item / npix);
@@ -730,9 +846,7 @@ __global__ void __launch_bounds__(256) render_kernel(const RenderLaunch L) {
               const float ut = ln.rng.uniform();
               V3 dir;
               if (ut < 1.0f - L.g.guide_fraction) {
-                dir = ln.hn + uniform_sphere(ln.rng.uniform(), ln.rng.uniform());
-                if (dot(dir, dir) < 1e-8f) dir = ln.hn;
-                dir = normalize(dir);
+                dir = cosine_direction(ln);
               } else {
                 const float a = ln.rng.uniform(), b = ln.rng.uniform(), c = ln.rng.uniform();
                 dir = mix_sample(mix, a, b, c);
@@ -753,9 +867,7 @@ __global__ void __launch_bounds__(256) render_kernel(const RenderLaunch L) {
               break;
             }
           }
-          V3 dir = ln.hn + uniform_sphere(ln.rng.uniform(), ln.rng.uniform());
-          if (dot(dir, dir) < 1e-8f) dir = ln.hn;
-          dir = normalize(dir);
+          const V3 dir = cosine_direction(ln);
           if constexpr (kMode == kModeRecord) {
             const uint32_t slot = aggregated_increment(L.g.record_count);
             if (slot < L.g.record_capacity) {
@@ -768,11 +880,7 @@ __global__ void __launch_bounds__(256) render_kernel(const RenderLaunch L) {
               r[3] = make_float4(ln.rad.x, ln.rad.y, ln.rad.z, t.z);
             }
           }
-          ln.ro = ln.hp;
-          ln.rd = dir;
-          ln.thr = ln.thr * ln.alb;
-          ln.include_emission = false;
-          ln.bsdf_pdf = fmaxf(dot(ln.hn, dir), 0.0f) / kPiF;
+          take_diffuse_bounce(ln, dir);
           ln.phase = kExtend;
           break;
         }
@@ -848,7 +956,7 @@ __global__ void __launch_bounds__(256) render_kernel(const RenderLaunch L) {
           ln.rad = ln.rad + ln.thr * background(s, ln.rd, ln.bsdf_pdf);
           finish_sample<kMode, kMoments>(L, J, ln, n_paths);
         } else {
-          shade_hit<kMode, kMoments>(L, J, ln, tr, n_paths);
+          shade_hit<kMode, kMoments, kBatch>(L, J, ln, tr, n_paths);
         }
       }
     }
@@ -889,17 +997,40 @@ static cudaError_t launch_mode(const RenderLaunch& r, int block_size, int grid_s
   return cudaGetLastError();
 }
 
-cudaError_t launch_render_batch(const RenderLaunch& r, int block_size, int grid_size, cudaStream_t stream) {
+cudaError_t launch_render_batch(const RenderLaunch& r, int block_size, int grid_size, cudaStream_t stream,
+                                bool guided) {
   if (!r.jobs || r.job_count == 0) return cudaErrorInvalidValue;
-  render_kernel<kModePlain, false, true, false><<<grid_size, block_size, 0, stream>>>(r);
+  if (guided) render_kernel<kModeGuided, false, true, false><<<grid_size, block_size, 0, stream>>>(r);
+  else render_kernel<kModePlain, false, true, false><<<grid_size, block_size, 0, stream>>>(r);
   return cudaGetLastError();
 }
 
-int render_batch_max_blocks_per_sm(int block_size, int /*short_stack*/) {
+int render_batch_max_blocks_per_sm(int block_size, bool guided) {
   int blocks = 0;
   const cudaError_t e =
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, render_kernel<kModePlain, false, true, false>, block_size, 0);
+      guided ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, render_kernel<kModeGuided, false, true, false>,
+                                                             block_size, 0)
+             : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, render_kernel<kModePlain, false, true, false>,
+                                                             block_size, 0);
   return e == cudaSuccess ? blocks : 0;
+}
+
+// Exclusive prefix of the per-frame suspended-path counts of one guided round; prefix[n] = total.
+__global__ void job_prefix_kernel(const uint32_t* __restrict__ counts, const FrameJob* __restrict__ jobs, uint32_t n,
+                                  uint32_t* __restrict__ prefix) {
+  if (threadIdx.x != 0) return;
+  uint32_t run = 0;
+  for (uint32_t i = 0; i < n; ++i) {
+    prefix[i] = run;
+    run += min(counts[i], jobs[i].wave_capacity);
+  }
+  prefix[n] = run;
+}
+
+cudaError_t launch_job_prefix(const uint32_t* counts, const FrameJob* jobs, uint32_t n, uint32_t* prefix,
+                              cudaStream_t stream) {
+  job_prefix_kernel<<<1, 32, 0, stream>>>(counts, jobs, n, prefix);
+  return cudaGetLastError();
 }
 
 cudaError_t launch_render(const RenderLaunch& r, int block_size, int grid_size, bool moments, cudaStream_t stream,
@@ -928,6 +1059,378 @@ int render_max_blocks_per_sm(int block_size, bool moments, int mode, int short_s
   if (mode == kModeRecord) return blocks_for<kModeRecord>(block_size, moments);
   if (mode == kModeGuided) return blocks_for<kModeGuided>(block_size, moments);
   return blocks_for<kModePlain>(block_size, moments);
+}
+
+// ------------------------------------------------------------------------ wavefront schedule
+// The estimator of render_kernel (plain mode), split into three launches per iteration over
+// per-path state in device memory (WavefrontLaunch). Every path draws its random numbers in the
+// order the megakernel does (camera jitter; then per diffuse vertex light NEE, environment NEE,
+// scatter; per metal or dielectric vertex its BSDF draws) from the same per-(frame, pixel, sample)
+// seed, and adds its contributions in the same order, so each path is the megakernel's path.
+
+__device__ __forceinline__ unsigned lanes_below() { return (1u << (threadIdx.x & 31u)) - 1u; }
+
+// Appends the lanes whose `pred` holds to a queue counter with one atomic per warp; returns each
+// such lane's position. Every lane of the warp must call it together.
+__device__ __forceinline__ uint32_t warp_append(uint32_t* counter, bool pred) {
+  const unsigned m = __ballot_sync(0xffffffffu, pred);
+  if (!m) return 0u;
+  const int leader = __ffs(m) - 1;
+  uint32_t base = 0;
+  if (int(threadIdx.x & 31u) == leader) base = atomicAdd(counter, uint32_t(__popc(m)));
+  base = __shfl_sync(0xffffffffu, base, leader);
+  return base + uint32_t(__popc(m & lanes_below()));
+}
+
+template <bool kMoments>
+__global__ void __launch_bounds__(256) wf_logic_kernel(const WavefrontLaunch W) {
+  const FrameJob& J = W.r.f;
+  const DevScene& s = J.scene;
+  const uint32_t npix = J.width * J.height;
+  const uint32_t stride = gridDim.x * blockDim.x;
+  uint32_t n_paths = 0, n_live = 0;
+  // The loop bound is uniform across the block, so whole warps run every iteration together.
+  for (uint32_t base = blockIdx.x * blockDim.x; base < W.capacity; base += stride) {
+    const uint32_t slot = base + threadIdx.x;
+    const bool valid = slot < W.capacity;
+    const uint32_t st = valid ? W.state[slot] : 0u;
+    bool free_slot = valid && !(st & kWfAlive);
+    int kind = -1;
+    if (st & kWfAlive) {
+      const float4 r4 = W.rad[slot];
+      const float4 t4 = W.thr[slot];
+      V3 rad = mk(r4.x, r4.y, r4.z);
+      const V3 thr = mk(t4.x, t4.y, t4.z);
+      if (st & kWfNeePending) {
+        const float4 a = W.nee[2 * size_t(slot)], b = W.nee[2 * size_t(slot) + 1];
+        rad = rad + mk(a.x, a.y, a.z);
+        rad = rad + mk(b.x, b.y, b.z);
+      }
+      bool done = (st & kWfTerminate) != 0u;
+      if (!done && (st & kWfExtPending)) {
+        const uint4 h = W.hit[slot];
+        if (h.y == kNoNode) {
+          const float4 d4 = W.ray_d[slot];
+          rad = rad + thr * background(s, mk(d4.x, d4.y, d4.z), W.ray_o[slot].w);
+          done = true;
+        } else {
+          const uint32_t mat = __float_as_uint(__ldg(&s.prims[h.y].b[3]));
+          const uint32_t k = __ldg(&s.materials[mat].kind);
+          if (k == kEmissive) {
+            if (st & kWfEmission) {
+              const DevMaterial& m = s.materials[mat];
+              rad = rad + thr * mk(__ldg(&m.emission[0]), __ldg(&m.emission[1]), __ldg(&m.emission[2]));
+            }
+            done = true;
+          } else {
+            kind = int(k);
+          }
+        }
+      }
+      if (done) {
+        const uint32_t pixel = __float_as_uint(t4.w);
+        double* a = J.accum + size_t(3) * pixel;
+        atomicAdd(a, double(rad.x));
+        atomicAdd(a + 1, double(rad.y));
+        atomicAdd(a + 2, double(rad.z));
+        if (kMoments) {
+          const V3 r2 = rad * rad;
+          double* q2 = J.accum_sq + size_t(3) * pixel;
+          atomicAdd(q2, double(r2.x));
+          atomicAdd(q2 + 1, double(r2.y));
+          atomicAdd(q2 + 2, double(r2.z));
+        }
+        ++n_paths;
+        free_slot = true;
+      } else {
+        W.rad[slot] = make_float4(rad.x, rad.y, rad.z, 0.0f);
+      }
+    }
+    // Paths that go on join the queue of their material (the shade launch rewrites their state).
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      const uint32_t pos = warp_append(W.q + kWfMatCount + k, kind == k);
+      if (kind == k) W.mat_q[size_t(k) * W.capacity + pos] = slot;
+    }
+    // Free slots start new camera paths: consecutive work items are consecutive pixels of one
+    // sample, so a warp's new rays are neighbours.
+    const unsigned want = __ballot_sync(0xffffffffu, free_slot);
+    bool started = false;
+    if (want) {
+      const int leader = __ffs(want) - 1;
+      unsigned long long first = 0;
+      if (int(threadIdx.x & 31u) == leader) first = atomicAdd(W.r.work_counter, (unsigned long long)__popc(want));
+      first = __shfl_sync(0xffffffffu, first, leader);
+      if (free_slot) {
+        const uint64_t item = first + __popc(want & lanes_below());
+        if (item < W.r.total_items) {
+          const uint32_t chunk = uint32_t(item / npix);
+          Lane ln;
+          ln.pixel = uint32_t(item - uint64_t(chunk) * npix);
+          ln.sample = J.sample_base + chunk;
+          start_sample(J, ln);
+          W.ray_o[slot] = make_float4(ln.ro.x, ln.ro.y, ln.ro.z, -1.0f);
+          W.ray_d[slot] = make_float4(ln.rd.x, ln.rd.y, ln.rd.z, 0.0f);
+          W.thr[slot] = make_float4(1.0f, 1.0f, 1.0f, __uint_as_float(ln.pixel));
+          W.rad[slot] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+          W.rng[slot] = make_uint4(uint32_t(ln.rng.state), uint32_t(ln.rng.state >> 32), uint32_t(ln.rng.inc),
+                                   uint32_t(ln.rng.inc >> 32));
+          W.state[slot] = kWfAlive | kWfExtPending | kWfEmission | (uint32_t(ln.depth) & kWfDepthMask);
+          started = true;
+        } else if (st & kWfAlive) {
+          W.state[slot] = 0u;
+        }
+      }
+    }
+    const uint32_t pos = warp_append(W.q + kWfExtCount, started);
+    if (started) W.ext_q[pos] = slot;
+    n_live += (kind >= 0 || started) ? 1u : 0u;
+  }
+  const unsigned long long tp = __reduce_add_sync(0xffffffffu, n_paths);
+  const uint32_t tl = __reduce_add_sync(0xffffffffu, n_live);
+  if ((threadIdx.x & 31u) == 0) {
+    if (tp) atomicAdd(W.r.counters, tp);
+    if (tl) atomicAdd(W.q + kWfLive, tl);
+  }
+}
+
+__global__ void __launch_bounds__(128) wf_shade_kernel(const WavefrontLaunch W) {
+  const FrameJob& J = W.r.f;
+  const DevScene& s = J.scene;
+  const uint32_t n0 = W.q[kWfMatCount], n1 = W.q[kWfMatCount + 1], n2 = W.q[kWfMatCount + 2];
+  const uint32_t total = n0 + n1 + n2;
+  const uint32_t stride = gridDim.x * blockDim.x;
+  // Entries are numbered diffuse, then metal, then dielectric, and a warp takes 32 consecutive
+  // ones, so all but the warps at the two boundaries shade a single material.
+  for (uint32_t base = blockIdx.x * blockDim.x + (threadIdx.x & ~31u); base < total; base += stride) {
+    const uint32_t i = base + (threadIdx.x & 31u);
+    const bool valid = i < total;
+    uint32_t slot = 0, kind = 0;
+    if (valid) {
+      if (i < n0) {
+        slot = W.mat_q[i];
+      } else if (i < n0 + n1) {
+        kind = kMetal;
+        slot = W.mat_q[size_t(W.capacity) + (i - n0)];
+      } else {
+        kind = kDielectric;
+        slot = W.mat_q[2 * size_t(W.capacity) + (i - n0 - n1)];
+      }
+    }
+    bool shadow_l = false, shadow_e = false, extend = false;
+    Lane ln;
+    float4 c0 = make_float4(0.f, 0.f, 0.f, 0.f), c1 = c0;
+    float4 sl0, sl1, se0, se1;
+    uint32_t nst = kWfAlive;
+    if (valid) {
+      const float4 o4 = W.ray_o[slot], d4 = W.ray_d[slot], t4 = W.thr[slot];
+      const uint4 r4 = W.rng[slot], h = W.hit[slot];
+      const uint32_t st = W.state[slot];
+      ln.ro = mk(o4.x, o4.y, o4.z);
+      ln.rd = mk(d4.x, d4.y, d4.z);
+      ln.thr = mk(t4.x, t4.y, t4.z);
+      ln.rng.state = uint64_t(r4.x) | (uint64_t(r4.y) << 32);
+      ln.rng.inc = uint64_t(r4.z) | (uint64_t(r4.w) << 32);
+      ln.depth = int(st & kWfDepthMask);
+      TraceResult tr;
+      tr.t = __uint_as_float(h.x);
+      tr.rec = h.y;
+      tr.tag = h.z;
+      const Surface f = surface_at(s, ln.ro, ln.rd, tr);
+      const DevMaterial m = s.materials[f.mat];
+      float bsdf_pdf = -1.0f;
+      if (kind == kDiffuse) {
+        ln.hp = f.hp;
+        ln.hn = f.nrm;
+        ln.alb = base_color(s, m, f.tu, f.tv);
+        if (prepare_light_shadow(s, ln)) {
+          shadow_l = true;
+          sl0 = make_float4(ln.ro.x, ln.ro.y, ln.ro.z, ln.tmax);
+          sl1 = make_float4(ln.rd.x, ln.rd.y, ln.rd.z, __uint_as_float(2u * slot));
+          c0 = make_float4(ln.pend.x, ln.pend.y, ln.pend.z, 0.0f);
+        }
+        if (prepare_env_shadow<kModePlain>(W.r, J, ln)) {
+          shadow_e = true;
+          se0 = make_float4(ln.ro.x, ln.ro.y, ln.ro.z, ln.tmax);
+          se1 = make_float4(ln.rd.x, ln.rd.y, ln.rd.z, __uint_as_float(2u * slot + 1u));
+          c1 = make_float4(ln.pend.x, ln.pend.y, ln.pend.z, 0.0f);
+        }
+        W.nee[2 * size_t(slot)] = c0;
+        W.nee[2 * size_t(slot) + 1] = c1;
+        nst |= kWfNeePending;
+        ln.depth -= 1;
+        if (ln.depth > 0) {
+          take_diffuse_bounce(ln, cosine_direction(ln));
+          bsdf_pdf = ln.bsdf_pdf;
+          extend = true;
+        }
+      } else {
+        const bool on = kind == kMetal ? bounce_metal(ln, m, f) : (bounce_dielectric(ln, m, f), true);
+        ln.depth -= 1;
+        extend = on && ln.depth > 0;
+        nst |= kWfEmission;
+      }
+      if (extend) nst |= kWfExtPending | (uint32_t(ln.depth) & kWfDepthMask);
+      else nst |= kWfTerminate;
+      W.ray_o[slot] = make_float4(ln.ro.x, ln.ro.y, ln.ro.z, bsdf_pdf);
+      W.ray_d[slot] = make_float4(ln.rd.x, ln.rd.y, ln.rd.z, 0.0f);
+      W.thr[slot] = make_float4(ln.thr.x, ln.thr.y, ln.thr.z, t4.w);
+      W.rng[slot] = make_uint4(uint32_t(ln.rng.state), uint32_t(ln.rng.state >> 32), uint32_t(ln.rng.inc),
+                               uint32_t(ln.rng.inc >> 32));
+      W.state[slot] = nst;
+    }
+    const uint32_t pl = warp_append(W.q + kWfShadowCount, shadow_l);
+    if (shadow_l) {
+      W.shadow_q[2 * size_t(pl)] = sl0;
+      W.shadow_q[2 * size_t(pl) + 1] = sl1;
+    }
+    const uint32_t pe = warp_append(W.q + kWfShadowCount, shadow_e);
+    if (shadow_e) {
+      W.shadow_q[2 * size_t(pe)] = se0;
+      W.shadow_q[2 * size_t(pe) + 1] = se1;
+    }
+    const uint32_t px = warp_append(W.q + kWfExtCount, extend);
+    if (extend) W.ext_q[px] = slot;
+  }
+}
+
+// Loads queue entry i (extension rays first, then shadow rays) as a ray with its distance limit.
+__device__ __forceinline__ RayQ wf_entry_ray(const WavefrontLaunch& W, uint32_t i, uint32_t n_ext, float& tmax,
+                                             uint32_t& target) {
+  if (i < n_ext) {
+    target = W.ext_q[i];
+    const float4 o = W.ray_o[target], d = W.ray_d[target];
+    tmax = CUDART_INF_F;
+    return make_ray(o.x, o.y, o.z, d.x, d.y, d.z);
+  }
+  const size_t j = i - n_ext;
+  const float4 a = W.shadow_q[2 * j], b = W.shadow_q[2 * j + 1];
+  tmax = a.w;
+  target = __float_as_uint(b.w);
+  return make_ray(a.x, a.y, a.z, b.x, b.y, b.z);
+}
+
+// Result of queue entry i: the closest hit of an extension ray, or the occlusion of a shadow ray
+// (an occluded shadow ray drops its contribution, integrator.rs:196-199 and :233-238).
+__device__ __forceinline__ void wf_entry_result(const WavefrontLaunch& W, uint32_t i, uint32_t n_ext, uint32_t target,
+                                                bool hit, float t, uint32_t rec, uint32_t tag) {
+  if (i < n_ext) W.hit[target] = make_uint4(__float_as_uint(t), hit ? rec : kNoNode, hit ? tag : 0u, 0u);
+  else if (hit) W.nee[target] = make_float4(0.f, 0.f, 0.f, 0.f);
+}
+
+// kRefill = false: a warp takes 32 consecutive queue entries and traces each to its end.
+// kRefill = true: dynamic ray fetching; a lane whose ray is done takes the next queue entry as
+// soon as fewer than W.refill_lanes lanes of its warp are still traversing (the others keep
+// their traversal state and stack meanwhile).
+// kWatertight: the watertight triangle test over the scene's vertex records.
+template <bool kRefill, bool kWatertight>
+__global__ void __launch_bounds__(128) wf_trace_kernel(const WavefrontLaunch W) {
+  static_assert(!(kRefill && kWatertight), "the resumable traversal tests triangles with Moller-Trumbore");
+  __shared__ ChildRec root;
+  __shared__ unsigned long long s_count[2];
+  if (threadIdx.x == 0) root = *W.r.f.scene.root;
+  if (threadIdx.x < 2) s_count[threadIdx.x] = 0ull;
+  __syncthreads();
+  const DevScene& s = W.r.f.scene;
+  const uint32_t n_ext = W.q[kWfExtCount], total = n_ext + W.q[kWfShadowCount];
+  const unsigned lane = threadIdx.x & 31u;
+  uint32_t c_ext = 0, c_sh = 0, visits = 0;
+  if constexpr (!kRefill) {
+    // Extension rays come first, then shadow rays, so a warp traces one kind of ray (only the
+    // warp at the boundary holds both).
+    for (;;) {
+      uint32_t base = 0;
+      if (lane == 0) base = atomicAdd(W.q + kWfTraceCursor, 32u);
+      base = __shfl_sync(0xffffffffu, base, 0);
+      if (base >= total) break;
+      const uint32_t i = base + lane;
+      if (i < total) {
+        float tmax;
+        uint32_t target;
+        const RayQ q = wf_entry_ray(W, i, n_ext, tmax, target);
+        TraceResult tr;
+        bool hit;
+        if (i < n_ext) {
+          hit = trace_ray<kWatertight>(s.pairs, s.prims, root, q, kRayEps, tmax, false, tr, visits, s.tri_verts);
+          ++c_ext;
+        } else {
+          hit = trace_ray<kWatertight>(s.pairs, s.prims, root, q, kRayEps, tmax, true, tr, visits, s.tri_verts);
+          ++c_sh;
+        }
+        wf_entry_result(W, i, n_ext, target, hit, tr.t, tr.rec, tr.tag);
+      }
+    }
+  } else {
+    Traversal T;
+    T.cur = kNoNode;
+    RayQ q = make_ray(0.f, 0.f, 0.f, 1.f, 1.f, 1.f);
+    uint32_t idx = 0, target = 0;
+    bool busy = false, exhausted = false;
+    uint2 st_local[kMaxStack];
+    for (;;) {
+      // Lanes without a ray take the next entries, one atomic per warp.
+      const bool need = !busy && !exhausted;
+      const unsigned m = __ballot_sync(0xffffffffu, need);
+      if (m) {
+        const int leader = __ffs(m) - 1;
+        uint32_t base = 0;
+        if (int(lane) == leader) base = atomicAdd(W.q + kWfTraceCursor, uint32_t(__popc(m)));
+        base = __shfl_sync(0xffffffffu, base, leader);
+        if (need) {
+          idx = base + uint32_t(__popc(m & lanes_below()));
+          if (idx < total) {
+            float tmax;
+            q = wf_entry_ray(W, idx, n_ext, tmax, target);
+            trav_start(T, root, q, kRayEps, tmax);
+            busy = true;
+            if (idx < n_ext) ++c_ext;
+            else ++c_sh;
+          } else {
+            exhausted = true;
+          }
+        }
+      }
+      if (!__any_sync(0xffffffffu, busy)) break;
+      trav_advance(T, q, kRayEps, idx >= n_ext, s.pairs, s.prims, st_local, nullptr, 0, 0, W.refill_lanes,
+                   !exhausted, visits);
+      if (busy && T.cur == kNoNode) {
+        wf_entry_result(W, idx, n_ext, target, T.found(), T.closest, T.rec, T.tag);
+        busy = false;
+      }
+    }
+  }
+  const unsigned long long te = __reduce_add_sync(0xffffffffu, c_ext);
+  const unsigned long long ts = __reduce_add_sync(0xffffffffu, c_sh);
+  if (lane == 0) {
+    if (te) atomicAdd(&s_count[0], te);
+    if (ts) atomicAdd(&s_count[1], ts);
+  }
+  __syncthreads();
+  if (threadIdx.x < 2 && s_count[threadIdx.x] != 0ull) atomicAdd(W.r.counters + 1 + threadIdx.x, s_count[threadIdx.x]);
+}
+
+// Resident blocks per SM of a kernel at a block size.
+template <class K>
+static int resident_blocks(K kernel, int block) {
+  int blocks = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, kernel, block, 0) != cudaSuccess) return 1;
+  return blocks > 0 ? blocks : 1;
+}
+
+cudaError_t launch_wavefront_iteration(const WavefrontLaunch& w, bool moments, int sm_count, cudaStream_t stream) {
+  static const int shade_per_sm = resident_blocks(wf_shade_kernel, 128);
+  static const int trace_per_sm = resident_blocks(wf_trace_kernel<false, false>, 128);
+  static const int refill_per_sm = resident_blocks(wf_trace_kernel<true, false>, 128);
+  static const int watertight_per_sm = resident_blocks(wf_trace_kernel<false, true>, 128);
+  const unsigned logic_grid =
+      unsigned(std::min<uint64_t>((uint64_t(w.capacity) + 255) / 256, uint64_t(sm_count) * 8));
+  if (moments) wf_logic_kernel<true><<<logic_grid, 256, 0, stream>>>(w);
+  else wf_logic_kernel<false><<<logic_grid, 256, 0, stream>>>(w);
+  wf_shade_kernel<<<shade_per_sm * sm_count, 128, 0, stream>>>(w);
+  if (w.r.f.scene.tri_verts) wf_trace_kernel<false, true><<<watertight_per_sm * sm_count, 128, 0, stream>>>(w);
+  else if (w.refill_lanes > 1) wf_trace_kernel<true, false><<<refill_per_sm * sm_count, 128, 0, stream>>>(w);
+  else wf_trace_kernel<false, false><<<trace_per_sm * sm_count, 128, 0, stream>>>(w);
+  return cudaGetLastError();
 }
 
 // ------------------------------------------------------------------------ training samples

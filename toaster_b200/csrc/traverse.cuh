@@ -106,6 +106,70 @@ __device__ __forceinline__ bool hit_sphere(const RayQ& r, float4 A, float4 B, fl
   return true;
 }
 
+// FP32 watertight ray/triangle test (Woop, Benthin and Wald, "Watertight Ray/Triangle
+// Intersection", JCGT 2(1), 2013): a non-parity option. The ray is sheared so that it runs along
+// +z from the origin; the triangle's vertices are projected into that frame and the three 2-D
+// edge functions decide the hit, recomputed in double when one is exactly zero. Every product and
+// sum is rounded on its own, so two triangles sharing an edge evaluate its edge function from the
+// same projected vertices to exactly opposite values: a ray cannot pass between them.
+struct RayW {
+  int kx, ky, kz;   // the dominant direction axis is kz; kx, ky complete a right-handed frame
+  float sx, sy, sz; // shear constants d[kx]/d[kz], d[ky]/d[kz], 1/d[kz]
+};
+
+__device__ __forceinline__ float axis_of(float x, float y, float z, int k) { return k == 0 ? x : (k == 1 ? y : z); }
+
+__device__ __forceinline__ RayW make_ray_watertight(const RayQ& r) {
+  const float ax = fabsf(r.dx), ay = fabsf(r.dy), az = fabsf(r.dz);
+  RayW w;
+  w.kz = ax > ay ? (ax > az ? 0 : 2) : (ay > az ? 1 : 2);
+  w.kx = w.kz == 2 ? 0 : w.kz + 1;
+  w.ky = w.kx == 2 ? 0 : w.kx + 1;
+  const float dz = axis_of(r.dx, r.dy, r.dz, w.kz);
+  if (dz < 0.0f) {  // keeps the winding, so the edge-function signs mean the same for every ray
+    const int t = w.kx;
+    w.kx = w.ky;
+    w.ky = t;
+  }
+  w.sx = __fdiv_rn(axis_of(r.dx, r.dy, r.dz, w.kx), dz);
+  w.sy = __fdiv_rn(axis_of(r.dx, r.dy, r.dz, w.ky), dz);
+  w.sz = __frcp_rn(dz);
+  return w;
+}
+
+// Double-sided watertight test of triangle (v0, v1, v2) accepting t in [tmin, tmax].
+__device__ __forceinline__ bool hit_triangle_watertight(const RayQ& r, const RayW& w, float4 v0, float4 v1, float4 v2,
+                                                        float tmin, float tmax, float& t_out) {
+  const float Ax0 = __fsub_rn(v0.x, r.ox), Ay0 = __fsub_rn(v0.y, r.oy), Az0 = __fsub_rn(v0.z, r.oz);
+  const float Bx0 = __fsub_rn(v1.x, r.ox), By0 = __fsub_rn(v1.y, r.oy), Bz0 = __fsub_rn(v1.z, r.oz);
+  const float Cx0 = __fsub_rn(v2.x, r.ox), Cy0 = __fsub_rn(v2.y, r.oy), Cz0 = __fsub_rn(v2.z, r.oz);
+  const float Ak = axis_of(Ax0, Ay0, Az0, w.kz), Bk = axis_of(Bx0, By0, Bz0, w.kz), Ck = axis_of(Cx0, Cy0, Cz0, w.kz);
+  const float Ax = __fsub_rn(axis_of(Ax0, Ay0, Az0, w.kx), __fmul_rn(w.sx, Ak));
+  const float Ay = __fsub_rn(axis_of(Ax0, Ay0, Az0, w.ky), __fmul_rn(w.sy, Ak));
+  const float Bx = __fsub_rn(axis_of(Bx0, By0, Bz0, w.kx), __fmul_rn(w.sx, Bk));
+  const float By = __fsub_rn(axis_of(Bx0, By0, Bz0, w.ky), __fmul_rn(w.sy, Bk));
+  const float Cx = __fsub_rn(axis_of(Cx0, Cy0, Cz0, w.kx), __fmul_rn(w.sx, Ck));
+  const float Cy = __fsub_rn(axis_of(Cx0, Cy0, Cz0, w.ky), __fmul_rn(w.sy, Ck));
+  float U = __fsub_rn(__fmul_rn(Cx, By), __fmul_rn(Cy, Bx));
+  float V = __fsub_rn(__fmul_rn(Ax, Cy), __fmul_rn(Ay, Cx));
+  float W = __fsub_rn(__fmul_rn(Bx, Ay), __fmul_rn(By, Ax));
+  if (U == 0.0f || V == 0.0f || W == 0.0f) {
+    // On an edge in single precision: decide with the exact products of the same inputs.
+    U = float(__dsub_rn(__dmul_rn(double(Cx), double(By)), __dmul_rn(double(Cy), double(Bx))));
+    V = float(__dsub_rn(__dmul_rn(double(Ax), double(Cy)), __dmul_rn(double(Ay), double(Cx))));
+    W = float(__dsub_rn(__dmul_rn(double(Bx), double(Ay)), __dmul_rn(double(By), double(Ax))));
+  }
+  if ((U < 0.0f || V < 0.0f || W < 0.0f) && (U > 0.0f || V > 0.0f || W > 0.0f)) return false;
+  const float det = __fadd_rn(__fadd_rn(U, V), W);
+  if (det == 0.0f) return false;
+  const float T = __fadd_rn(__fadd_rn(__fmul_rn(U, __fmul_rn(w.sz, Ak)), __fmul_rn(V, __fmul_rn(w.sz, Bk))),
+                            __fmul_rn(W, __fmul_rn(w.sz, Ck)));
+  const float t = __fdiv_rn(T, det);
+  if (!(t >= tmin && t <= tmax)) return false;
+  t_out = t;
+  return true;
+}
+
 struct TraceResult {
   float t;        // closest accepted distance (or tmax when nothing was accepted)
   uint32_t tag;   // PrimRecord tag of the accepted primitive
@@ -253,9 +317,16 @@ __device__ __forceinline__ void trav_step(Traversal& T, const RayQ& r, float tmi
 // Whole traversal of one ray in one call (the form every launch uses unless it pauses traversals
 // for refills): the same node and primitive order as trav_step's, with the state in registers and
 // the stack in local memory.
+//
+// kWatertight selects the watertight triangle test (hit_triangle_watertight) with the vertices of
+// leaf-order primitive record k at verts[3k..3k+2]; the default is the reference's Moller-Trumbore.
+template <bool kWatertight = false>
 __device__ __forceinline__ bool trace_ray(const PairNode* __restrict__ pairs, const PrimRecord* __restrict__ prims,
                                           const ChildRec& root, const RayQ& r, float tmin, float tmax,
-                                          bool any_hit, TraceResult& res, uint32_t& node_visits) {
+                                          bool any_hit, TraceResult& res, uint32_t& node_visits,
+                                          const float4* __restrict__ verts = nullptr) {
+  RayW rw;
+  if constexpr (kWatertight) rw = make_ray_watertight(r);
   float closest = tmax;
   bool found = false;
   float entry, tn;
@@ -308,8 +379,13 @@ __device__ __forceinline__ bool trace_ray(const PairNode* __restrict__ pairs, co
       float t;
       bool ok;
       if (tag & kTagTriangle) {
-        const float4 C = __ldg(p + 2);
-        ok = hit_triangle(r, A, B, C, tmin, closest, t);
+        if constexpr (kWatertight) {
+          const float4* v = verts + 3 * size_t(k);
+          ok = hit_triangle_watertight(r, rw, __ldg(v), __ldg(v + 1), __ldg(v + 2), tmin, closest, t);
+        } else {
+          const float4 C = __ldg(p + 2);
+          ok = hit_triangle(r, A, B, C, tmin, closest, t);
+        }
       } else {
         ok = hit_sphere(r, A, B, tmin, closest, t);
       }

@@ -46,6 +46,7 @@ EXPORTED_SYMBOLS = (
     "tc_record_sizes",
     "tc_umma_selftest",
     "tc_probe_cache_read",
+    "tc_set_triangle_test",
     "tc_probe_last_error",
     "tc_guide_set_params",
     "tc_guide_get_params",
@@ -126,7 +127,11 @@ class RenderOptions(ctypes.Structure):
         ("short_stack", ctypes.c_uint32),
         ("refill_lanes", ctypes.c_uint32),
         ("guide_fraction", ctypes.c_float),
+        ("schedule", ctypes.c_uint32),
     ]
+
+
+SCHEDULES = {"auto": 0, "megakernel": 1, "wavefront": 2}
 
 
 class TuneResult(ctypes.Structure):
@@ -199,6 +204,7 @@ def load_library(path: os.PathLike | None = None) -> ctypes.CDLL:
     lib.tc_animation_destroy.argtypes = [vp]
     lib.tc_autotune.argtypes = [vp, vp, ctypes.POINTER(RenderOptions), u32, ctypes.POINTER(TuneResult)]
     lib.tc_set_hierarchy_build.argtypes = [vp, i32]
+    lib.tc_set_triangle_test.argtypes = [vp, i32]
     lib.tc_encode_jpeg.argtypes = [vp, u32, f32, vp, sz, ctypes.POINTER(sz)]
     lib.tc_scene_load.argtypes = [ctypes.c_char_p, ctypes.POINTER(vp), ctypes.c_char_p, sz]
     lib.tc_loaded_scene_data.argtypes = [vp]

@@ -72,11 +72,14 @@ class Animation:
 
 
 def render_batch(renderers, samples=None, frame_index: int = 0, accumulate: bool = False, block_size: int = 0,
-                 samples_per_item: int = 0, short_stack: int = 0, refill_lanes: int = 0) -> dict:
+                 samples_per_item: int = 0, short_stack: int = 0, refill_lanes: int = 0, guiding: bool = False,
+                 guide_fraction: float = 0.0, wave_paths: int = 0) -> dict:
     """One persistent launch over the uploaded scenes of several renderers (same device).
 
-    ``samples`` may be one count or one per renderer. Returns the batch's stats (paths, rays,
-    kernel and total milliseconds)."""
+    ``samples`` may be one count or one per renderer (one count for all when ``guiding``).
+    ``guiding``: every renderer needs guide parameters; each frame's queries go to its own
+    network, in rounds of (batched path kernel, per-frame inference, batched resume). Returns the
+    batch's stats (paths, rays, kernel and total milliseconds)."""
     if not renderers:
         raise ValueError("empty batch")
     lib = renderers[0]._lib
@@ -98,6 +101,9 @@ def render_batch(renderers, samples=None, frame_index: int = 0, accumulate: bool
     opts.samples_per_item = samples_per_item
     opts.short_stack = short_stack
     opts.refill_lanes = refill_lanes
+    opts.guiding = 1 if guiding else 0
+    opts.guide_fraction = guide_fraction
+    opts.wave_paths = wave_paths
     native.check(lib, renderers[0]._ctx, lib.tc_render_batch(ctxs, params.ctypes.data, n, ctypes.byref(opts)))
     for i, r in enumerate(renderers):
         r.width, r.height = int(params[i]["width"]), int(params[i]["height"])
@@ -213,6 +219,12 @@ class GpuRenderer:
         """Where uploads build the hierarchy: "auto", "host" or "device"."""
         self._check(self._lib.tc_set_hierarchy_build(self._ctx, {"auto": 0, "host": 1, "device": 2}[mode]))
 
+    def set_triangle_test(self, test: str) -> None:
+        """Triangle test of later uploads: "moller_trumbore" (the reference's, bit-exact hits) or
+        "watertight" (no ray slips between triangles sharing an edge; traced by trace_closest and
+        wavefront renders)."""
+        self._check(self._lib.tc_set_triangle_test(self._ctx, {"moller_trumbore": 0, "watertight": 1}[test]))
+
     def set_stream(self, stream: int) -> None:
         """Enqueue on a caller-owned cudaStream_t (0 = the context's own stream)."""
         self._check(self._lib.tc_set_stream(self._ctx, stream or None))
@@ -225,10 +237,11 @@ class GpuRenderer:
                height: Optional[int] = None, frame_index: int = 0, accumulate: bool = False,
                keep_moments: bool = False, block_size: int = 0, samples_per_item: int = 0, guiding: bool = False,
                guide_record: bool = False, wave_paths: int = 0, short_stack: int = 0, refill_lanes: int = 0,
-               guide_fraction: float = 0.0) -> None:
+               guide_fraction: float = 0.0, schedule: str = "auto") -> None:
         """Traces ``samples`` paths per pixel; ``accumulate`` adds them to the previous batches.
         ``guide_fraction``: probability of sampling the network's mixture at a guided diffuse
-        vertex (0 = the library's default, 0.5)."""
+        vertex (0 = the library's default, 0.5). ``schedule`` (plain renders): "auto",
+        "megakernel" or "wavefront"."""
         if self._params is None:
             raise RuntimeError("render before upload")
         p = self._params.copy()
@@ -252,6 +265,7 @@ class GpuRenderer:
         opts.short_stack = short_stack
         opts.refill_lanes = refill_lanes
         opts.guide_fraction = guide_fraction
+        opts.schedule = native.SCHEDULES[schedule]
         self._check(self._lib.tc_render(self._ctx, p.ctypes.data, ctypes.byref(opts)))
         self.width, self.height = int(p["width"][0]), int(p["height"][0])
         self.accumulated = (self.accumulated if accumulate else 0) + int(p["samples"][0])
