@@ -84,3 +84,51 @@ def test_launch_shapes_trace_the_same_paths(renderer, refill, short_stack):
     renderer.render(frame_index=5, refill_lanes=refill, short_stack=short_stack, block_size=256)
     b = renderer.readback_sums()[0]
     assert close(b, a) > 0.999
+
+
+def test_guided_batch_matches_individual_guided_renders(native_lib):
+    # Each frame's queries are inferred by its own network, and every path keeps its seed, so a
+    # guided frame traced inside a batch takes the paths of its own guided render.
+    from toaster_b200 import guiding_eval
+
+    sc = [configs.room_with_window(width=64, height=36, samples=8, clutter=1024),
+          configs.mixed(width=80, height=45, samples=8, max_bounces=6),
+          configs.plain_small()]
+    for s in sc:
+        s.samples = 8
+    rs = [GpuRenderer(0) for _ in sc]
+    try:
+        for i, (r, s) in enumerate(zip(rs, sc)):
+            r.upload(scene_to_gpu(s))
+            r.guide_set_params(guiding_eval.initial_params(3 + i), configs.scene_bounds(s))
+        # A small wave, so the batch runs several waves of whole samples per pixel.
+        st = render_batch(rs, frame_index=4, guiding=True, wave_paths=40000)
+        assert st["paths"] == sum(s.width * s.height * 8 for s in sc)
+        batched = [r.readback_sums()[0] for r in rs]
+        for r, s, b in zip(rs, sc, batched):
+            r.render(frame_index=4, guiding=True)
+            single = r.readback_sums()[0]
+            assert close(b, single) > 0.999
+            assert b.sum() > 0
+    finally:
+        for r in rs:
+            r.close()
+
+
+def test_guided_batch_needs_networks_and_one_sample_count(native_lib):
+    from toaster_b200 import guiding_eval
+
+    a, b = GpuRenderer(0), GpuRenderer(0)
+    try:
+        s = configs.plain_small()
+        a.upload(scene_to_gpu(s))
+        b.upload(scene_to_gpu(s))
+        a.guide_set_params(guiding_eval.initial_params(1), configs.scene_bounds(s))
+        with pytest.raises(TcError, match="tc_guide_set_params"):
+            render_batch([a, b], guiding=True)
+        b.guide_set_params(guiding_eval.initial_params(2), configs.scene_bounds(s))
+        with pytest.raises(TcError, match="one sample count"):
+            render_batch([a, b], samples=[4, 8], guiding=True)
+    finally:
+        a.close()
+        b.close()

@@ -3,15 +3,20 @@
 Closest hit: the primitive index must match bit-exactly and the hit distance within 4 ulp
 (this implementation reproduces the reference's f32 arithmetic, so the distances are expected to
 be identical; the 4-ulp bound is the stated tolerance). Images: per-pixel means must agree
-within a 3-sigma band built from both renderers' per-pixel sample variances.
+within a 3-sigma band built from both renderers' per-pixel sample variances, with the fraction of
+pixels outside it, the median block z-score and the image-mean difference held to bars calibrated
+by running the oracle against itself (tests/calibrate_parity.py).
 """
 
-import math
+import json
+from pathlib import Path
 
 import numpy as np
 import pytest
 
 import oracle
+import parity_cases
+import parity_stats
 from toaster_b200 import configs, gpu_types as gt
 from toaster_b200.native import TcError
 from toaster_b200.scene import EnvironmentMap, Material, Scene, box_triangles, scene_to_gpu
@@ -125,82 +130,52 @@ def test_emissive_and_black_known_answers(renderer):  # integrator.rs:682-700 on
     assert np.array_equal(render_image(renderer, zero_depth, max_bounces=0)[..., :3], np.zeros((8, 8, 3), np.float32))
 
 
-def _blocks(x, b):
-    h, w = x.shape
-    h2, w2 = h // b * b, w // b * b
-    return x[:h2, :w2].reshape(h2 // b, b, w2 // b, b).sum(axis=(1, 3))
+CALIBRATION = Path(__file__).resolve().parent / "golden" / "parity_calibration.json"
+# Bars over the oracle-against-itself calibration (worst of three independent seed pairs at the
+# same sample counts): limit = factor x worst + slack. The slack covers the sampling noise of a
+# statistic that three pairs cannot pin (binomial noise of a 1% fraction over ~7,000 z-scores is
+# about 0.1%; the median of ~600 block z-scores moves by about 0.05).
+BARS = {"outside_pixel": (1.5, 0.005), "outside_block": (1.5, 0.01), "median_z": (1.5, 0.15),
+        "global_dz": (1.5, 2.0), "rel_mean": (1.5, 0.01)}
 
 
-def statistical_parity(renderer, scene, gpu_spp=4096, cpu_spp=256, block=2, upload=None):
-    """GPU image vs the oracle's at the same scene.
+def statistical_parity(renderer, case_name, upload=None, scene=None):
+    """GPU image vs the oracle's on one case of tests/parity_cases.py.
 
-    Path-tracing samples are heavy-tailed (small lights, a 1e4 sun), so z-scores use the
-    per-pixel variance of the high-spp GPU run for both sides and are taken over 2x2 pixel
-    blocks. Thresholds were calibrated by running the oracle against itself with independent
-    seeds at the same sample counts (worst seen: 3.5% of blocks beyond 3 sigma, |median z| 0.21,
-    |global dz/se| 3.3): at most 6% of blocks outside 3 sigma, |median z| <= 0.35, global mean
-    within 6 standard errors and 3% relative. ``upload`` replaces the default upload of
-    ``scene_to_gpu(scene)`` (the oracle always renders ``scene``).
+    Both renderers keep per-pixel sums of squared samples, and every z-score uses the variance of
+    the difference of the two means (GPU variance / GPU samples + oracle variance / oracle
+    samples), per pixel and channel and over 2x2-pixel luminance blocks (tests/parity_stats.py).
+    The bars come from running the oracle against itself at the same sample counts
+    (tests/calibrate_parity.py, tests/golden/parity_calibration.json). ``upload`` replaces the
+    default upload of ``scene_to_gpu(scene)`` (the oracle always renders ``scene``).
     """
+    case = parity_cases.BY_NAME[case_name]
+    scene = scene if scene is not None else case.make()
     if upload is None:
         renderer.upload(scene_to_gpu(scene))
     else:
         upload()
-    renderer.render(samples=gpu_spp, keep_moments=True, frame_index=17)
+    renderer.render(samples=case.gpu_spp, keep_moments=True, frame_index=17)
     s, q, n = renderer.readback_sums(moments=True)
-    assert n == gpu_spp
-    w = np.array([0.2126, 0.7152, 0.0722])
+    assert n == case.gpu_spp
     g_mean = s / n
-    g_var = np.maximum(q / n - g_mean**2, 0.0) * n / (n - 1)
-    cpu_scene = Scene(**{**scene.__dict__, "samples": cpu_spp})
-    o_mean, _, _ = oracle.Oracle(cpu_scene).render(seed=3)
-    gl, ol = g_mean @ w, o_mean.astype(np.float64) @ w
-    gv = g_var @ (w**2)
-    dm = _blocks(gl - ol, block) / block**2
-    var = _blocks(gv, block) * (1.0 / gpu_spp + 1.0 / cpu_spp) / block**4
-    const = var == 0
-    assert np.allclose(dm[const], 0.0, atol=1e-5)
-    z = dm[~const] / np.sqrt(var[~const])
-    outside = float(np.mean(np.abs(z) > 3.0))
-    assert outside <= 0.06, f"{outside:.4f} of blocks outside the 3-sigma band"
-    assert abs(float(np.median(z))) <= 0.35, f"median z {np.median(z):.3f}"
-    se = math.sqrt(gv.sum() * (1.0 / gpu_spp + 1.0 / cpu_spp)) / gv.size
-    dz = (gl.mean() - ol.mean()) / se
-    assert abs(dz) <= 6.0, f"global mean differs by {dz:.2f} standard errors"
-    assert abs(gl.mean() - ol.mean()) <= 0.03 * abs(ol.mean()), (gl.mean(), ol.mean())
-    return outside
+    g_var = parity_stats.sample_variance(g_mean, q, n)
+    cpu_scene = Scene(**{**scene.__dict__, "samples": case.cpu_spp})
+    o_mean, o_sq, _ = oracle.Oracle(cpu_scene).render(seed=3, moments=True)
+    o_var = parity_stats.sample_variance(o_mean, o_sq, case.cpu_spp)
+    st = parity_stats.compare(g_mean, g_var, case.gpu_spp, o_mean, o_var, case.cpu_spp)
+    print(json.dumps({"case": case_name, **st}))
+    worst = json.loads(CALIBRATION.read_text())[case_name]["worst"]
+    assert st["constant_mismatch"] == 0, st
+    for key, (factor, slack) in BARS.items():
+        limit = factor * worst[key] + slack
+        assert abs(st[key]) <= limit, f"{case_name}: {key} = {st[key]:.4f} beyond {limit:.4f} ({st})"
+    return st
 
 
-def test_image_statistical_parity_plain_small(renderer):
-    s = configs.plain_small()
-    s.width, s.height = 80, 45
-    statistical_parity(renderer, s)
-
-
-def test_image_statistical_parity_mixed(renderer):
-    s = configs.mixed(width=64, height=36, samples=64)
-    statistical_parity(renderer, s)
-
-
-def test_image_statistical_parity_sky_dielectric_metal(renderer):
-    mats = [Material.dielectric(1.5), Material.metal((0.9, 0.6, 0.3), 0.3), Material.diffuse((0.6, 0.7, 0.8)),
-            Material.emissive((1.0, 0.9, 0.8), 6.0)]
-    s = Scene(camera_position=(0, 1, 5), camera_look_at=(0, 0.3, 0), width=48, height=32, samples=64, max_bounces=6,
-              background=gt.SKY, materials=mats,
-              sphere_centers=np.array([(-0.8, 0.5, 0), (0.8, 0.5, 0), (0, -100, 0), (0, 3, 0)], np.float32),
-              sphere_radii=np.array([0.5, 0.5, 99.9, 0.4], np.float32), sphere_materials=np.array([0, 1, 2, 3], np.uint32))
-    statistical_parity(renderer, s)
-
-
-def test_image_statistical_parity_window_room(renderer):
-    # The learned-guiding workload's plain estimator: a closed room lit only through a small window,
-    # diffuse and metal clutter (long paths, environment NEE through an opening). The sky has no
-    # sun here: with it, a 256-spp mean of this room moves by 3% between seeds and by 19% between
-    # 256 and 4,096 spp (rare sun paths), which no mean comparison at these counts can bound. The
-    # oracle takes 1,024 spp, so its image mean varies about 1%.
-    env = configs.sky_environment(width=256, height=128, sun_radiance=0.0)
-    s = configs.room_with_window(width=48, height=27, samples=64, clutter=1024, environment=env)
-    statistical_parity(renderer, s, cpu_spp=1024)
+@pytest.mark.parametrize("case_name", [c.name for c in parity_cases.CASES])
+def test_image_statistical_parity(renderer, case_name):
+    statistical_parity(renderer, case_name)
 
 
 def test_progressive_accumulation_contract(renderer):

@@ -1,0 +1,87 @@
+"""The wavefront schedule against the megakernel (needs a B200).
+
+Both schedules trace the same estimator (crates/toaster-cpu/src/integrator.rs:99-244) and every
+path draws its random numbers in the same order from the same per-(frame, pixel, sample) seed,
+so each path is the same in both: the extension and shadow ray counts must be equal, and the
+per-pixel FP64 sums may differ only by the order in which the paths of a pixel were added.
+"""
+
+import numpy as np
+import pytest
+
+from toaster_b200 import configs
+from toaster_b200.scene import scene_to_gpu
+
+pytestmark = pytest.mark.gpu
+
+
+def render_both(renderer, samples, max_bounces=None, keep_moments=False, wave_paths=0, refill_lanes=0,
+                frame_index=3):
+    out = {}
+    for schedule in ("megakernel", "wavefront"):
+        renderer.render(samples=samples, max_bounces=max_bounces, frame_index=frame_index, keep_moments=keep_moments,
+                        schedule=schedule, wave_paths=wave_paths,
+                        refill_lanes=refill_lanes if schedule == "wavefront" else 0)
+        s, q, n = renderer.readback_sums(moments=keep_moments)
+        out[schedule] = (s, q, renderer.stats())
+    return out
+
+
+def assert_same_paths(out, scene, samples):
+    (s0, q0, st0), (s1, q1, st1) = out["megakernel"], out["wavefront"]
+    paths = scene.width * scene.height * samples
+    assert st0["paths"] == st1["paths"] == paths
+    assert st1["extension_rays"] == st0["extension_rays"]
+    assert st1["shadow_rays"] == st0["shadow_rays"]
+    # Only the FP64 summation order differs.
+    assert np.allclose(s1, s0, rtol=1e-9, atol=1e-9), np.abs(s1 - s0).max()
+    if q0 is not None:
+        assert np.allclose(q1, q0, rtol=1e-9, atol=1e-9), np.abs(q1 - q0).max()
+    assert s0.sum() > 0
+
+
+@pytest.mark.parametrize("make,samples", [(lambda: configs.mixed(width=96, height=54), 32),
+                                           (lambda: configs.plain_small(), 4),
+                                           (lambda: configs.room_with_window(width=64, height=36, clutter=1024), 32)],
+                         ids=["mixed", "plain_small", "window_room"])
+def test_wavefront_traces_the_megakernel_paths(renderer, make, samples):
+    scene = make()
+    renderer.upload(scene_to_gpu(scene))
+    assert_same_paths(render_both(renderer, samples), scene, samples)
+
+
+@pytest.mark.parametrize("bounces", [1, 2, 3])
+def test_wavefront_short_paths_and_moments(renderer, bounces):
+    scene = configs.mixed(width=64, height=36)
+    renderer.upload(scene_to_gpu(scene))
+    assert_same_paths(render_both(renderer, 16, max_bounces=bounces, keep_moments=True), scene, 16)
+
+
+@pytest.mark.parametrize("wave_paths", [32, 1000, 1 << 16])
+def test_wavefront_slot_counts(renderer, wave_paths):
+    # Fewer slots than paths: slots are refilled many times over, and a partial last warp of slots.
+    scene = configs.mixed(width=48, height=27)
+    renderer.upload(scene_to_gpu(scene))
+    assert_same_paths(render_both(renderer, 8, wave_paths=wave_paths), scene, 8)
+
+
+@pytest.mark.parametrize("refill_lanes", [8, 16, 28])
+def test_wavefront_dynamic_ray_fetching(renderer, refill_lanes):
+    # Trace lanes refill from the queue mid-traversal: the same rays, so the same paths.
+    scene = configs.mixed(width=64, height=36)
+    renderer.upload(scene_to_gpu(scene))
+    assert_same_paths(render_both(renderer, 16, refill_lanes=refill_lanes), scene, 16)
+
+
+def test_wavefront_progressive_batches(renderer):
+    # The progressive contract holds across schedules: a wavefront batch adds to megakernel batches.
+    scene = configs.mixed(width=64, height=36)
+    renderer.upload(scene_to_gpu(scene))
+    renderer.render(samples=8, frame_index=1, schedule="megakernel")
+    renderer.render(samples=8, frame_index=1, accumulate=True, schedule="wavefront")
+    mixed_sums, _, n = renderer.readback_sums()
+    assert n == 16
+    renderer.render(samples=8, frame_index=1, schedule="megakernel")
+    renderer.render(samples=8, frame_index=1, accumulate=True, schedule="megakernel")
+    mega_sums, _, _ = renderer.readback_sums()
+    assert np.allclose(mixed_sums, mega_sums, rtol=1e-9, atol=1e-9)
