@@ -1177,13 +1177,15 @@ int tc_autotune(tc_context* ctx, const tc_gpu_render_params* params, const tc_re
   p.accumulated_samples = 0;
   p.samples = probe_samples ? probe_samples : std::min<uint32_t>(params->samples, 4u);
   // Coordinate search over the launch shape, one knob at a time in this order, each stage keeping
-  // the fastest value so far: block size, dynamic-fetch threshold (refill lanes), shared
-  // short-stack entries, then (plain) samples per work item or (guided) wavefront width.
+  // the fastest value so far: (plain) schedule, then block size, dynamic-fetch threshold (refill
+  // lanes) and shared short-stack entries of the megakernel, or the trace launch's refill lanes of
+  // the wavefront; last the wavefront's path slots (guided or plain wavefront) or the
+  // megakernel's samples per work item.
   tc_render_options best = b;
   if (!best.block_size) best.block_size = 128;
   if (!best.refill_lanes) best.refill_lanes = kDefaultRefillLanes;
   if (!best.samples_per_item) best.samples_per_item = 1;
-  if (!best.wave_paths) best.wave_paths = 1u << 23;
+  if (!best.wave_paths && b.guiding) best.wave_paths = 1u << 23;
   float best_ms = -1.0f;
   uint32_t tried = 0;
   auto time_shape = [&](const tc_render_options& o, float& ms) -> int {
@@ -1212,11 +1214,19 @@ int tc_autotune(tc_context* ctx, const tc_gpu_render_params* params, const tc_re
     }
     return TC_OK;
   };
-  if (int rc = stage(&tc_render_options::block_size, {64u, 128u, 256u})) return rc;
+  const bool can_wavefront = !b.guiding && p.max_bounces > 0 && !ctx->scene.tri_verts;
+  if (can_wavefront)
+    if (int rc = stage(&tc_render_options::schedule, {TC_SCHEDULE_MEGAKERNEL, TC_SCHEDULE_WAVEFRONT})) return rc;
+  const bool wavefront = best.schedule == TC_SCHEDULE_WAVEFRONT;
+  if (!wavefront)
+    if (int rc = stage(&tc_render_options::block_size, {64u, 128u, 256u})) return rc;
   if (int rc = stage(&tc_render_options::refill_lanes, {1u, 12u, 20u, 28u})) return rc;
-  if (int rc = stage(&tc_render_options::short_stack, {0u, 8u, 16u})) return rc;
+  if (!wavefront)
+    if (int rc = stage(&tc_render_options::short_stack, {0u, 8u, 16u})) return rc;
   if (b.guiding) {
     if (int rc = stage(&tc_render_options::wave_paths, {1u << 21, 1u << 22, 1u << 23})) return rc;
+  } else if (wavefront) {
+    if (int rc = stage(&tc_render_options::wave_paths, {1u << 20, 1u << 21, 1u << 22})) return rc;
   } else {
     if (int rc = stage(&tc_render_options::samples_per_item, {1u, 2u, 4u})) return rc;
   }

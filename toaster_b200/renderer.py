@@ -288,7 +288,9 @@ class GpuRenderer:
         self.width, self.height = int(p["width"][0]), int(p["height"][0])
         self.accumulated = res.probe_samples
         b = res.best
-        return {"block_size": b.block_size, "short_stack": b.short_stack, "samples_per_item": b.samples_per_item,
+        schedule = {v: k for k, v in native.SCHEDULES.items()}[b.schedule]
+        return {"schedule": schedule, "block_size": b.block_size, "short_stack": b.short_stack,
+                "samples_per_item": b.samples_per_item,
                 "wave_paths": b.wave_paths, "refill_lanes": b.refill_lanes, "kernel_ms": res.best_kernel_ms,
                 "mpaths_per_s": res.best_mpaths_per_s, "candidates": res.candidates,
                 "probe_samples": res.probe_samples}
