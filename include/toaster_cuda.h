@@ -144,7 +144,7 @@ typedef struct tc_render_options {
                                 samples at every diffuse scatter of this batch and at every
                                 environment shadow ray that reaches the sky (plain sampling) */
   uint32_t wave_paths;       /* paths in flight: guided wavefront (0 = 2^23) or plain wavefront
-                                schedule (0 = 2^21) */
+                                schedule (0 = 2^22) */
   uint32_t short_stack;      /* traversal stack entries per thread held in shared memory (0..16;
                                 deeper entries live in local memory); 0 = none */
   uint32_t refill_lanes;     /* a warp pauses traversal to refill finished lanes once fewer than
@@ -161,7 +161,7 @@ typedef struct tc_render_options {
                                 path kernel; TC_SCHEDULE_WAVEFRONT (2) = per-path state in device
                                 memory and three launches per bounce (logic, material-sorted
                                 shading, tracing with one ray kind per warp), wave_paths slots
-                                (0 = 2^21). Captured animation frames use the megakernel. */
+                                (0 = 2^22). Captured animation frames use the megakernel. */
 } tc_render_options;
 #define TC_SCHEDULE_AUTO 0u
 #define TC_SCHEDULE_MEGAKERNEL 1u
@@ -256,15 +256,22 @@ int tc_render(tc_context* ctx, const tc_gpu_render_params* params, const tc_rend
  * fill the GPU together instead of one launch (and one tail) each. No reference counterpart: the
  * reference renders scenes one dispatch at a time (dispatch.rs:28-60). All contexts must be on
  * one device and distinct; the launch runs on contexts[0]'s stream after the others' pending
- * work, and tc_get_stats(contexts[0]) reports the whole batch. Plain sampling only (options may
- * set block_size and samples_per_item). Synchronous. */
+ * work, and tc_get_stats(contexts[0]) reports the whole batch. Options may set block_size and
+ * samples_per_item; moments and recording are rejected. With options->guiding every context needs
+ * guide parameters (tc_guide_set_params) and all frames one sample count: the batch then runs the
+ * guided wavefront over all frames at once, in waves of whole samples per pixel (wave_paths, 0 =
+ * 2^23 paths), each frame's suspended paths in a region of their own that the frame's own
+ * network infers. Synchronous. */
 int tc_render_batch(tc_context* const* contexts, const tc_gpu_render_params* params, size_t n,
                     const tc_render_options* options);
 
 /* Autotuner: a coordinate search over the launch shape on the uploaded scene at params' size,
- * one knob at a time, each stage keeping the fastest value: block size {64, 128, 256}, refill
- * lanes {1, 12, 20, 28}, shared-memory short-stack entries {0, 8, 16}, then samples per work item
- * {1, 2, 4} or, when base->guiding is set, wavefront width {2^21, 2^22, 2^23} paths. Each shape
+ * one knob at a time, each stage keeping the fastest value: for plain renders first the schedule
+ * {megakernel, wavefront}; then for the megakernel block size {64, 128, 256}, refill lanes
+ * {1, 12, 20, 28}, shared-memory short-stack entries {0, 8, 16} and samples per work item
+ * {1, 2, 4}; for the wavefront the trace launch's refill lanes {1, 12, 20, 28} and its path slots
+ * {2^20, 2^21, 2^22}; when base->guiding is set, the megakernel stages and then the guided
+ * wavefront width {2^21, 2^22, 2^23} paths. Each shape
  * runs once untimed and once timed (CUDA events) with probe_samples spp (0 = min(params->samples,
  * 4)). Other fields of `base` are kept. The context's accumulated image is replaced by the last
  * probe. No reference counterpart. */

@@ -4,9 +4,10 @@ Both schedules trace the same estimator (crates/toaster-cpu/src/integrator.rs:99
 path draws its random numbers in the same order from the same per-(frame, pixel, sample) seed,
 so each path is the same in both up to the compiler's fusing of multiply-adds, which may differ
 between the two kernels and, very rarely, tips a borderline decision (a metal reflection grazing
-the surface, Schlick against refraction) the other way. So the ray counts must agree within one
-ray in ten thousand, and all but 0.2% of the per-pixel FP64 sums may differ only by the order in
-which the paths of a pixel were added.
+the surface, Schlick against refraction) the other way; elsewhere it moves a path's radiance by
+an FP32 rounding or two. So the ray counts must agree within one ray in ten thousand, and all but
+0.2% of the per-pixel sums must agree to 1e-5 relative (a path that went another way moves its
+pixel by a few percent).
 """
 
 import numpy as np
@@ -31,8 +32,8 @@ def render_both(renderer, samples, max_bounces=None, keep_moments=False, wave_pa
 
 
 def same_fraction(a, b):
-    """Fraction of pixels whose three sums agree to FP64 summation-order noise."""
-    return float(np.mean(np.isclose(a, b, rtol=1e-9, atol=1e-9).all(axis=-1)))
+    """Fraction of pixels whose three sums agree to FP32 rounding of the paths' radiance."""
+    return float(np.mean(np.isclose(a, b, rtol=1e-5, atol=1e-7).all(axis=-1)))
 
 
 def assert_same_paths(out, scene, samples):

@@ -38,7 +38,7 @@ namespace {
 constexpr int kDefaultRefillLanes = 1;
 // Plain wavefront schedule: default path slots, and the smallest frame (in paths) that the
 // automatic schedule gives it (smaller frames run in less time than its per-bounce launches cost).
-constexpr uint32_t kWavefrontSlots = 1u << 21;
+constexpr uint32_t kWavefrontSlots = 1u << 22;
 constexpr uint64_t kWavefrontMinPaths = 1ull << 20;
 // Iterations the host runs ahead of the live-slot count it waits for (kWfRing = kWfLag + 1).
 constexpr int kWfLag = 4;
@@ -1215,6 +1215,11 @@ int tc_autotune(tc_context* ctx, const tc_gpu_render_params* params, const tc_re
     return TC_OK;
   };
   const bool can_wavefront = !b.guiding && p.max_bounces > 0 && !ctx->scene.tri_verts;
+  // The schedule the automatic choice takes for this probe, so the result names a concrete one.
+  if (best.schedule == TC_SCHEDULE_AUTO && !b.guiding)
+    best.schedule = can_wavefront && uint64_t(p.width) * p.height * p.samples >= kWavefrontMinPaths
+                        ? TC_SCHEDULE_WAVEFRONT
+                        : TC_SCHEDULE_MEGAKERNEL;
   if (can_wavefront)
     if (int rc = stage(&tc_render_options::schedule, {TC_SCHEDULE_MEGAKERNEL, TC_SCHEDULE_WAVEFRONT})) return rc;
   const bool wavefront = best.schedule == TC_SCHEDULE_WAVEFRONT;
