@@ -155,13 +155,16 @@ typedef struct tc_render_options {
   float guide_fraction;      /* guided renders: probability of sampling the network's mixture at a
                                 diffuse vertex (one-sample MIS with cosine sampling, the mixture pdf
                                 (1 - f) cos/pi + f q); in [0, 1), 0 = default 0.5 */
-  uint32_t schedule;         /* plain renders: TC_SCHEDULE_AUTO (0) = the wavefront for tc_render and
-                                tc_autotune calls of at least 2^20 paths and 1 or more bounces, the
-                                megakernel otherwise; TC_SCHEDULE_MEGAKERNEL (1) = one persistent
-                                path kernel; TC_SCHEDULE_WAVEFRONT (2) = per-path state in device
-                                memory and three launches per bounce (logic, material-sorted
-                                shading, tracing with one ray kind per warp), wave_paths slots
-                                (0 = 2^22). Captured animation frames use the megakernel. */
+  uint32_t schedule;         /* plain and guided renders: TC_SCHEDULE_AUTO (0) = the wavefront for
+                                tc_render and tc_autotune calls of at least 2^20 paths and 1 or more
+                                bounces, the megakernel otherwise; TC_SCHEDULE_MEGAKERNEL (1) = one
+                                persistent path kernel (guided: in rounds with inference between);
+                                TC_SCHEDULE_WAVEFRONT (2) = per-path state in device memory and
+                                three launches per bounce (logic, material-sorted shading, tracing
+                                with one ray kind per warp; guided: the diffuse queue inferred
+                                between logic and shading), wave_paths slots (0 = 2^22). Recording
+                                renders, batched launches and captured animation frames use the
+                                megakernel. */
 } tc_render_options;
 #define TC_SCHEDULE_AUTO 0u
 #define TC_SCHEDULE_MEGAKERNEL 1u
@@ -266,12 +269,11 @@ int tc_render_batch(tc_context* const* contexts, const tc_gpu_render_params* par
                     const tc_render_options* options);
 
 /* Autotuner: a coordinate search over the launch shape on the uploaded scene at params' size,
- * one knob at a time, each stage keeping the fastest value: for plain renders first the schedule
- * {megakernel, wavefront}; then for the megakernel block size {64, 128, 256}, refill lanes
- * {1, 12, 20, 28}, shared-memory short-stack entries {0, 8, 16} and samples per work item
- * {1, 2, 4}; for the wavefront the trace launch's refill lanes {1, 12, 20, 28} and its path slots
- * {2^20, 2^21, 2^22}; when base->guiding is set, the megakernel stages and then the guided
- * wavefront width {2^21, 2^22, 2^23} paths. Each shape
+ * one knob at a time, each stage keeping the fastest value: first the schedule {megakernel,
+ * wavefront}; then for the megakernel block size {64, 128, 256}, refill lanes {1, 12, 20, 28},
+ * shared-memory short-stack entries {0, 8, 16} and samples per work item {1, 2, 4} (guided: its
+ * wave width {2^21, 2^22, 2^23} paths instead); for the wavefront the trace launch's refill lanes
+ * {1, 12, 20, 28} and its path slots {2^20, 2^21, 2^22}. Each shape
  * runs once untimed and once timed (CUDA events) with probe_samples spp (0 = min(params->samples,
  * 4)). Other fields of `base` are kept. The context's accumulated image is replaced by the last
  * probe. No reference counterpart. */

@@ -93,3 +93,19 @@ def test_wavefront_progressive_batches(renderer):
     renderer.render(samples=8, frame_index=1, accumulate=True, schedule="megakernel")
     mega_sums, _, _ = renderer.readback_sums()
     assert same_fraction(mixed_sums, mega_sums) >= 0.998
+
+
+@pytest.mark.parametrize("fraction", [0.5, 0.85])
+def test_guided_wavefront_traces_the_guided_megakernel_paths(renderer, fraction):
+    # Guided: the same network infers the same (point, normal) queries in both schedules, and the
+    # paths draw in the same order (light NEE, environment NEE, then the one-sample MIS bounce).
+    from toaster_b200 import guiding_eval
+
+    scene = configs.room_with_window(width=64, height=36, clutter=1024)
+    renderer.upload(scene_to_gpu(scene))
+    renderer.guide_set_params(guiding_eval.initial_params(4), configs.scene_bounds(scene))
+    out = {}
+    for schedule in ("megakernel", "wavefront"):
+        renderer.render(samples=16, frame_index=2, guiding=True, guide_fraction=fraction, schedule=schedule)
+        out[schedule] = (renderer.readback_sums()[0], None, renderer.stats())
+    assert_same_paths(out, scene, 16)

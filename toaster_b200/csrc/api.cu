@@ -759,7 +759,7 @@ int tc_set_camera(tc_context* ctx, const tc_gpu_camera* cam) {
 // behind the last one it enqueued, for the live-slot count of an earlier iteration, so the GPU
 // always has queued work; the iterations launched after the last path finished find nothing to do.
 static int run_wavefront(tc_context* ctx, const tcb::RenderLaunch& L, uint32_t slots, uint32_t max_bounces,
-                         int refill_lanes, bool moments, cudaStream_t st) {
+                         int refill_lanes, bool moments, bool guided, cudaStream_t st) {
   const uint64_t items = L.total_items;
   const uint32_t cap = uint32_t(std::max<uint64_t>(32, std::min<uint64_t>(slots, items)));
   if (cap != ctx->wf_capacity) {
@@ -800,6 +800,13 @@ static int run_wavefront(tc_context* ctx, const tcb::RenderLaunch& L, uint32_t s
   w.mat_q = ctx->wf_mat_q.as<uint32_t>();
   w.q = ctx->wf_q.as<uint32_t>();
   w.refill_lanes = refill_lanes;
+  if (guided) {
+    // The diffuse queue's inference queries and decoded mixtures, one entry per slot.
+    TC_CUDA(ctx, ctx->w_query.reserve(sizeof(float4) * 2 * size_t(cap)));
+    TC_CUDA(ctx, ctx->w_mix.reserve(sizeof(float4) * tcb::kGuideDecodedF4 * size_t(cap)));
+    w.query = ctx->w_query.as<float4>();
+    w.r.g.in_mix = ctx->w_mix.as<float4>();
+  }
   TC_CUDA(ctx, cudaMemsetAsync(w.state, 0, sizeof(uint32_t) * cap, st));
   // Every iteration advances each live path by one vertex and refills every free slot, so the
   // frame drains in at most (waves + 1) x (bounces + 2) iterations; the bound only guards the loop.
@@ -807,7 +814,7 @@ static int run_wavefront(tc_context* ctx, const tcb::RenderLaunch& L, uint32_t s
   for (uint64_t it = 0;; ++it) {
     if (it > bound) return fail(ctx, TC_ERR_DEVICE_STATUS, "wavefront render did not drain its paths");
     TC_CUDA(ctx, cudaMemsetAsync(w.q, 0, sizeof(uint32_t) * tcb::kWfCounters, st));
-    TC_CUDA(ctx, tcb::launch_wavefront_iteration(w, moments, ctx->sm_count, st));
+    TC_CUDA(ctx, tcb::launch_wavefront_iteration(w, moments, ctx->sm_count, st, guided ? &ctx->guide : nullptr));
     const int k = int(it % kWfRing);
     TC_CUDA(ctx, cudaMemcpyAsync(ctx->wf_live_host + k, w.q + tcb::kWfLive, sizeof(uint32_t), cudaMemcpyDeviceToHost,
                                  st));
@@ -887,13 +894,14 @@ static int enqueue_render(tc_context* ctx, const tc_gpu_render_params* p, const 
     L.g.record_capacity = ctx->rec_capacity;
     L.g.path_radiance = ctx->rec_path_rad.as<float4>();
   }
-  // Plain renders called directly (not captured into a graph) may run as a wavefront.
+  // Plain and guided renders called directly (not captured into a graph) may run as a wavefront.
   const bool direct = !camera_dev && !frame_index_dev;
+  const bool wf_mode = mode == tcb::kModePlain || mode == tcb::kModeGuided;
   if (o.schedule > TC_SCHEDULE_WAVEFRONT) return fail(ctx, TC_ERR_INVALID, "schedule must be 0 (auto), 1 or 2");
-  if (o.schedule == TC_SCHEDULE_WAVEFRONT && mode == tcb::kModePlain && !direct)
+  if (o.schedule == TC_SCHEDULE_WAVEFRONT && wf_mode && !direct)
     return fail(ctx, TC_ERR_INVALID, "the wavefront schedule renders direct calls only, not captured frames");
   const bool wavefront =
-      mode == tcb::kModePlain && direct && p->max_bounces > 0 && p->max_bounces <= tcb::kWfDepthMask &&
+      wf_mode && direct && p->max_bounces > 0 && p->max_bounces <= tcb::kWfDepthMask &&
       (o.schedule == TC_SCHEDULE_WAVEFRONT ||
        (o.schedule == TC_SCHEDULE_AUTO && uint64_t(npix) * p->samples >= kWavefrontMinPaths));
   if (ctx->scene.tri_verts && !wavefront)
@@ -902,8 +910,9 @@ static int enqueue_render(tc_context* ctx, const tc_gpu_render_params* p, const 
   if (timing) TC_CUDA(ctx, cudaEventRecord(ctx->ev_kernel0, st));
   if (wavefront) {
     L.total_items = uint64_t(npix) * p->samples;  // one path per work item
+    L.g.guide_fraction = o.guide_fraction > 0.0f ? o.guide_fraction : 0.5f;
     if (int rc = run_wavefront(ctx, L, o.wave_paths ? o.wave_paths : kWavefrontSlots, p->max_bounces,
-                               int(o.refill_lanes), moments, st))
+                               int(o.refill_lanes), moments, mode == tcb::kModeGuided, st))
       return rc;
   } else if (mode != tcb::kModeGuided) {
     TC_CUDA(ctx, tcb::launch_render(L, block, grid, moments, st, mode));
@@ -1185,7 +1194,7 @@ int tc_autotune(tc_context* ctx, const tc_gpu_render_params* params, const tc_re
   if (!best.block_size) best.block_size = 128;
   if (!best.refill_lanes) best.refill_lanes = kDefaultRefillLanes;
   if (!best.samples_per_item) best.samples_per_item = 1;
-  if (!best.wave_paths && b.guiding) best.wave_paths = 1u << 23;
+
   float best_ms = -1.0f;
   uint32_t tried = 0;
   auto time_shape = [&](const tc_render_options& o, float& ms) -> int {
@@ -1214,9 +1223,9 @@ int tc_autotune(tc_context* ctx, const tc_gpu_render_params* params, const tc_re
     }
     return TC_OK;
   };
-  const bool can_wavefront = !b.guiding && p.max_bounces > 0 && !ctx->scene.tri_verts;
+  const bool can_wavefront = p.max_bounces > 0 && !ctx->scene.tri_verts;
   // The schedule the automatic choice takes for this probe, so the result names a concrete one.
-  if (best.schedule == TC_SCHEDULE_AUTO && !b.guiding)
+  if (best.schedule == TC_SCHEDULE_AUTO)
     best.schedule = can_wavefront && uint64_t(p.width) * p.height * p.samples >= kWavefrontMinPaths
                         ? TC_SCHEDULE_WAVEFRONT
                         : TC_SCHEDULE_MEGAKERNEL;
@@ -1228,10 +1237,10 @@ int tc_autotune(tc_context* ctx, const tc_gpu_render_params* params, const tc_re
   if (int rc = stage(&tc_render_options::refill_lanes, {1u, 12u, 20u, 28u})) return rc;
   if (!wavefront)
     if (int rc = stage(&tc_render_options::short_stack, {0u, 8u, 16u})) return rc;
-  if (b.guiding) {
-    if (int rc = stage(&tc_render_options::wave_paths, {1u << 21, 1u << 22, 1u << 23})) return rc;
-  } else if (wavefront) {
+  if (wavefront) {
     if (int rc = stage(&tc_render_options::wave_paths, {1u << 20, 1u << 21, 1u << 22})) return rc;
+  } else if (b.guiding) {
+    if (int rc = stage(&tc_render_options::wave_paths, {1u << 21, 1u << 22, 1u << 23})) return rc;
   } else {
     if (int rc = stage(&tc_render_options::samples_per_item, {1u, 2u, 4u})) return rc;
   }

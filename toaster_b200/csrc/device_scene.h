@@ -142,6 +142,9 @@ struct WavefrontLaunch {
   uint32_t* mat_q;       // 3 x capacity: slots to shade, per material kind
   uint32_t* q;           // kWfCounters counters
   int refill_lanes;      // > 1: trace lanes refill once fewer than this many of a warp still traverse
+  // Guided renders: the inference queries of the diffuse queue (2 float4 per entry); their decoded
+  // mixtures go to r.g.in_mix (kGuideDecodedF4 float4 per entry) with r.g.guide_fraction.
+  float4* query;
 };
 
 // Vertices of every triangle record in leaf order (verts[3k..3k+2]) gathered from the scene-order
@@ -156,8 +159,11 @@ cudaError_t launch_render(const RenderLaunch& r, int block_size, int grid_size, 
                           int mode = kModePlain);
 int render_max_blocks_per_sm(int block_size, bool moments, int mode = kModePlain, int short_stack = 0,
                              int min_active = 1);
-// One wavefront iteration (logic, shade, trace) on `stream`; the caller clears w.q first.
-cudaError_t launch_wavefront_iteration(const WavefrontLaunch& w, bool moments, int sm_count, cudaStream_t stream);
+// One wavefront iteration (logic, [guide inference,] shade, trace) on `stream`; the caller
+// clears w.q first. `guide` (guided renders) is the network that infers the diffuse queue.
+struct GuideDevice;
+cudaError_t launch_wavefront_iteration(const WavefrontLaunch& w, bool moments, int sm_count, cudaStream_t stream,
+                                       const GuideDevice* guide = nullptr);
 // Batched launch over r.jobs (r.job_count frames, items concatenated in job order): plain, or one
 // round of the guided wavefront (r.g, with per-frame regions of the wave buffers).
 cudaError_t launch_render_batch(const RenderLaunch& r, int block_size, int grid_size, cudaStream_t stream,

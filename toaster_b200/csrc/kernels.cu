@@ -20,6 +20,7 @@
 #include <algorithm>
 
 #include "device_scene.h"
+#include "guide.h"
 #include "traverse.cuh"
 
 namespace tcb {
@@ -643,6 +644,30 @@ __device__ __forceinline__ void take_diffuse_bounce(Lane& ln, V3 dir) {
   ln.bsdf_pdf = fmaxf(dot(ln.hn, dir), 0.0f) / kPiF;
 }
 
+// Guided diffuse bounce: one-sample MIS of cosine and guide sampling (the balance heuristic =
+// the mixture pdf, the guide taken with probability g.guide_fraction), so the estimator stays
+// unbiased whatever the network predicts. `mix` is the vertex's decoded mixture. False when the
+// sampled direction leaves below the surface (the path ends).
+__device__ __forceinline__ bool take_guided_bounce(const GuideLaunch& g, const float4* __restrict__ mix, Lane& ln) {
+  const float ut = ln.rng.uniform();
+  V3 dir;
+  if (ut < 1.0f - g.guide_fraction) {
+    dir = cosine_direction(ln);
+  } else {
+    const float a = ln.rng.uniform(), b = ln.rng.uniform(), c = ln.rng.uniform();
+    dir = mix_sample(mix, a, b, c);
+  }
+  const float cs = dot(ln.hn, dir);
+  if (!(cs > 0.0f)) return false;
+  const float p = (1.0f - g.guide_fraction) * cs / kPiF + g.guide_fraction * mix_pdf(mix, dir);
+  ln.ro = ln.hp;
+  ln.rd = dir;
+  ln.thr = ln.thr * ln.alb * (cs / (kPiF * p));
+  ln.include_emission = false;
+  ln.bsdf_pdf = p;
+  return true;
+}
+
 template <int kMode, bool kMoments, bool kBatch>
 __device__ __forceinline__ void shade_hit(const RenderLaunch& L, const FrameJob& J, Lane& ln, const TraceResult& tr,
                                           uint32_t& n_paths) {
@@ -839,30 +864,12 @@ __global__ void __launch_bounds__(256) render_kernel(const RenderLaunch L) {
           }
           if constexpr (kMode == kModeGuided) {
             if (ln.mix_slot >= 0) {
-              // One-sample MIS of BSDF and guide sampling (the balance heuristic = the mixture
-              // pdf, guide taken with probability guide_fraction), so the estimator stays
-              // unbiased whatever the network predicts.
               const float4* mix = L.g.in_mix + 10 * size_t(ln.mix_slot);
-              const float ut = ln.rng.uniform();
-              V3 dir;
-              if (ut < 1.0f - L.g.guide_fraction) {
-                dir = cosine_direction(ln);
-              } else {
-                const float a = ln.rng.uniform(), b = ln.rng.uniform(), c = ln.rng.uniform();
-                dir = mix_sample(mix, a, b, c);
-              }
-              const float cs = dot(ln.hn, dir);
               ln.mix_slot = -1;
-              if (!(cs > 0.0f)) {
+              if (!take_guided_bounce(L.g, mix, ln)) {
                 finish_sample<kMode, kMoments>(L, J, ln, n_paths);
                 break;
               }
-              const float p = (1.0f - L.g.guide_fraction) * cs / kPiF + L.g.guide_fraction * mix_pdf(mix, dir);
-              ln.ro = ln.hp;
-              ln.rd = dir;
-              ln.thr = ln.thr * ln.alb * (cs / (kPiF * p));
-              ln.include_emission = false;
-              ln.bsdf_pdf = p;
               ln.phase = kExtend;
               break;
             }
@@ -1082,7 +1089,7 @@ __device__ __forceinline__ uint32_t warp_append(uint32_t* counter, bool pred) {
   return base + uint32_t(__popc(m & lanes_below()));
 }
 
-template <bool kMoments>
+template <bool kMoments, bool kGuided>
 __global__ void __launch_bounds__(256) wf_logic_kernel(const WavefrontLaunch W) {
   const FrameJob& J = W.r.f;
   const DevScene& s = J.scene;
@@ -1150,7 +1157,25 @@ __global__ void __launch_bounds__(256) wf_logic_kernel(const WavefrontLaunch W) 
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
       const uint32_t pos = warp_append(W.q + kWfMatCount + k, kind == k);
-      if (kind == k) W.mat_q[size_t(k) * W.capacity + pos] = slot;
+      if (kind == k) {
+        W.mat_q[size_t(k) * W.capacity + pos] = slot;
+        if constexpr (kGuided) {
+          if (k == kDiffuse) {
+            // The query of the guide's inference launch, at the vertex's place in the diffuse
+            // queue: the surface point and shading normal the shade launch will scatter from.
+            // Vertices that only do next-event estimation (depth 1) get a query too, unused.
+            const uint4 h = W.hit[slot];
+            const float4 o4 = W.ray_o[slot], d4 = W.ray_d[slot];
+            TraceResult tr;
+            tr.t = __uint_as_float(h.x);
+            tr.rec = h.y;
+            tr.tag = h.z;
+            const Surface f = surface_at(s, mk(o4.x, o4.y, o4.z), mk(d4.x, d4.y, d4.z), tr);
+            W.query[2 * size_t(pos)] = make_float4(f.hp.x, f.hp.y, f.hp.z, 0.0f);
+            W.query[2 * size_t(pos) + 1] = make_float4(f.nrm.x, f.nrm.y, f.nrm.z, 0.0f);
+          }
+        }
+      }
     }
     // Free slots start new camera paths: consecutive work items are consecutive pixels of one
     // sample, so a warp's new rays are neighbours.
@@ -1194,6 +1219,7 @@ __global__ void __launch_bounds__(256) wf_logic_kernel(const WavefrontLaunch W) 
   }
 }
 
+template <bool kGuided>
 __global__ void __launch_bounds__(128) wf_shade_kernel(const WavefrontLaunch W) {
   const FrameJob& J = W.r.f;
   const DevScene& s = J.scene;
@@ -1243,13 +1269,17 @@ __global__ void __launch_bounds__(128) wf_shade_kernel(const WavefrontLaunch W) 
         ln.hp = f.hp;
         ln.hn = f.nrm;
         ln.alb = base_color(s, m, f.tu, f.tv);
+        // Guided: a vertex that will scatter (depth > 1) uses the mixture inferred for its place i
+        // in the diffuse queue, in the environment NEE weight and in the bounce, as render_kernel's
+        // guided mode does.
+        ln.mix_slot = (kGuided && ln.depth > 1) ? int(i) : -1;
         if (prepare_light_shadow(s, ln)) {
           shadow_l = true;
           sl0 = make_float4(ln.ro.x, ln.ro.y, ln.ro.z, ln.tmax);
           sl1 = make_float4(ln.rd.x, ln.rd.y, ln.rd.z, __uint_as_float(2u * slot));
           c0 = make_float4(ln.pend.x, ln.pend.y, ln.pend.z, 0.0f);
         }
-        if (prepare_env_shadow<kModePlain>(W.r, J, ln)) {
+        if (prepare_env_shadow<kGuided ? kModeGuided : kModePlain>(W.r, J, ln)) {
           shadow_e = true;
           se0 = make_float4(ln.ro.x, ln.ro.y, ln.ro.z, ln.tmax);
           se1 = make_float4(ln.rd.x, ln.rd.y, ln.rd.z, __uint_as_float(2u * slot + 1u));
@@ -1260,9 +1290,13 @@ __global__ void __launch_bounds__(128) wf_shade_kernel(const WavefrontLaunch W) 
         nst |= kWfNeePending;
         ln.depth -= 1;
         if (ln.depth > 0) {
-          take_diffuse_bounce(ln, cosine_direction(ln));
+          if (kGuided && ln.mix_slot >= 0) {
+            extend = take_guided_bounce(W.r.g, W.r.g.in_mix + 10 * size_t(ln.mix_slot), ln);
+          } else {
+            take_diffuse_bounce(ln, cosine_direction(ln));
+            extend = true;
+          }
           bsdf_pdf = ln.bsdf_pdf;
-          extend = true;
         }
       } else {
         const bool on = kind == kMetal ? bounce_metal(ln, m, f) : (bounce_dielectric(ln, m, f), true);
@@ -1417,16 +1451,28 @@ static int resident_blocks(K kernel, int block) {
   return blocks > 0 ? blocks : 1;
 }
 
-cudaError_t launch_wavefront_iteration(const WavefrontLaunch& w, bool moments, int sm_count, cudaStream_t stream) {
-  static const int shade_per_sm = resident_blocks(wf_shade_kernel, 128);
+cudaError_t launch_wavefront_iteration(const WavefrontLaunch& w, bool moments, int sm_count, cudaStream_t stream,
+                                       const GuideDevice* guide) {
+  static const int shade_per_sm = resident_blocks(wf_shade_kernel<false>, 128);
+  static const int guided_shade_per_sm = resident_blocks(wf_shade_kernel<true>, 128);
   static const int trace_per_sm = resident_blocks(wf_trace_kernel<false, false>, 128);
   static const int refill_per_sm = resident_blocks(wf_trace_kernel<true, false>, 128);
   static const int watertight_per_sm = resident_blocks(wf_trace_kernel<false, true>, 128);
   const unsigned logic_grid =
       unsigned(std::min<uint64_t>((uint64_t(w.capacity) + 255) / 256, uint64_t(sm_count) * 8));
-  if (moments) wf_logic_kernel<true><<<logic_grid, 256, 0, stream>>>(w);
-  else wf_logic_kernel<false><<<logic_grid, 256, 0, stream>>>(w);
-  wf_shade_kernel<<<shade_per_sm * sm_count, 128, 0, stream>>>(w);
+  if (guide) {
+    // Guided: the diffuse queue's queries are inferred between the logic and shade launches.
+    if (moments) wf_logic_kernel<true, true><<<logic_grid, 256, 0, stream>>>(w);
+    else wf_logic_kernel<false, true><<<logic_grid, 256, 0, stream>>>(w);
+    cudaError_t e = guide_launch_infer(*guide, w.query, w.capacity, const_cast<float4*>(w.r.g.in_mix), sm_count,
+                                       stream, w.q + kWfMatCount);
+    if (e != cudaSuccess) return e;
+    wf_shade_kernel<true><<<guided_shade_per_sm * sm_count, 128, 0, stream>>>(w);
+  } else {
+    if (moments) wf_logic_kernel<true, false><<<logic_grid, 256, 0, stream>>>(w);
+    else wf_logic_kernel<false, false><<<logic_grid, 256, 0, stream>>>(w);
+    wf_shade_kernel<false><<<shade_per_sm * sm_count, 128, 0, stream>>>(w);
+  }
   if (w.r.f.scene.tri_verts) wf_trace_kernel<false, true><<<watertight_per_sm * sm_count, 128, 0, stream>>>(w);
   else if (w.refill_lanes > 1) wf_trace_kernel<true, false><<<refill_per_sm * sm_count, 128, 0, stream>>>(w);
   else wf_trace_kernel<false, false><<<trace_per_sm * sm_count, 128, 0, stream>>>(w);
