@@ -13,6 +13,12 @@ widen its own band by itself. Reported:
 
 Luminance variances are bounded by the perfectly correlated case, (sum_c w_c sigma_c)^2, because
 only per-channel sums of squares are kept and the channels of one path are strongly correlated.
+
+The oracle returns its means as FP32 sums of FP32 samples, so a pixel whose samples are all
+nearly equal can show a sample variance of zero (cancellation) while its two means differ by
+accumulation rounding. The variance of the difference therefore includes that rounding, taken as
+4e-6 of each mean (the FP32 error of a 4,096-term sum); only pixels that are zero on both sides
+are required to agree exactly.
 """
 
 from __future__ import annotations
@@ -20,6 +26,7 @@ from __future__ import annotations
 import numpy as np
 
 LUMA = np.array([0.2126, 0.7152, 0.0722])
+FP32_SUM_ERROR = 4e-6
 
 
 def sample_variance(mean: np.ndarray, sumsq: np.ndarray, n: int) -> np.ndarray:
@@ -38,11 +45,12 @@ def compare(g_mean, g_var, n_g, o_mean, o_var, n_o, block: int = 2) -> dict:
     """Parity statistics of two (height, width, 3) mean images with their sample variances."""
     g_mean = g_mean.astype(np.float64)
     o_mean = o_mean.astype(np.float64)
-    var = g_var / n_g + o_var / n_o  # variance of the difference of the two means
+    # Variance of the difference of the two means, plus the FP32 rounding of the means themselves.
+    var = g_var / n_g + o_var / n_o + (FP32_SUM_ERROR * g_mean) ** 2 + (FP32_SUM_ERROR * o_mean) ** 2
     diff = g_mean - o_mean
     flat = var <= 0.0
-    # Pixels whose samples were all equal on both sides must agree (black pixels, a constant sky).
-    const_bad = int(np.sum(np.abs(diff[flat]) > 1e-5 * np.maximum(1.0, np.abs(o_mean[flat]))))
+    # Pixels that are zero on both sides (black) must agree exactly.
+    const_bad = int(np.sum(diff[flat] != 0.0))
     z = diff[~flat] / np.sqrt(var[~flat])
     sd_l = np.sqrt(var) @ LUMA  # per-pixel luminance standard deviation bound
     d_l = diff @ LUMA
