@@ -265,7 +265,7 @@ def run_ours(args):
     barrier()
     torch.cuda.synchronize()
     clocks.start()
-    step_ms, kernel_ms, rays = [], [], []
+    step_ms, kernel_ms, rays, launches = [], [], [], 0
     for k in range(args.steps):
         with torch.cuda.stream(stream):
             flush.zero_()
@@ -279,6 +279,7 @@ def run_ours(args):
         st = r.stats()
         kernel_ms.append(st["kernel_ms"])
         rays.append(st["rays"])
+        launches += st["kernel_launches"]
     torch.cuda.synchronize()
     clk = clocks.stop()
     barrier()
@@ -354,7 +355,7 @@ def run_ours(args):
             "kernel_ms": mean_kernel_ms,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
                     "timing": "host clock over K steps of upload + render + readback"},
-            "gpu_launches": args.steps,
+            "gpu_launches": launches,
             "clocks": clk,
         }
         if roofline is not None:

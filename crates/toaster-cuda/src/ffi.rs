@@ -154,6 +154,10 @@ pub struct TcStats {
     pub bvh_depth: u32,
     /// Device status word.
     pub status_flags: u32,
+    /// Kernel launches of the last render call.
+    pub kernel_launches: u32,
+    /// Padding.
+    pub _pad0: u32,
 }
 
 /// Opaque `tc_context`.

@@ -180,6 +180,9 @@ typedef struct tc_stats {
   float total_ms;            /* device time of the whole call including copies */
   uint32_t bvh_depth;        /* deepest leaf of the uploaded hierarchy */
   uint32_t status_flags;     /* device status word (0 = clean) */
+  uint32_t kernel_launches;  /* this library's kernel launches of the last render call (path kernels,
+                                guide inference; not memsets or copies) */
+  uint32_t _pad0;
 } tc_stats;
 
 typedef struct tc_context tc_context;

@@ -815,6 +815,7 @@ static int run_wavefront(tc_context* ctx, const tcb::RenderLaunch& L, uint32_t s
     if (it > bound) return fail(ctx, TC_ERR_DEVICE_STATUS, "wavefront render did not drain its paths");
     TC_CUDA(ctx, cudaMemsetAsync(w.q, 0, sizeof(uint32_t) * tcb::kWfCounters, st));
     TC_CUDA(ctx, tcb::launch_wavefront_iteration(w, moments, ctx->sm_count, st, guided ? &ctx->guide : nullptr));
+    ctx->stats.kernel_launches += guided ? 4u : 3u;
     const int k = int(it % kWfRing);
     TC_CUDA(ctx, cudaMemcpyAsync(ctx->wf_live_host + k, w.q + tcb::kWfLive, sizeof(uint32_t), cudaMemcpyDeviceToHost,
                                  st));
@@ -849,6 +850,7 @@ static int enqueue_render(tc_context* ctx, const tc_gpu_render_params* p, const 
   if (o.refill_lanes > 32) return fail(ctx, TC_ERR_INVALID, "refill_lanes must be at most 32");
   if (timing) TC_CUDA(ctx, cudaEventRecord(ctx->ev_begin, st));
   if (int rc = prepare_accumulation(ctx, p, moments, st)) return rc;
+  ctx->stats.kernel_launches = 0;
 
   tcb::RenderLaunch L{};
   L.f.scene = ctx->scene;
@@ -916,6 +918,7 @@ static int enqueue_render(tc_context* ctx, const tc_gpu_render_params* p, const 
       return rc;
   } else if (mode != tcb::kModeGuided) {
     TC_CUDA(ctx, tcb::launch_render(L, block, grid, moments, st, mode));
+    ctx->stats.kernel_launches = 1;
   } else {
     // Wavefront: waves of whole samples per pixel; within a wave, rounds of (path kernel ->
     // suspended diffuse vertices -> tensor-core inference of their mixtures -> resume). Counts
@@ -947,6 +950,7 @@ static int enqueue_render(tc_context* ctx, const tc_gpu_render_params* p, const 
       R.g.out_count = counts;
       TC_CUDA(ctx, cudaMemsetAsync(ctx->work_counter.ptr, 0, sizeof(unsigned long long), st));
       TC_CUDA(ctx, tcb::launch_render(R, block, grid, moments, st, mode));
+      ctx->stats.kernel_launches += 1 + 2 * rounds;
       for (uint32_t r = 0; r < rounds; ++r) {
         std::swap(state_in, state_out);
         TC_CUDA(ctx, tcb::guide_launch_infer(ctx->guide, ctx->w_query.as<float4>(), cap, ctx->w_mix.as<float4>(),
@@ -1100,8 +1104,10 @@ int tc_render_batch(tc_context* const* contexts, const tc_gpu_render_params* par
   if (per_sm <= 0) return fail(lead, TC_ERR_CUDA, "batched render kernel cannot be resident with this block size");
   const int grid = per_sm * lead->sm_count;
   TC_CUDA(lead, cudaEventRecord(lead->ev_kernel0, st));
+  lead->stats.kernel_launches = 0;
   if (!o.guiding) {
     TC_CUDA(lead, tcb::launch_render_batch(L, block, grid, st));
+    lead->stats.kernel_launches = 1;
   } else {
     // Rounds of (batched path kernel -> each frame's network infers its frame's queries -> prefix
     // of the per-frame counts -> batched resume), as the single-frame guided wavefront does.
@@ -1133,6 +1139,7 @@ int tc_render_batch(tc_context* const* contexts, const tc_gpu_render_params* par
       R.g.job_out_count = counts;
       TC_CUDA(lead, cudaMemsetAsync(lead->work_counter.ptr, 0, sizeof(unsigned long long), st));
       TC_CUDA(lead, tcb::launch_render_batch(R, block, grid, st, true));
+      lead->stats.kernel_launches += 1 + rounds * uint32_t(n + 2);
       for (uint32_t r = 0; r < rounds; ++r) {
         std::swap(state_in, state_out);
         for (size_t i = 0; i < n; ++i)

@@ -149,6 +149,8 @@ class Stats(ctypes.Structure):
         ("total_ms", ctypes.c_float),
         ("bvh_depth", ctypes.c_uint32),
         ("status_flags", ctypes.c_uint32),
+        ("kernel_launches", ctypes.c_uint32),
+        ("_pad0", ctypes.c_uint32),
     ]
 
 
