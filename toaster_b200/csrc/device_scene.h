@@ -120,6 +120,9 @@ constexpr uint32_t kWfExtPending = 1u << 25;     // its extension ray is queued 
 constexpr uint32_t kWfNeePending = 1u << 26;     // its two shadow-ray contributions are to be added
 constexpr uint32_t kWfTerminate = 1u << 27;      // the path ends once its contributions are added
 constexpr uint32_t kWfEmission = 1u << 28;       // emission seen by the extension ray counts
+// Material word of an extension hit (hit.w): material index in the low bits, kind on top.
+constexpr uint32_t kWfKindShift = 28;
+constexpr uint32_t kWfMaterialMask = (1u << kWfKindShift) - 1u;
 // Queue counters (uint32 each), cleared before every iteration.
 enum WfCounter : int {
   kWfExtCount = 0, kWfShadowCount = 1, kWfMatCount = 2,  // [2..4]: diffuse, metal, dielectric
@@ -135,7 +138,7 @@ struct WavefrontLaunch {
   float4* thr;           // (throughput.xyz, pixel)
   float4* rad;           // (radiance.xyz, -)
   uint4* rng;            // PCG32 state and increment
-  uint4* hit;            // (t bits, primitive record or kNoNode, tag, -) of the extension ray
+  uint4* hit;            // (t bits, primitive record or kNoNode, tag, material word) of the extension ray
   float4* nee;           // 2 per slot: light and environment shadow-ray contributions
   float4* shadow_q;      // 2 per entry: (origin.xyz, tmax), (direction.xyz, target nee index)
   uint32_t* ext_q;       // slots whose extension ray is to be traced

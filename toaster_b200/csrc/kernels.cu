@@ -1077,52 +1077,76 @@ int render_max_blocks_per_sm(int block_size, bool moments, int mode, int short_s
 
 __device__ __forceinline__ unsigned lanes_below() { return (1u << (threadIdx.x & 31u)) - 1u; }
 
-// Appends the lanes whose `pred` holds to a queue counter with one atomic per warp; returns each
-// such lane's position. Every lane of the warp must call it together.
-__device__ __forceinline__ uint32_t warp_append(uint32_t* counter, bool pred) {
+// Appends the threads of the block whose `pred` holds to a queue counter with one atomic per
+// block (all the block's warps append to the same few counters in every launch, so per-warp atomics
+// would queue up at those addresses); returns each such thread's position. Every thread of the
+// block (at most kWfBlock threads) must call it together; `sh` is kWfBlock / 32 + 1 words of
+// shared memory.
+constexpr int kWfBlock = 256;
+__device__ __forceinline__ uint32_t block_append(uint32_t* counter, bool pred, uint32_t* sh) {
   const unsigned m = __ballot_sync(0xffffffffu, pred);
-  if (!m) return 0u;
-  const int leader = __ffs(m) - 1;
-  uint32_t base = 0;
-  if (int(threadIdx.x & 31u) == leader) base = atomicAdd(counter, uint32_t(__popc(m)));
-  base = __shfl_sync(0xffffffffu, base, leader);
-  return base + uint32_t(__popc(m & lanes_below()));
+  const int warp = int(threadIdx.x >> 5);
+  if ((threadIdx.x & 31u) == 0) sh[warp] = uint32_t(__popc(m));
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    uint32_t run = 0;
+    for (int w = 0; w < int(blockDim.x >> 5); ++w) {
+      const uint32_t c = sh[w];
+      sh[w] = run;
+      run += c;
+    }
+    sh[kWfBlock / 32] = run ? atomicAdd(counter, run) : 0u;
+  }
+  __syncthreads();
+  const uint32_t pos = sh[kWfBlock / 32] + sh[warp] + uint32_t(__popc(m & lanes_below()));
+  __syncthreads();  // sh is reused by the next call
+  return pos;
 }
 
 template <bool kMoments, bool kGuided>
-__global__ void __launch_bounds__(256) wf_logic_kernel(const WavefrontLaunch W) {
+__global__ void __launch_bounds__(kWfBlock) wf_logic_kernel(const WavefrontLaunch W) {
+  __shared__ uint32_t sh[kWfBlock / 32 + 1];
+  __shared__ unsigned long long s_first;
   const FrameJob& J = W.r.f;
   const DevScene& s = J.scene;
   const uint32_t npix = J.width * J.height;
-  const uint32_t stride = gridDim.x * blockDim.x;
   uint32_t n_paths = 0, n_live = 0;
-  // The loop bound is uniform across the block, so whole warps run every iteration together.
-  for (uint32_t base = blockIdx.x * blockDim.x; base < W.capacity; base += stride) {
-    const uint32_t slot = base + threadIdx.x;
+  // One slot per thread; whole warps are either in range or the last partial warp.
+  {
+    const uint32_t slot = blockIdx.x * blockDim.x + threadIdx.x;
     const bool valid = slot < W.capacity;
     const uint32_t st = valid ? W.state[slot] : 0u;
     bool free_slot = valid && !(st & kWfAlive);
     int kind = -1;
     if (st & kWfAlive) {
+      // Every load this slot may need is issued before any result is used: the state word alone
+      // decides which of them matter.
       const float4 r4 = W.rad[slot];
       const float4 t4 = W.thr[slot];
+      const bool nee_pending = (st & kWfNeePending) != 0u;
+      const bool ext = (st & (kWfTerminate | kWfExtPending)) == kWfExtPending;
+      float4 na = make_float4(0.f, 0.f, 0.f, 0.f), nb = na;
+      uint4 h = make_uint4(0u, kNoNode, 0u, 0u);
+      if (nee_pending) {
+        na = W.nee[2 * size_t(slot)];
+        nb = W.nee[2 * size_t(slot) + 1];
+      }
+      if (ext) h = W.hit[slot];
       V3 rad = mk(r4.x, r4.y, r4.z);
       const V3 thr = mk(t4.x, t4.y, t4.z);
-      if (st & kWfNeePending) {
-        const float4 a = W.nee[2 * size_t(slot)], b = W.nee[2 * size_t(slot) + 1];
-        rad = rad + mk(a.x, a.y, a.z);
-        rad = rad + mk(b.x, b.y, b.z);
+      if (nee_pending) {
+        rad = rad + mk(na.x, na.y, na.z);
+        rad = rad + mk(nb.x, nb.y, nb.z);
       }
       bool done = (st & kWfTerminate) != 0u;
-      if (!done && (st & kWfExtPending)) {
-        const uint4 h = W.hit[slot];
+      if (ext) {
         if (h.y == kNoNode) {
           const float4 d4 = W.ray_d[slot];
           rad = rad + thr * background(s, mk(d4.x, d4.y, d4.z), W.ray_o[slot].w);
           done = true;
         } else {
-          const uint32_t mat = __float_as_uint(__ldg(&s.prims[h.y].b[3]));
-          const uint32_t k = __ldg(&s.materials[mat].kind);
+          const uint32_t mat = h.w & kWfMaterialMask;
+          const uint32_t k = h.w >> kWfKindShift;
           if (k == kEmissive) {
             if (st & kWfEmission) {
               const DevMaterial& m = s.materials[mat];
@@ -1156,7 +1180,7 @@ __global__ void __launch_bounds__(256) wf_logic_kernel(const WavefrontLaunch W) 
     // Paths that go on join the queue of their material (the shade launch rewrites their state).
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
-      const uint32_t pos = warp_append(W.q + kWfMatCount + k, kind == k);
+      const uint32_t pos = block_append(W.q + kWfMatCount + k, kind == k, sh);
       if (kind == k) {
         W.mat_q[size_t(k) * W.capacity + pos] = slot;
         if constexpr (kGuided) {
@@ -1178,14 +1202,25 @@ __global__ void __launch_bounds__(256) wf_logic_kernel(const WavefrontLaunch W) 
       }
     }
     // Free slots start new camera paths: consecutive work items are consecutive pixels of one
-    // sample, so a warp's new rays are neighbours.
-    const unsigned want = __ballot_sync(0xffffffffu, free_slot);
+    // sample, so a warp's new rays are neighbours. One atomic on the work counter per block.
     bool started = false;
-    if (want) {
-      const int leader = __ffs(want) - 1;
-      unsigned long long first = 0;
-      if (int(threadIdx.x & 31u) == leader) first = atomicAdd(W.r.work_counter, (unsigned long long)__popc(want));
-      first = __shfl_sync(0xffffffffu, first, leader);
+    {
+      const unsigned want = __ballot_sync(0xffffffffu, free_slot);
+      const int warp = int(threadIdx.x >> 5);
+      if ((threadIdx.x & 31u) == 0) sh[warp] = uint32_t(__popc(want));
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        uint32_t run = 0;
+        for (int w = 0; w < int(blockDim.x >> 5); ++w) {
+          const uint32_t c = sh[w];
+          sh[w] = run;
+          run += c;
+        }
+        s_first = run ? atomicAdd(W.r.work_counter, (unsigned long long)run) : 0ull;
+      }
+      __syncthreads();
+      const unsigned long long first = s_first + sh[warp];
+      __syncthreads();
       if (free_slot) {
         const uint64_t item = first + __popc(want & lanes_below());
         if (item < W.r.total_items) {
@@ -1207,15 +1242,28 @@ __global__ void __launch_bounds__(256) wf_logic_kernel(const WavefrontLaunch W) 
         }
       }
     }
-    const uint32_t pos = warp_append(W.q + kWfExtCount, started);
+    const uint32_t pos = block_append(W.q + kWfExtCount, started, sh);
     if (started) W.ext_q[pos] = slot;
     n_live += (kind >= 0 || started) ? 1u : 0u;
   }
+  // Path and live-slot counts: one atomic per block each.
+  __shared__ unsigned long long s_paths;
+  __shared__ uint32_t s_live;
+  if (threadIdx.x == 0) {
+    s_paths = 0ull;
+    s_live = 0u;
+  }
+  __syncthreads();
   const unsigned long long tp = __reduce_add_sync(0xffffffffu, n_paths);
   const uint32_t tl = __reduce_add_sync(0xffffffffu, n_live);
   if ((threadIdx.x & 31u) == 0) {
-    if (tp) atomicAdd(W.r.counters, tp);
-    if (tl) atomicAdd(W.q + kWfLive, tl);
+    if (tp) atomicAdd(&s_paths, tp);
+    if (tl) atomicAdd(&s_live, tl);
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    if (s_paths) atomicAdd(W.r.counters, s_paths);
+    if (s_live) atomicAdd(W.q + kWfLive, s_live);
   }
 }
 
@@ -1223,13 +1271,15 @@ template <bool kGuided>
 __global__ void __launch_bounds__(128) wf_shade_kernel(const WavefrontLaunch W) {
   const FrameJob& J = W.r.f;
   const DevScene& s = J.scene;
+  __shared__ uint32_t sh[kWfBlock / 32 + 1];
   const uint32_t n0 = W.q[kWfMatCount], n1 = W.q[kWfMatCount + 1], n2 = W.q[kWfMatCount + 2];
   const uint32_t total = n0 + n1 + n2;
   const uint32_t stride = gridDim.x * blockDim.x;
   // Entries are numbered diffuse, then metal, then dielectric, and a warp takes 32 consecutive
-  // ones, so all but the warps at the two boundaries shade a single material.
-  for (uint32_t base = blockIdx.x * blockDim.x + (threadIdx.x & ~31u); base < total; base += stride) {
-    const uint32_t i = base + (threadIdx.x & 31u);
+  // ones, so all but the warps at the two boundaries shade a single material. The loop bound is
+  // uniform across the block (its appends synchronise the block).
+  for (uint32_t base = blockIdx.x * blockDim.x; base < total; base += stride) {
+    const uint32_t i = base + threadIdx.x;
     const bool valid = i < total;
     uint32_t slot = 0, kind = 0;
     if (valid) {
@@ -1313,17 +1363,17 @@ __global__ void __launch_bounds__(128) wf_shade_kernel(const WavefrontLaunch W) 
                                uint32_t(ln.rng.inc >> 32));
       W.state[slot] = nst;
     }
-    const uint32_t pl = warp_append(W.q + kWfShadowCount, shadow_l);
+    const uint32_t pl = block_append(W.q + kWfShadowCount, shadow_l, sh);
     if (shadow_l) {
       W.shadow_q[2 * size_t(pl)] = sl0;
       W.shadow_q[2 * size_t(pl) + 1] = sl1;
     }
-    const uint32_t pe = warp_append(W.q + kWfShadowCount, shadow_e);
+    const uint32_t pe = block_append(W.q + kWfShadowCount, shadow_e, sh);
     if (shadow_e) {
       W.shadow_q[2 * size_t(pe)] = se0;
       W.shadow_q[2 * size_t(pe) + 1] = se1;
     }
-    const uint32_t px = warp_append(W.q + kWfExtCount, extend);
+    const uint32_t px = block_append(W.q + kWfExtCount, extend, sh);
     if (extend) W.ext_q[px] = slot;
   }
 }
@@ -1345,11 +1395,21 @@ __device__ __forceinline__ RayQ wf_entry_ray(const WavefrontLaunch& W, uint32_t 
 }
 
 // Result of queue entry i: the closest hit of an extension ray, or the occlusion of a shadow ray
-// (an occluded shadow ray drops its contribution, integrator.rs:196-199 and :233-238).
+// (an occluded shadow ray drops its contribution, integrator.rs:196-199 and :233-238). An extension
+// hit also records its material (index in bits 0-27, kind in bits 28-31), which the primitive
+// record just tested holds, so the logic launch needs no dependent loads to classify the slot.
 __device__ __forceinline__ void wf_entry_result(const WavefrontLaunch& W, uint32_t i, uint32_t n_ext, uint32_t target,
                                                 bool hit, float t, uint32_t rec, uint32_t tag) {
-  if (i < n_ext) W.hit[target] = make_uint4(__float_as_uint(t), hit ? rec : kNoNode, hit ? tag : 0u, 0u);
-  else if (hit) W.nee[target] = make_float4(0.f, 0.f, 0.f, 0.f);
+  if (i < n_ext) {
+    uint32_t mat = 0u;
+    if (hit) {
+      const uint32_t m = __float_as_uint(__ldg(&W.r.f.scene.prims[rec].b[3]));
+      mat = m | (__ldg(&W.r.f.scene.materials[m].kind) << kWfKindShift);
+    }
+    W.hit[target] = make_uint4(__float_as_uint(t), hit ? rec : kNoNode, hit ? tag : 0u, mat);
+  } else if (hit) {
+    W.nee[target] = make_float4(0.f, 0.f, 0.f, 0.f);
+  }
 }
 
 // kRefill = false: a warp takes 32 consecutive queue entries and traces each to its end.
@@ -1458,19 +1518,18 @@ cudaError_t launch_wavefront_iteration(const WavefrontLaunch& w, bool moments, i
   static const int trace_per_sm = resident_blocks(wf_trace_kernel<false, false>, 128);
   static const int refill_per_sm = resident_blocks(wf_trace_kernel<true, false>, 128);
   static const int watertight_per_sm = resident_blocks(wf_trace_kernel<false, true>, 128);
-  const unsigned logic_grid =
-      unsigned(std::min<uint64_t>((uint64_t(w.capacity) + 255) / 256, uint64_t(sm_count) * 8));
+  const unsigned logic_grid = unsigned((uint64_t(w.capacity) + kWfBlock - 1) / kWfBlock);
   if (guide) {
     // Guided: the diffuse queue's queries are inferred between the logic and shade launches.
-    if (moments) wf_logic_kernel<true, true><<<logic_grid, 256, 0, stream>>>(w);
-    else wf_logic_kernel<false, true><<<logic_grid, 256, 0, stream>>>(w);
+    if (moments) wf_logic_kernel<true, true><<<logic_grid, kWfBlock, 0, stream>>>(w);
+    else wf_logic_kernel<false, true><<<logic_grid, kWfBlock, 0, stream>>>(w);
     cudaError_t e = guide_launch_infer(*guide, w.query, w.capacity, const_cast<float4*>(w.r.g.in_mix), sm_count,
                                        stream, w.q + kWfMatCount);
     if (e != cudaSuccess) return e;
     wf_shade_kernel<true><<<guided_shade_per_sm * sm_count, 128, 0, stream>>>(w);
   } else {
-    if (moments) wf_logic_kernel<true, false><<<logic_grid, 256, 0, stream>>>(w);
-    else wf_logic_kernel<false, false><<<logic_grid, 256, 0, stream>>>(w);
+    if (moments) wf_logic_kernel<true, false><<<logic_grid, kWfBlock, 0, stream>>>(w);
+    else wf_logic_kernel<false, false><<<logic_grid, kWfBlock, 0, stream>>>(w);
     wf_shade_kernel<false><<<shade_per_sm * sm_count, 128, 0, stream>>>(w);
   }
   if (w.r.f.scene.tri_verts) wf_trace_kernel<false, true><<<watertight_per_sm * sm_count, 128, 0, stream>>>(w);
