@@ -116,8 +116,10 @@ pub struct TcRenderOptions {
     pub refill_lanes: u32,
     /// Guided renders: probability of sampling the network's mixture.
     pub guide_fraction: f32,
-    /// Plain renders: 0 automatic, 1 megakernel, 2 wavefront.
+    /// Plain and guided renders: 0 automatic, 1 megakernel, 2 wavefront.
     pub schedule: u32,
+    /// Wavefront: 0 default, 1 no ray sorting, 2 rays sorted before tracing.
+    pub ray_sort: u32,
 }
 
 /// `tc_scene_changes`, the `SceneChanges` of an evaluated frame.

@@ -165,6 +165,10 @@ typedef struct tc_render_options {
                                 between logic and shading), wave_paths slots (0 = 2^22). Recording
                                 renders, batched launches and captured animation frames use the
                                 megakernel. */
+  uint32_t ray_sort;         /* wavefront schedule: sort each iteration's queued rays by kind, direction
+                                octant and the leaf-order bucket of their origin's primitive before
+                                tracing (three small launches), so a warp's rays start near each other
+                                and head the same way. 0 = library default (off), 1 = off, 2 = on */
 } tc_render_options;
 #define TC_SCHEDULE_AUTO 0u
 #define TC_SCHEDULE_MEGAKERNEL 1u

@@ -20,12 +20,13 @@ pytestmark = pytest.mark.gpu
 
 
 def render_both(renderer, samples, max_bounces=None, keep_moments=False, wave_paths=0, refill_lanes=0,
-                frame_index=3):
+                frame_index=3, ray_sort=0):
     out = {}
     for schedule in ("megakernel", "wavefront"):
         renderer.render(samples=samples, max_bounces=max_bounces, frame_index=frame_index, keep_moments=keep_moments,
                         schedule=schedule, wave_paths=wave_paths,
-                        refill_lanes=refill_lanes if schedule == "wavefront" else 0)
+                        refill_lanes=refill_lanes if schedule == "wavefront" else 0,
+                        ray_sort=ray_sort if schedule == "wavefront" else 0)
         s, q, n = renderer.readback_sums(moments=keep_moments)
         out[schedule] = (s, q, renderer.stats())
     return out
@@ -79,6 +80,14 @@ def test_wavefront_dynamic_ray_fetching(renderer, refill_lanes):
     scene = configs.mixed(width=64, height=36)
     renderer.upload(scene_to_gpu(scene))
     assert_same_paths(render_both(renderer, 16, refill_lanes=refill_lanes), scene, 16)
+
+
+@pytest.mark.parametrize("wave_paths", [0, 1000])
+def test_wavefront_sorted_rays(renderer, wave_paths):
+    # Sorting the queued rays changes the order in which they are traced, not the rays.
+    scene = configs.mixed(width=96, height=54)
+    renderer.upload(scene_to_gpu(scene))
+    assert_same_paths(render_both(renderer, 32, wave_paths=wave_paths, ray_sort=2), scene, 32)
 
 
 def test_wavefront_progressive_batches(renderer):

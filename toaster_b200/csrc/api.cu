@@ -141,6 +141,7 @@ struct tc_context {
   // ring of live-slot counts with one event per entry (the host's drain check).
   uint32_t wf_capacity = 0;
   DevBuf wf_state, wf_ray_o, wf_ray_d, wf_thr, wf_rad, wf_rng, wf_hit, wf_nee, wf_shadow_q, wf_ext_q, wf_mat_q, wf_q;
+  DevBuf wf_ext_key, wf_shadow_key, wf_sort_counts, wf_sorted;
   uint32_t* wf_live_host = nullptr;
   cudaEvent_t wf_events[kWfRing] = {};
 
@@ -759,7 +760,7 @@ int tc_set_camera(tc_context* ctx, const tc_gpu_camera* cam) {
 // behind the last one it enqueued, for the live-slot count of an earlier iteration, so the GPU
 // always has queued work; the iterations launched after the last path finished find nothing to do.
 static int run_wavefront(tc_context* ctx, const tcb::RenderLaunch& L, uint32_t slots, uint32_t max_bounces,
-                         int refill_lanes, bool moments, bool guided, cudaStream_t st) {
+                         int refill_lanes, bool moments, bool guided, bool sort_rays, cudaStream_t st) {
   const uint64_t items = L.total_items;
   const uint32_t cap = uint32_t(std::max<uint64_t>(32, std::min<uint64_t>(slots, items)));
   if (cap != ctx->wf_capacity) {
@@ -800,6 +801,17 @@ static int run_wavefront(tc_context* ctx, const tcb::RenderLaunch& L, uint32_t s
   w.mat_q = ctx->wf_mat_q.as<uint32_t>();
   w.q = ctx->wf_q.as<uint32_t>();
   w.refill_lanes = refill_lanes;
+  w.prim_count = ctx->bvh_prims;
+  if (sort_rays) {
+    TC_CUDA(ctx, ctx->wf_ext_key.reserve(sizeof(uint32_t) * size_t(cap)));
+    TC_CUDA(ctx, ctx->wf_shadow_key.reserve(2 * sizeof(uint32_t) * size_t(cap)));
+    TC_CUDA(ctx, ctx->wf_sort_counts.reserve(sizeof(uint32_t) * size_t(tcb::kWfSortBins) * tcb::kWfSortBlocks));
+    TC_CUDA(ctx, ctx->wf_sorted.reserve(3 * sizeof(uint32_t) * size_t(cap)));
+    w.ext_key = ctx->wf_ext_key.as<uint32_t>();
+    w.shadow_key = ctx->wf_shadow_key.as<uint32_t>();
+    w.sort_counts = ctx->wf_sort_counts.as<uint32_t>();
+    w.sorted = ctx->wf_sorted.as<uint32_t>();
+  }
   if (guided) {
     // The diffuse queue's inference queries and decoded mixtures, one entry per slot.
     TC_CUDA(ctx, ctx->w_query.reserve(sizeof(float4) * 2 * size_t(cap)));
@@ -815,7 +827,7 @@ static int run_wavefront(tc_context* ctx, const tcb::RenderLaunch& L, uint32_t s
     if (it > bound) return fail(ctx, TC_ERR_DEVICE_STATUS, "wavefront render did not drain its paths");
     TC_CUDA(ctx, cudaMemsetAsync(w.q, 0, sizeof(uint32_t) * tcb::kWfCounters, st));
     TC_CUDA(ctx, tcb::launch_wavefront_iteration(w, moments, ctx->sm_count, st, guided ? &ctx->guide : nullptr));
-    ctx->stats.kernel_launches += guided ? 4u : 3u;
+    ctx->stats.kernel_launches += (guided ? 4u : 3u) + (sort_rays ? 3u : 0u);
     const int k = int(it % kWfRing);
     TC_CUDA(ctx, cudaMemcpyAsync(ctx->wf_live_host + k, w.q + tcb::kWfLive, sizeof(uint32_t), cudaMemcpyDeviceToHost,
                                  st));
@@ -913,8 +925,9 @@ static int enqueue_render(tc_context* ctx, const tc_gpu_render_params* p, const 
   if (wavefront) {
     L.total_items = uint64_t(npix) * p->samples;  // one path per work item
     L.g.guide_fraction = o.guide_fraction > 0.0f ? o.guide_fraction : 0.5f;
+    if (o.ray_sort > 2) return fail(ctx, TC_ERR_INVALID, "ray_sort must be 0 (default), 1 (off) or 2 (on)");
     if (int rc = run_wavefront(ctx, L, o.wave_paths ? o.wave_paths : kWavefrontSlots, p->max_bounces,
-                               int(o.refill_lanes), moments, mode == tcb::kModeGuided, st))
+                               int(o.refill_lanes), moments, mode == tcb::kModeGuided, o.ray_sort == 2, st))
       return rc;
   } else if (mode != tcb::kModeGuided) {
     TC_CUDA(ctx, tcb::launch_render(L, block, grid, moments, st, mode));

@@ -148,7 +148,18 @@ struct WavefrontLaunch {
   // Guided renders: the inference queries of the diffuse queue (2 float4 per entry); their decoded
   // mixtures go to r.g.in_mix (kGuideDecodedF4 float4 per entry) with r.g.guide_fraction.
   float4* query;
+  // Ray sorting (sort_keys != null): every queued ray's key (kind, direction octant, bucket of its
+  // origin's primitive in leaf order), per-block bin counts and the sorted order of the entries.
+  uint32_t* ext_key;     // capacity entries
+  uint32_t* shadow_key;  // 2 x capacity entries
+  uint32_t* sort_counts; // kWfSortBins x kWfSortBlocks
+  uint32_t* sorted;      // 3 x capacity entries: queue entry at each sorted position
+  uint32_t prim_count;   // primitive records (bucket scale)
 };
+// Ray sorting: 2 kinds x 8 direction octants x 64 origin buckets, counted by kWfSortBlocks blocks.
+constexpr int kWfSortBuckets = 64;
+constexpr int kWfSortBins = 2 * 8 * kWfSortBuckets;
+constexpr int kWfSortBlocks = 148;
 
 // Vertices of every triangle record in leaf order (verts[3k..3k+2]) gathered from the scene-order
 // triangles (tc_gpu_triangle records) through the records' tags.

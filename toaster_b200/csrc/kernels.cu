@@ -1077,6 +1077,17 @@ int render_max_blocks_per_sm(int block_size, bool moments, int mode, int short_s
 
 __device__ __forceinline__ unsigned lanes_below() { return (1u << (threadIdx.x & 31u)) - 1u; }
 
+// Sort key of a queued ray: direction octant, and the bucket of the primitive record its origin
+// lies on (records are in leaf order, so nearby records are nearby surfaces); camera rays, which
+// start at the eye in pixel order, take the last bucket. Shadow rays use the second half of the bins.
+__device__ __forceinline__ uint32_t wf_sort_key(const WavefrontLaunch& W, V3 d, uint32_t rec, bool shadow) {
+  const uint32_t octant = (d.x < 0.0f ? 1u : 0u) | (d.y < 0.0f ? 2u : 0u) | (d.z < 0.0f ? 4u : 0u);
+  const uint32_t bucket =
+      rec == kNoNode ? uint32_t(kWfSortBuckets - 1)
+                     : uint32_t((uint64_t(rec) * (kWfSortBuckets - 1)) / max(W.prim_count, 1u));
+  return (shadow ? uint32_t(8 * kWfSortBuckets) : 0u) + octant * kWfSortBuckets + bucket;
+}
+
 // Appends the threads of the block whose `pred` holds to a queue counter with one atomic per
 // block (all the block's warps append to the same few counters in every launch, so per-warp atomics
 // would queue up at those addresses); returns each such thread's position. Every thread of the
@@ -1243,7 +1254,10 @@ __global__ void __launch_bounds__(kWfBlock) wf_logic_kernel(const WavefrontLaunc
       }
     }
     const uint32_t pos = block_append(W.q + kWfExtCount, started, sh);
-    if (started) W.ext_q[pos] = slot;
+    if (started) {
+      W.ext_q[pos] = slot;
+      if (W.sorted) W.ext_key[pos] = wf_sort_key(W, mk(0.f, 0.f, 0.f), kNoNode, false);
+    }
     n_live += (kind >= 0 || started) ? 1u : 0u;
   }
   // Path and live-slot counts: one atomic per block each.
@@ -1294,6 +1308,7 @@ __global__ void __launch_bounds__(128) wf_shade_kernel(const WavefrontLaunch W) 
       }
     }
     bool shadow_l = false, shadow_e = false, extend = false;
+    uint32_t h_rec = kNoNode;  // primitive record of the vertex (sort key of the rays it spawns)
     Lane ln;
     float4 c0 = make_float4(0.f, 0.f, 0.f, 0.f), c1 = c0;
     float4 sl0, sl1, se0, se1;
@@ -1312,6 +1327,7 @@ __global__ void __launch_bounds__(128) wf_shade_kernel(const WavefrontLaunch W) 
       tr.t = __uint_as_float(h.x);
       tr.rec = h.y;
       tr.tag = h.z;
+      h_rec = h.y;
       const Surface f = surface_at(s, ln.ro, ln.rd, tr);
       const DevMaterial m = s.materials[f.mat];
       float bsdf_pdf = -1.0f;
@@ -1365,22 +1381,29 @@ __global__ void __launch_bounds__(128) wf_shade_kernel(const WavefrontLaunch W) 
     }
     const uint32_t pl = block_append(W.q + kWfShadowCount, shadow_l, sh);
     if (shadow_l) {
+      if (W.sorted) W.shadow_key[pl] = wf_sort_key(W, mk(sl1.x, sl1.y, sl1.z), h_rec, true);
       W.shadow_q[2 * size_t(pl)] = sl0;
       W.shadow_q[2 * size_t(pl) + 1] = sl1;
     }
     const uint32_t pe = block_append(W.q + kWfShadowCount, shadow_e, sh);
     if (shadow_e) {
+      if (W.sorted) W.shadow_key[pe] = wf_sort_key(W, mk(se1.x, se1.y, se1.z), h_rec, true);
       W.shadow_q[2 * size_t(pe)] = se0;
       W.shadow_q[2 * size_t(pe) + 1] = se1;
     }
     const uint32_t px = block_append(W.q + kWfExtCount, extend, sh);
-    if (extend) W.ext_q[px] = slot;
+    if (extend) {
+      W.ext_q[px] = slot;
+      if (W.sorted) W.ext_key[px] = wf_sort_key(W, ln.rd, h_rec, false);
+    }
   }
 }
 
 // Loads queue entry i (extension rays first, then shadow rays) as a ray with its distance limit.
+template <bool kSorted>
 __device__ __forceinline__ RayQ wf_entry_ray(const WavefrontLaunch& W, uint32_t i, uint32_t n_ext, float& tmax,
                                              uint32_t& target) {
+  if constexpr (kSorted) i = W.sorted[i];  // sorted position -> queue entry (extension entries sort first)
   if (i < n_ext) {
     target = W.ext_q[i];
     const float4 o = W.ray_o[target], d = W.ray_d[target];
@@ -1417,7 +1440,8 @@ __device__ __forceinline__ void wf_entry_result(const WavefrontLaunch& W, uint32
 // soon as fewer than W.refill_lanes lanes of its warp are still traversing (the others keep
 // their traversal state and stack meanwhile).
 // kWatertight: the watertight triangle test over the scene's vertex records.
-template <bool kRefill, bool kWatertight>
+// kSorted: queue entries are taken in the order of W.sorted (ray sorting).
+template <bool kRefill, bool kWatertight, bool kSorted>
 __global__ void __launch_bounds__(128) wf_trace_kernel(const WavefrontLaunch W) {
   static_assert(!(kRefill && kWatertight), "the resumable traversal tests triangles with Moller-Trumbore");
   __shared__ ChildRec root;
@@ -1441,7 +1465,7 @@ __global__ void __launch_bounds__(128) wf_trace_kernel(const WavefrontLaunch W) 
       if (i < total) {
         float tmax;
         uint32_t target;
-        const RayQ q = wf_entry_ray(W, i, n_ext, tmax, target);
+        const RayQ q = wf_entry_ray<kSorted>(W, i, n_ext, tmax, target);
         TraceResult tr;
         bool hit;
         if (i < n_ext) {
@@ -1474,7 +1498,7 @@ __global__ void __launch_bounds__(128) wf_trace_kernel(const WavefrontLaunch W) 
           idx = base + uint32_t(__popc(m & lanes_below()));
           if (idx < total) {
             float tmax;
-            q = wf_entry_ray(W, idx, n_ext, tmax, target);
+            q = wf_entry_ray<kSorted>(W, idx, n_ext, tmax, target);
             trav_start(T, root, q, kRayEps, tmax);
             busy = true;
             if (idx < n_ext) ++c_ext;
@@ -1503,6 +1527,69 @@ __global__ void __launch_bounds__(128) wf_trace_kernel(const WavefrontLaunch W) 
   if (threadIdx.x < 2 && s_count[threadIdx.x] != 0ull) atomicAdd(W.r.counters + 1 + threadIdx.x, s_count[threadIdx.x]);
 }
 
+// Counting sort of one iteration's queued rays by key (extension entries 0..n_ext, then shadow
+// entries): block b of kWfSortBlocks counts the keys of its contiguous share of the entries in
+// shared memory and stores its counts bin-major; a one-block scan turns the counts into each
+// (bin, block)'s first position; the scatter pass repeats the partition and places every entry.
+__device__ __forceinline__ void wf_sort_share(const WavefrontLaunch& W, uint32_t& begin, uint32_t& end,
+                                              uint32_t& n_ext) {
+  n_ext = W.q[kWfExtCount];
+  const uint32_t n = n_ext + W.q[kWfShadowCount];
+  const uint32_t chunk = (n + gridDim.x - 1) / gridDim.x;
+  begin = min(n, blockIdx.x * chunk);
+  end = min(n, begin + chunk);
+}
+
+__global__ void __launch_bounds__(512) wf_sort_count_kernel(const WavefrontLaunch W) {
+  __shared__ uint32_t hist[kWfSortBins];
+  for (int b = threadIdx.x; b < kWfSortBins; b += blockDim.x) hist[b] = 0u;
+  __syncthreads();
+  uint32_t begin, end, n_ext;
+  wf_sort_share(W, begin, end, n_ext);
+  for (uint32_t i = begin + threadIdx.x; i < end; i += blockDim.x)
+    atomicAdd(&hist[i < n_ext ? W.ext_key[i] : W.shadow_key[i - n_ext]], 1u);
+  __syncthreads();
+  for (int b = threadIdx.x; b < kWfSortBins; b += blockDim.x) W.sort_counts[b * kWfSortBlocks + blockIdx.x] = hist[b];
+}
+
+__global__ void __launch_bounds__(1024) wf_sort_scan_kernel(const WavefrontLaunch W) {
+  constexpr uint32_t kN = uint32_t(kWfSortBins) * kWfSortBlocks;
+  __shared__ uint32_t part[1024];
+  const uint32_t per = (kN + 1023) / 1024;
+  const uint32_t begin = min(kN, threadIdx.x * per), end = min(kN, begin + per);
+  uint32_t sum = 0;
+  for (uint32_t i = begin; i < end; ++i) sum += W.sort_counts[i];
+  part[threadIdx.x] = sum;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    uint32_t run = 0;
+    for (int t = 0; t < 1024; ++t) {
+      const uint32_t c = part[t];
+      part[t] = run;
+      run += c;
+    }
+  }
+  __syncthreads();
+  uint32_t run = part[threadIdx.x];
+  for (uint32_t i = begin; i < end; ++i) {
+    const uint32_t c = W.sort_counts[i];
+    W.sort_counts[i] = run;
+    run += c;
+  }
+}
+
+__global__ void __launch_bounds__(512) wf_sort_scatter_kernel(const WavefrontLaunch W) {
+  __shared__ uint32_t cursor[kWfSortBins];
+  for (int b = threadIdx.x; b < kWfSortBins; b += blockDim.x) cursor[b] = W.sort_counts[b * kWfSortBlocks + blockIdx.x];
+  __syncthreads();
+  uint32_t begin, end, n_ext;
+  wf_sort_share(W, begin, end, n_ext);
+  for (uint32_t i = begin + threadIdx.x; i < end; i += blockDim.x) {
+    const uint32_t key = i < n_ext ? W.ext_key[i] : W.shadow_key[i - n_ext];
+    W.sorted[atomicAdd(&cursor[key], 1u)] = i;
+  }
+}
+
 // Resident blocks per SM of a kernel at a block size.
 template <class K>
 static int resident_blocks(K kernel, int block) {
@@ -1515,9 +1602,10 @@ cudaError_t launch_wavefront_iteration(const WavefrontLaunch& w, bool moments, i
                                        const GuideDevice* guide) {
   static const int shade_per_sm = resident_blocks(wf_shade_kernel<false>, 128);
   static const int guided_shade_per_sm = resident_blocks(wf_shade_kernel<true>, 128);
-  static const int trace_per_sm = resident_blocks(wf_trace_kernel<false, false>, 128);
-  static const int refill_per_sm = resident_blocks(wf_trace_kernel<true, false>, 128);
-  static const int watertight_per_sm = resident_blocks(wf_trace_kernel<false, true>, 128);
+  static const int trace_per_sm = resident_blocks(wf_trace_kernel<false, false, false>, 128);
+  static const int sorted_per_sm = resident_blocks(wf_trace_kernel<false, false, true>, 128);
+  static const int refill_per_sm = resident_blocks(wf_trace_kernel<true, false, false>, 128);
+  static const int watertight_per_sm = resident_blocks(wf_trace_kernel<false, true, false>, 128);
   const unsigned logic_grid = unsigned((uint64_t(w.capacity) + kWfBlock - 1) / kWfBlock);
   if (guide) {
     // Guided: the diffuse queue's queries are inferred between the logic and shade launches.
@@ -1532,9 +1620,21 @@ cudaError_t launch_wavefront_iteration(const WavefrontLaunch& w, bool moments, i
     else wf_logic_kernel<false, false><<<logic_grid, kWfBlock, 0, stream>>>(w);
     wf_shade_kernel<false><<<shade_per_sm * sm_count, 128, 0, stream>>>(w);
   }
-  if (w.r.f.scene.tri_verts) wf_trace_kernel<false, true><<<watertight_per_sm * sm_count, 128, 0, stream>>>(w);
-  else if (w.refill_lanes > 1) wf_trace_kernel<true, false><<<refill_per_sm * sm_count, 128, 0, stream>>>(w);
-  else wf_trace_kernel<false, false><<<trace_per_sm * sm_count, 128, 0, stream>>>(w);
+  // Ray sorting applies to the plain trace launch (the watertight and refilling ones take the
+  // queues in append order).
+  const bool sorted = w.sorted && !w.r.f.scene.tri_verts && w.refill_lanes <= 1;
+  if (sorted) {
+    wf_sort_count_kernel<<<kWfSortBlocks, 512, 0, stream>>>(w);
+    wf_sort_scan_kernel<<<1, 1024, 0, stream>>>(w);
+    wf_sort_scatter_kernel<<<kWfSortBlocks, 512, 0, stream>>>(w);
+    wf_trace_kernel<false, false, true><<<sorted_per_sm * sm_count, 128, 0, stream>>>(w);
+  } else if (w.r.f.scene.tri_verts) {
+    wf_trace_kernel<false, true, false><<<watertight_per_sm * sm_count, 128, 0, stream>>>(w);
+  } else if (w.refill_lanes > 1) {
+    wf_trace_kernel<true, false, false><<<refill_per_sm * sm_count, 128, 0, stream>>>(w);
+  } else {
+    wf_trace_kernel<false, false, false><<<trace_per_sm * sm_count, 128, 0, stream>>>(w);
+  }
   return cudaGetLastError();
 }
 

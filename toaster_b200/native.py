@@ -128,6 +128,7 @@ class RenderOptions(ctypes.Structure):
         ("refill_lanes", ctypes.c_uint32),
         ("guide_fraction", ctypes.c_float),
         ("schedule", ctypes.c_uint32),
+        ("ray_sort", ctypes.c_uint32),
     ]
 
 
