@@ -2,10 +2,12 @@
 
     python -m toaster_b200.batch_eval [--frames 240] [--width 1280 --height 720] [--spp 32]
 
-Two workloads:
+Workloads:
 - ``uneven``: 16 independent scenes (triangle counts log-uniform in [128, 262,144], resolutions
   320x180 to 1280x720) rendered by one persistent launch (tc_render_batch) versus one tc_render
   per scene. Reports aggregate Mpaths/s of both.
+- ``uneven_guided``: the same scenes with guided sampling on, each scene's network trained on its
+  own recorded samples: one guided batched launch against guided and plain renders per scene.
 - ``animation``: 240 frames of 64 spheres + 64 boxes on ballistic trajectories. The graph path
   replays one captured CUDA graph per frame (pinned staging -> hierarchy update -> render -> device
   display conversion -> RGBA8 readback): with a device refit of frame 0's tree, with a per-frame
@@ -93,6 +95,56 @@ def uneven(count: int = 16, samples: int = 32, max_bounces: int = 8, repeats: in
             r.close()
 
 
+def uneven_guided(count: int = 16, samples: int = 32, max_bounces: int = 8, repeats: int = 3, record_spp: int = 8,
+                  train_steps: int = guiding_eval.TRAIN_STEPS, device: int = 0, min_width: int = 320,
+                  max_width: int = 1280) -> dict:
+    """The uneven scene set with guided sampling on: every scene trains its own network on its own
+    recorded samples (record_spp plain spp, the guiding recipe's Adam steps), then one guided
+    batched launch over all scenes (each frame's queries inferred by its own network) against one
+    guided tc_render per scene and one plain tc_render per scene. Device time of the path and
+    inference kernels; per-scene times of the unbatched calls give their p50 / p99."""
+    scenes = configs.uneven_batch(count=count, samples=samples, max_bounces=max_bounces, min_width=min_width,
+                                  max_width=max_width)
+    rs = [GpuRenderer(device) for _ in scenes]
+    try:
+        train_ms = 0.0
+        for i, (r, s) in enumerate(zip(rs, scenes)):
+            r.upload(scene_to_gpu(s))
+            r.guide_set_params(guiding_eval.initial_params(i), configs.scene_bounds(s))
+            r.render(samples=record_spp, frame_index=0, guide_record=True)
+            r.guide_train_recorded(train_steps, 8192, 1e-2, i)
+            train_ms += r.stats()["kernel_ms"]
+        paths = sum(s.width * s.height * s.samples for s in scenes)
+        render_batch(rs, frame_index=1, guiding=True)  # warm-up
+        batched = [render_batch(rs, frame_index=2 + k, guiding=True)["kernel_ms"] for k in range(repeats)]
+        per_scene = {"guided": [], "plain": []}
+        totals = {"guided": [], "plain": []}
+        for key, guided in (("guided", True), ("plain", False)):
+            for r in rs:
+                r.render(frame_index=1, guiding=guided)
+            for k in range(repeats):
+                tot = 0.0
+                for r in rs:
+                    r.render(frame_index=2 + k, guiding=guided)
+                    ms = r.stats()["kernel_ms"]
+                    tot += ms
+                    per_scene[key].append(ms)
+                totals[key].append(tot)
+        b = float(np.median(batched))
+        g, pl = float(np.median(totals["guided"])), float(np.median(totals["plain"]))
+        return {"scenes": count, "spp": samples, "max_bounces": max_bounces, "paths": paths,
+                "train_ms_all_scenes": train_ms, "batched_guided_ms": b, "unbatched_guided_ms": g,
+                "unbatched_plain_ms": pl, "batched_guided_mpaths_per_s": paths / (b * 1e3),
+                "unbatched_guided_mpaths_per_s": paths / (g * 1e3), "unbatched_plain_mpaths_per_s": paths / (pl * 1e3),
+                "guided_scene_ms_p50": float(np.percentile(per_scene["guided"], 50)),
+                "guided_scene_ms_p99": float(np.percentile(per_scene["guided"], 99)),
+                "plain_scene_ms_p50": float(np.percentile(per_scene["plain"], 50)),
+                "plain_scene_ms_p99": float(np.percentile(per_scene["plain"], 99))}
+    finally:
+        for r in rs:
+            r.close()
+
+
 def animation(frames: int = 240, width: int = 1280, height: int = 720, samples: int = 32, max_bounces: int = 8,
               guiding: bool = True, train_steps: int = guiding_eval.TRAIN_STEPS, device: int = 0) -> dict:
     anim = configs.BallisticAnimation(width=width, height=height, samples=samples, max_bounces=max_bounces,
@@ -169,8 +221,14 @@ def main():
     ap.add_argument("--height", type=int, default=720)
     ap.add_argument("--spp", type=int, default=32)
     ap.add_argument("--no-guiding", action="store_true")
+    ap.add_argument("--only", choices=["uneven", "uneven_guided", "uneven_small", "animation"], default=None)
     args = ap.parse_args()
+    if args.only == "uneven_guided":
+        print(json.dumps({"uneven_guided": uneven_guided(samples=args.spp)}), flush=True)
+        return
     print(json.dumps({"uneven": uneven(samples=args.spp)}), flush=True)
+    if not args.no_guiding:
+        print(json.dumps({"uneven_guided": uneven_guided(samples=args.spp)}), flush=True)
     print(json.dumps({"uneven_small": uneven(samples=4, max_bounces=4, min_width=160, max_width=480)}), flush=True)
     print(json.dumps({"animation": animation(args.frames, args.width, args.height, args.spp,
                                              guiding=not args.no_guiding)}), flush=True)
