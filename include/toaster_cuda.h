@@ -144,7 +144,7 @@ typedef struct tc_render_options {
                                 samples at every diffuse scatter of this batch and at every
                                 environment shadow ray that reaches the sky (plain sampling) */
   uint32_t wave_paths;       /* paths in flight: guided wavefront (0 = 2^23) or plain wavefront
-                                schedule (0 = 2^22) */
+                                schedule (0 = 2^23) */
   uint32_t short_stack;      /* traversal stack entries per thread held in shared memory (0..16;
                                 deeper entries live in local memory); 0 = none */
   uint32_t refill_lanes;     /* a warp pauses traversal to refill finished lanes once fewer than
@@ -162,7 +162,7 @@ typedef struct tc_render_options {
                                 TC_SCHEDULE_WAVEFRONT (2) = per-path state in device memory and
                                 three launches per bounce (logic, material-sorted shading, tracing
                                 with one ray kind per warp; guided: the diffuse queue inferred
-                                between logic and shading), wave_paths slots (0 = 2^22). Recording
+                                between logic and shading), wave_paths slots (0 = 2^23). Recording
                                 renders, batched launches and captured animation frames use the
                                 megakernel. */
   uint32_t ray_sort;         /* wavefront schedule: sort each iteration's queued rays by kind, direction
@@ -280,7 +280,7 @@ int tc_render_batch(tc_context* const* contexts, const tc_gpu_render_params* par
  * wavefront}; then for the megakernel block size {64, 128, 256}, refill lanes {1, 12, 20, 28},
  * shared-memory short-stack entries {0, 8, 16} and samples per work item {1, 2, 4} (guided: its
  * wave width {2^21, 2^22, 2^23} paths instead); for the wavefront the trace launch's refill lanes
- * {1, 12, 20, 28} and its path slots {2^20, 2^21, 2^22}. Each shape
+ * {1, 12, 20, 28} and its path slots {2^21, 2^22, 2^23}. Each shape
  * runs once untimed and once timed (CUDA events) with probe_samples spp (0 = min(params->samples,
  * 4)). Other fields of `base` are kept. The context's accumulated image is replaced by the last
  * probe. No reference counterpart. */

@@ -9,7 +9,8 @@ widen its own band by itself. Reported:
 - ``outside_block``: the same for the luminance of 2x2 pixel blocks;
 - ``median_z``: median block z-score (a consistent bias shifts it);
 - ``global_dz``: difference of the image-mean luminances in standard errors, and ``rel_mean`` the
-  same difference relative to the oracle's image mean.
+  same difference relative to the oracle's image mean (``rel_se`` is one standard error of it, in
+  the same units).
 
 Luminance variances are bounded by the perfectly correlated case, (sum_c w_c sigma_c)^2, because
 only per-channel sums of squares are kept and the channels of one path are strongly correlated.
@@ -69,6 +70,7 @@ def compare(g_mean, g_var, n_g, o_mean, o_var, n_o, block: int = 2) -> dict:
         "median_z": float(np.median(bz)) if bz.size else 0.0,
         "global_dz": delta / se if se > 0 else 0.0,
         "rel_mean": abs(delta) / max(abs(float(o_l.mean())), 1e-12),
+        "rel_se": se / max(abs(float(o_l.mean())), 1e-12),
         "constant_mismatch": const_bad,
         "pixels": int(d_l.size),
     }

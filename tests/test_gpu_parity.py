@@ -169,6 +169,10 @@ def statistical_parity(renderer, case_name, upload=None, scene=None):
     assert st["constant_mismatch"] == 0, st
     for key, (factor, slack) in BARS.items():
         limit = factor * worst[key] + slack
+        if key == "rel_mean":
+            # Heavy-tailed scenes (the sun room) move their image mean by more than three seed pairs
+            # show; the relative bar is then at least three standard errors of this run's difference.
+            limit = max(limit, 3.0 * st["rel_se"])
         assert abs(st[key]) <= limit, f"{case_name}: {key} = {st[key]:.4f} beyond {limit:.4f} ({st})"
     return st
 

@@ -38,7 +38,7 @@ namespace {
 constexpr int kDefaultRefillLanes = 1;
 // Plain wavefront schedule: default path slots, and the smallest frame (in paths) that the
 // automatic schedule gives it (smaller frames run in less time than its per-bounce launches cost).
-constexpr uint32_t kWavefrontSlots = 1u << 22;
+constexpr uint32_t kWavefrontSlots = 1u << 23;
 constexpr uint64_t kWavefrontMinPaths = 1ull << 20;
 // Iterations the host runs ahead of the live-slot count it waits for (kWfRing = kWfLag + 1).
 constexpr int kWfLag = 4;
@@ -1258,7 +1258,7 @@ int tc_autotune(tc_context* ctx, const tc_gpu_render_params* params, const tc_re
   if (!wavefront)
     if (int rc = stage(&tc_render_options::short_stack, {0u, 8u, 16u})) return rc;
   if (wavefront) {
-    if (int rc = stage(&tc_render_options::wave_paths, {1u << 20, 1u << 21, 1u << 22})) return rc;
+    if (int rc = stage(&tc_render_options::wave_paths, {1u << 21, 1u << 22, 1u << 23})) return rc;
   } else if (b.guiding) {
     if (int rc = stage(&tc_render_options::wave_paths, {1u << 21, 1u << 22, 1u << 23})) return rc;
   } else {
