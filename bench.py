@@ -438,7 +438,7 @@ def equal_time_block(ref_spp: int, device: int, seeds: int = 3) -> dict:
 def kernel_profile():
     """The committed ncu figures of the bench's dominant kernel (DRAM bytes per ray, threads per
     executed instruction), or None."""
-    p = ROOT / "profiles" / "render_kernel_traffic.json"
+    p = ROOT / "profiles" / "bench_frame_figures.json"
     if not p.exists():
         return None
     try:
