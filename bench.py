@@ -266,13 +266,14 @@ def run_ours(args):
     torch.cuda.synchronize()
     clocks.start()
     step_ms, kernel_ms, rays, launches = [], [], [], 0
+    phases = {"trace_ms": [], "logic_ms": [], "shade_ms": [], "wf_iterations": []}
     for k in range(args.steps):
         with torch.cuda.stream(stream):
             flush.zero_()
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        r.render(frame_index=0)
+        r.render(frame_index=0, phase_timing=True)
         e1.record(stream)
         e1.synchronize()
         step_ms.append(e0.elapsed_time(e1))
@@ -280,6 +281,8 @@ def run_ours(args):
         kernel_ms.append(st["kernel_ms"])
         rays.append(st["rays"])
         launches += st["kernel_launches"]
+        for key in phases:
+            phases[key].append(st[key])
     torch.cuda.synchronize()
     clk = clocks.stop()
     barrier()
@@ -321,21 +324,35 @@ def run_ours(args):
         hbm_peak, peak_kind = measured_peaks()
         roofline = None
         if cpu is not None:
+            # Dominant kernel: the wavefront's trace launches (one per iteration), timed live by the
+            # library's per-phase CUDA events on the render stream. Their algorithmic bytes are the
+            # traversal's node and primitive fetches of every ray the step traced.
             bpr = algorithmic_bytes_per_ray(cpu["counts"])
-            achieved = bpr * mean_rays / (mean_kernel_ms * 1e-3) / 1e9
+            trace_ms = statistics.mean(phases["trace_ms"])
+            iterations = statistics.mean(phases["wf_iterations"])
+            achieved = bpr * mean_rays / (trace_ms * 1e-3) / 1e9
             prof = kernel_profile()
             tpi = prof.get("threads_per_instruction") if prof else None
+            trace_dram = prof.get("dram_bytes_per_ray_trace_kernel") if prof else None
             roofline = {"bound": "l2", "achieved": achieved, "peak": l2_peak, "unit": "GB/s",
                         "frac": achieved / l2_peak,
-                        "traffic": prof["dram_bytes_per_ray"] * mean_rays if prof else None,
+                        "traffic": None if trace_dram is None else trace_dram * mean_rays / iterations,
+                        "traffic_note": "DRAM bytes per trace launch: ncu's dram__bytes_read + write per ray of "
+                                        "the trace launches (8-spp frames of this scene) x rays per launch",
                         "peak_source": "measured live: L2 read bandwidth of a 64 MiB buffer streamed by every SM "
                                        "(tc_probe_cache_read, loads bypassing L1)",
                         "hbm_peak": hbm_peak, "hbm_peak_source": peak_kind, "frac_of_hbm": achieved / hbm_peak,
                         "issue": None if tpi is None else {
                             "threads_per_instruction": tpi, "of": 32, "frac": tpi / 32.0,
                             "source": prof.get("source")},
-                        "kernel": prof.get("kernel") if prof else "render_kernel", "bytes_per_ray": bpr,
-                        "rays_per_launch": mean_rays, "kernel_ms": mean_kernel_ms}
+                        "kernel": "wf_trace_kernel<0, 0, 0> (wavefront trace launches)",
+                        "launches_per_step": iterations, "bytes_per_ray": bpr,
+                        "algorithmic_bytes_per_launch": bpr * mean_rays / iterations,
+                        "launch_ms": trace_ms / iterations,
+                        "phases_ms_per_step": {k: statistics.mean(phases[k])
+                                               for k in ("trace_ms", "logic_ms", "shade_ms")},
+                        "step_kernel_ms": mean_kernel_ms,
+                        "frac_over_whole_step": bpr * mean_rays / (mean_kernel_ms * 1e-3) / 1e9 / l2_peak}
         line = {
             "metric": METRIC,
             "value": value,

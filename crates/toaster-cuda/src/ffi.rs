@@ -120,6 +120,8 @@ pub struct TcRenderOptions {
     pub schedule: u32,
     /// Wavefront: 0 default, 1 no ray sorting, 2 rays sorted before tracing.
     pub ray_sort: u32,
+    /// Wavefront: 1 = device time of each launch group in the statistics.
+    pub phase_timing: u32,
 }
 
 /// `tc_scene_changes`, the `SceneChanges` of an evaluated frame.
@@ -158,8 +160,16 @@ pub struct TcStats {
     pub status_flags: u32,
     /// Kernel launches of the last render call.
     pub kernel_launches: u32,
-    /// Padding.
-    pub _pad0: u32,
+    /// Wavefront with phase timing: device time of the trace launches.
+    pub trace_ms: f32,
+    /// ... of the logic launches.
+    pub logic_ms: f32,
+    /// ... of the shading launches.
+    pub shade_ms: f32,
+    /// ... of the guide inference launches.
+    pub guide_ms: f32,
+    /// Wavefront iterations of the last render.
+    pub wf_iterations: u32,
 }
 
 /// Opaque `tc_context`.

@@ -169,6 +169,9 @@ typedef struct tc_render_options {
                                 octant and the leaf-order bucket of their origin's primitive before
                                 tracing (three small launches), so a warp's rays start near each other
                                 and head the same way. 0 = library default (off), 1 = off, 2 = on */
+  uint32_t phase_timing;     /* wavefront schedule: 1 = record CUDA events between each iteration's
+                                launch groups on the render's stream and report their summed device
+                                time in tc_stats (trace_ms, logic_ms, shade_ms, guide_ms); 0 = off */
 } tc_render_options;
 #define TC_SCHEDULE_AUTO 0u
 #define TC_SCHEDULE_MEGAKERNEL 1u
@@ -186,7 +189,12 @@ typedef struct tc_stats {
   uint32_t status_flags;     /* device status word (0 = clean) */
   uint32_t kernel_launches;  /* this library's kernel launches of the last render call (path kernels,
                                 guide inference; not memsets or copies) */
-  uint32_t _pad0;
+  float trace_ms;            /* wavefront render with phase_timing: device time of the trace launches
+                                (ray sorting included); 0 otherwise */
+  float logic_ms;            /* ... of the logic launches */
+  float shade_ms;            /* ... of the shading launches */
+  float guide_ms;            /* ... of the guide inference launches (guided wavefront) */
+  uint32_t wf_iterations;    /* wavefront iterations of the last render; 0 for the megakernel */
 } tc_stats;
 
 typedef struct tc_context tc_context;

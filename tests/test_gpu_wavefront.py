@@ -118,3 +118,22 @@ def test_guided_wavefront_traces_the_guided_megakernel_paths(renderer, fraction)
         renderer.render(samples=16, frame_index=2, guiding=True, guide_fraction=fraction, schedule=schedule)
         out[schedule] = (renderer.readback_sums()[0], None, renderer.stats())
     assert_same_paths(out, scene, 16)
+
+
+def test_phase_timing_splits_the_wavefront_time(renderer):
+    """Per-phase device times of a wavefront render add up to at most its kernel time; a render
+    without phase timing, and a megakernel render, report none."""
+    scene = configs.mixed(width=256, height=144)
+    renderer.upload(scene_to_gpu(scene))
+    renderer.render(samples=32, schedule="wavefront", wave_paths=1 << 18, phase_timing=True)
+    st = renderer.stats()
+    assert st["wf_iterations"] >= scene.max_bounces + 2
+    assert st["kernel_launches"] == 3 * st["wf_iterations"]
+    assert st["trace_ms"] > 0 and st["logic_ms"] > 0 and st["shade_ms"] > 0 and st["guide_ms"] == 0
+    assert st["trace_ms"] + st["logic_ms"] + st["shade_ms"] <= st["kernel_ms"] * 1.001
+    renderer.render(samples=32, schedule="wavefront", wave_paths=1 << 18)
+    st = renderer.stats()
+    assert st["wf_iterations"] > 0 and st["trace_ms"] == 0
+    renderer.render(samples=32, schedule="megakernel", phase_timing=True)
+    st = renderer.stats()
+    assert st["wf_iterations"] == 0 and st["trace_ms"] == 0 and st["kernel_launches"] == 1

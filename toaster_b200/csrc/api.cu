@@ -11,6 +11,7 @@
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <array>
 #include <vector>
 
 #include "../../include/toaster_cuda.h"
@@ -144,6 +145,11 @@ struct tc_context {
   DevBuf wf_ext_key, wf_shadow_key, wf_sort_counts, wf_sorted;
   uint32_t* wf_live_host = nullptr;
   cudaEvent_t wf_events[kWfRing] = {};
+  // Phase timing (tc_render_options.phase_timing): kWfMarks events per iteration of the last
+  // wavefront render, wf_marks_used iterations of them recorded.
+  std::vector<std::array<cudaEvent_t, tcb::kWfMarks>> wf_marks;
+  uint32_t wf_marks_used = 0;
+  bool wf_marks_guided = false;
 
   // Triangle test of the next upload (tc_set_triangle_test) and, for the watertight test, the
   // vertex records of the uploaded scene in leaf order.
@@ -446,6 +452,8 @@ int tc_destroy(tc_context* ctx) {
   if (ctx->ev_end) cudaEventDestroy(ctx->ev_end);
   for (cudaEvent_t e : ctx->wf_events)
     if (e) cudaEventDestroy(e);
+  for (auto& m : ctx->wf_marks)
+    for (cudaEvent_t e : m) cudaEventDestroy(e);
   if (ctx->wf_live_host) cudaFreeHost(ctx->wf_live_host);
   if (ctx->jpeg_params) nvjpegEncoderParamsDestroy(ctx->jpeg_params);
   if (ctx->jpeg_state) nvjpegEncoderStateDestroy(ctx->jpeg_state);
@@ -760,7 +768,8 @@ int tc_set_camera(tc_context* ctx, const tc_gpu_camera* cam) {
 // behind the last one it enqueued, for the live-slot count of an earlier iteration, so the GPU
 // always has queued work; the iterations launched after the last path finished find nothing to do.
 static int run_wavefront(tc_context* ctx, const tcb::RenderLaunch& L, uint32_t slots, uint32_t max_bounces,
-                         int refill_lanes, bool moments, bool guided, bool sort_rays, cudaStream_t st) {
+                         int refill_lanes, bool moments, bool guided, bool sort_rays, bool phase_timing,
+                         cudaStream_t st) {
   const uint64_t items = L.total_items;
   const uint32_t cap = uint32_t(std::max<uint64_t>(32, std::min<uint64_t>(slots, items)));
   if (cap != ctx->wf_capacity) {
@@ -826,8 +835,20 @@ static int run_wavefront(tc_context* ctx, const tcb::RenderLaunch& L, uint32_t s
   for (uint64_t it = 0;; ++it) {
     if (it > bound) return fail(ctx, TC_ERR_DEVICE_STATUS, "wavefront render did not drain its paths");
     TC_CUDA(ctx, cudaMemsetAsync(w.q, 0, sizeof(uint32_t) * tcb::kWfCounters, st));
-    TC_CUDA(ctx, tcb::launch_wavefront_iteration(w, moments, ctx->sm_count, st, guided ? &ctx->guide : nullptr));
+    const cudaEvent_t* marks = nullptr;
+    ctx->wf_marks_guided = guided;
+    if (phase_timing) {
+      if (ctx->wf_marks.size() <= ctx->wf_marks_used) {
+        std::array<cudaEvent_t, tcb::kWfMarks> m{};
+        for (cudaEvent_t& e : m) TC_CUDA(ctx, cudaEventCreate(&e));
+        ctx->wf_marks.push_back(m);
+      }
+      marks = ctx->wf_marks[ctx->wf_marks_used++].data();
+    }
+    TC_CUDA(ctx, tcb::launch_wavefront_iteration(w, moments, ctx->sm_count, st, guided ? &ctx->guide : nullptr,
+                                                 marks));
     ctx->stats.kernel_launches += (guided ? 4u : 3u) + (sort_rays ? 3u : 0u);
+    ctx->stats.wf_iterations += 1;
     const int k = int(it % kWfRing);
     TC_CUDA(ctx, cudaMemcpyAsync(ctx->wf_live_host + k, w.q + tcb::kWfLive, sizeof(uint32_t), cudaMemcpyDeviceToHost,
                                  st));
@@ -863,6 +884,9 @@ static int enqueue_render(tc_context* ctx, const tc_gpu_render_params* p, const 
   if (timing) TC_CUDA(ctx, cudaEventRecord(ctx->ev_begin, st));
   if (int rc = prepare_accumulation(ctx, p, moments, st)) return rc;
   ctx->stats.kernel_launches = 0;
+  ctx->stats.wf_iterations = 0;
+  ctx->stats.trace_ms = ctx->stats.logic_ms = ctx->stats.shade_ms = ctx->stats.guide_ms = 0.0f;
+  ctx->wf_marks_used = 0;
 
   tcb::RenderLaunch L{};
   L.f.scene = ctx->scene;
@@ -927,7 +951,8 @@ static int enqueue_render(tc_context* ctx, const tc_gpu_render_params* p, const 
     L.g.guide_fraction = o.guide_fraction > 0.0f ? o.guide_fraction : 0.5f;
     if (o.ray_sort > 2) return fail(ctx, TC_ERR_INVALID, "ray_sort must be 0 (default), 1 (off) or 2 (on)");
     if (int rc = run_wavefront(ctx, L, o.wave_paths ? o.wave_paths : kWavefrontSlots, p->max_bounces,
-                               int(o.refill_lanes), moments, mode == tcb::kModeGuided, o.ray_sort == 2, st))
+                               int(o.refill_lanes), moments, mode == tcb::kModeGuided, o.ray_sort == 2,
+                               timing && o.phase_timing != 0, st))
       return rc;
   } else if (mode != tcb::kModeGuided) {
     TC_CUDA(ctx, tcb::launch_render(L, block, grid, moments, st, mode));
@@ -989,6 +1014,12 @@ static int enqueue_render(tc_context* ctx, const tc_gpu_render_params* p, const 
   return TC_OK;
 }
 
+// The wavefront-only statistics, zeroed by the calls that do not run the wavefront schedule.
+static void clear_phase_stats(tc_stats& st) {
+  st.trace_ms = st.logic_ms = st.shade_ms = st.guide_ms = 0.0f;
+  st.wf_iterations = 0;
+}
+
 // Counters of a finished render into the context's statistics; fails when paths went missing.
 static int finish_render_stats(tc_context* ctx, const unsigned long long* counters, uint64_t expected_paths,
                                bool timing) {
@@ -999,6 +1030,23 @@ static int finish_render_stats(tc_context* ctx, const unsigned long long* counte
   if (timing) {
     cudaEventElapsedTime(&ctx->stats.kernel_ms, ctx->ev_kernel0, ctx->ev_kernel1);
     cudaEventElapsedTime(&ctx->stats.total_ms, ctx->ev_begin, ctx->ev_end);
+    // Phase timing, per iteration: marks 0-1 logic, 1-2 inference, 2-3 shading, 3-4 tracing
+    // (plain renders leave mark 2 out: shading is 1-3).
+    auto span = [&](uint32_t i, int a, int b) {
+      float ms = 0.0f;
+      cudaEventElapsedTime(&ms, ctx->wf_marks[i][a], ctx->wf_marks[i][b]);
+      return ms;
+    };
+    for (uint32_t i = 0; i < ctx->wf_marks_used; ++i) {
+      ctx->stats.logic_ms += span(i, 0, 1);
+      if (ctx->wf_marks_guided) {
+        ctx->stats.guide_ms += span(i, 1, 2);
+        ctx->stats.shade_ms += span(i, 2, 3);
+      } else {
+        ctx->stats.shade_ms += span(i, 1, 3);
+      }
+      ctx->stats.trace_ms += span(i, 3, 4);
+    }
   }
   if (counters[0] != expected_paths)
     return fail(ctx, TC_ERR_DEVICE_STATUS, "path kernel completed " + std::to_string(counters[0]) + " of " +
@@ -1183,6 +1231,7 @@ int tc_render_batch(tc_context* const* contexts, const tc_gpu_render_params* par
   lead->stats.extension_rays = counters[1];
   lead->stats.shadow_rays = counters[2];
   lead->stats.rays = counters[1] + counters[2];
+  clear_phase_stats(lead->stats);
   cudaEventElapsedTime(&lead->stats.kernel_ms, lead->ev_kernel0, lead->ev_kernel1);
   cudaEventElapsedTime(&lead->stats.total_ms, lead->ev_begin, lead->ev_end);
   if (counters[0] != paths)
@@ -1486,6 +1535,7 @@ int tc_animation_frame(tc_animation* a, const tc_scene_data* frame, uint32_t fra
                 "the frame's centroids coincide in a node of more than four primitives (a degenerate leaf); "
                 "animate this scene with refits or upload its frames");
   cudaEventElapsedTime(&ctx->stats.total_ms, ctx->ev_begin, ctx->ev_end);
+  clear_phase_stats(ctx->stats);
   ctx->stats.kernel_ms = ctx->stats.total_ms;
   if (int rc = finish_render_stats(ctx, a->h_counters, uint64_t(a->npix) * a->params.samples, false)) return rc;
   if (rgba) std::memcpy(rgba, a->h_rgba, 4 * a->npix);
@@ -1688,6 +1738,7 @@ int tc_trace_closest(tc_context* ctx, const float* rays, size_t n, float tmin, u
   TC_CUDA(ctx, cudaMemcpyAsync(t, ctx->t_buf.ptr, sizeof(float) * n, cudaMemcpyDeviceToHost, st));
   TC_CUDA(ctx, cudaEventRecord(ctx->ev_end, st));
   TC_CUDA(ctx, cudaStreamSynchronize(st));
+  clear_phase_stats(ctx->stats);
   cudaEventElapsedTime(&ctx->stats.kernel_ms, ctx->ev_kernel0, ctx->ev_kernel1);
   cudaEventElapsedTime(&ctx->stats.total_ms, ctx->ev_begin, ctx->ev_end);
   ctx->stats.rays = n;
@@ -1796,6 +1847,7 @@ int tc_guide_infer(tc_context* ctx, const float* queries, size_t n, float* out) 
   TC_CUDA(ctx, cudaEventRecord(ctx->ev_kernel1, st));
   TC_CUDA(ctx, cudaMemcpyAsync(out, ctx->g_out.ptr, sizeof(float4) * tcb::kGuideDecodedF4 * n, cudaMemcpyDeviceToHost, st));
   int rc = guide_check_status(ctx);
+  clear_phase_stats(ctx->stats);
   cudaEventElapsedTime(&ctx->stats.kernel_ms, ctx->ev_kernel0, ctx->ev_kernel1);
   return rc;
 }
@@ -1818,6 +1870,7 @@ int tc_guide_loss_grad(tc_context* ctx, const float* samples, size_t n, float* g
   std::vector<float> g(tcb::kGuideParams + 1);
   TC_CUDA(ctx, cudaMemcpyAsync(g.data(), ctx->guide.grad, sizeof(float) * g.size(), cudaMemcpyDeviceToHost, st));
   int rc = guide_check_status(ctx);
+  clear_phase_stats(ctx->stats);
   cudaEventElapsedTime(&ctx->stats.kernel_ms, ctx->ev_kernel0, ctx->ev_kernel1);
   if (rc != TC_OK) return rc;
   if (grad) std::memcpy(grad, g.data(), sizeof(float) * tcb::kGuideParams);
@@ -1877,6 +1930,7 @@ int tc_guide_train(tc_context* ctx, const float* samples, size_t n, uint32_t ste
   TC_CUDA(ctx, cudaEventRecord(ctx->ev_kernel1, st));
   if (steps) TC_CUDA(ctx, cudaMemcpyAsync(step_loss.data(), ctx->g_out.ptr, sizeof(float) * steps, cudaMemcpyDeviceToHost, st));
   int rc = guide_check_status(ctx);
+  clear_phase_stats(ctx->stats);
   cudaEventElapsedTime(&ctx->stats.kernel_ms, ctx->ev_kernel0, ctx->ev_kernel1);
   if (rc != TC_OK) return rc;
   if (losses) std::memcpy(losses, step_loss.data(), sizeof(float) * steps);
@@ -1937,6 +1991,7 @@ int tc_guide_train_recorded(tc_context* ctx, uint32_t steps, uint32_t batch, flo
   std::vector<float> step_loss(steps);
   if (steps) TC_CUDA(ctx, cudaMemcpyAsync(step_loss.data(), ctx->g_out.ptr, sizeof(float) * steps, cudaMemcpyDeviceToHost, st));
   int rc = guide_check_status(ctx);
+  clear_phase_stats(ctx->stats);
   cudaEventElapsedTime(&ctx->stats.kernel_ms, ctx->ev_kernel0, ctx->ev_kernel1);
   if (rc != TC_OK) return rc;
   if (losses && steps) std::memcpy(losses, step_loss.data(), sizeof(float) * steps);

@@ -175,9 +175,12 @@ int render_max_blocks_per_sm(int block_size, bool moments, int mode = kModePlain
                              int min_active = 1);
 // One wavefront iteration (logic, [guide inference,] shade, trace) on `stream`; the caller
 // clears w.q first. `guide` (guided renders) is the network that infers the diffuse queue.
+// `marks`, when set, are kWfMarks timing events recorded before the logic launch and after the
+// logic, inference (guided only), shading and trace groups.
 struct GuideDevice;
+constexpr int kWfMarks = 5;
 cudaError_t launch_wavefront_iteration(const WavefrontLaunch& w, bool moments, int sm_count, cudaStream_t stream,
-                                       const GuideDevice* guide = nullptr);
+                                       const GuideDevice* guide = nullptr, const cudaEvent_t* marks = nullptr);
 // Batched launch over r.jobs (r.job_count frames, items concatenated in job order): plain, or one
 // round of the guided wavefront (r.g, with per-frame regions of the wave buffers).
 cudaError_t launch_render_batch(const RenderLaunch& r, int block_size, int grid_size, cudaStream_t stream,

@@ -1599,7 +1599,7 @@ static int resident_blocks(K kernel, int block) {
 }
 
 cudaError_t launch_wavefront_iteration(const WavefrontLaunch& w, bool moments, int sm_count, cudaStream_t stream,
-                                       const GuideDevice* guide) {
+                                       const GuideDevice* guide, const cudaEvent_t* marks) {
   static const int shade_per_sm = resident_blocks(wf_shade_kernel<false>, 128);
   static const int guided_shade_per_sm = resident_blocks(wf_shade_kernel<true>, 128);
   static const int trace_per_sm = resident_blocks(wf_trace_kernel<false, false, false>, 128);
@@ -1607,19 +1607,27 @@ cudaError_t launch_wavefront_iteration(const WavefrontLaunch& w, bool moments, i
   static const int refill_per_sm = resident_blocks(wf_trace_kernel<true, false, false>, 128);
   static const int watertight_per_sm = resident_blocks(wf_trace_kernel<false, true, false>, 128);
   const unsigned logic_grid = unsigned((uint64_t(w.capacity) + kWfBlock - 1) / kWfBlock);
+  auto mark = [&](int i) {
+    if (marks) cudaEventRecord(marks[i], stream);
+  };
+  mark(0);
   if (guide) {
     // Guided: the diffuse queue's queries are inferred between the logic and shade launches.
     if (moments) wf_logic_kernel<true, true><<<logic_grid, kWfBlock, 0, stream>>>(w);
     else wf_logic_kernel<false, true><<<logic_grid, kWfBlock, 0, stream>>>(w);
+    mark(1);
     cudaError_t e = guide_launch_infer(*guide, w.query, w.capacity, const_cast<float4*>(w.r.g.in_mix), sm_count,
                                        stream, w.q + kWfMatCount);
     if (e != cudaSuccess) return e;
+    mark(2);
     wf_shade_kernel<true><<<guided_shade_per_sm * sm_count, 128, 0, stream>>>(w);
   } else {
     if (moments) wf_logic_kernel<true, false><<<logic_grid, kWfBlock, 0, stream>>>(w);
     else wf_logic_kernel<false, false><<<logic_grid, kWfBlock, 0, stream>>>(w);
+    mark(1);  // no inference: marks[2] stays unrecorded
     wf_shade_kernel<false><<<shade_per_sm * sm_count, 128, 0, stream>>>(w);
   }
+  mark(3);
   // Ray sorting applies to the plain trace launch (the watertight and refilling ones take the
   // queues in append order).
   const bool sorted = w.sorted && !w.r.f.scene.tri_verts && w.refill_lanes <= 1;
@@ -1635,6 +1643,7 @@ cudaError_t launch_wavefront_iteration(const WavefrontLaunch& w, bool moments, i
   } else {
     wf_trace_kernel<false, false, false><<<trace_per_sm * sm_count, 128, 0, stream>>>(w);
   }
+  mark(4);
   return cudaGetLastError();
 }
 

@@ -129,6 +129,7 @@ class RenderOptions(ctypes.Structure):
         ("guide_fraction", ctypes.c_float),
         ("schedule", ctypes.c_uint32),
         ("ray_sort", ctypes.c_uint32),
+        ("phase_timing", ctypes.c_uint32),
     ]
 
 
@@ -151,7 +152,11 @@ class Stats(ctypes.Structure):
         ("bvh_depth", ctypes.c_uint32),
         ("status_flags", ctypes.c_uint32),
         ("kernel_launches", ctypes.c_uint32),
-        ("_pad0", ctypes.c_uint32),
+        ("trace_ms", ctypes.c_float),
+        ("logic_ms", ctypes.c_float),
+        ("shade_ms", ctypes.c_float),
+        ("guide_ms", ctypes.c_float),
+        ("wf_iterations", ctypes.c_uint32),
     ]
 
 

@@ -237,11 +237,13 @@ class GpuRenderer:
                height: Optional[int] = None, frame_index: int = 0, accumulate: bool = False,
                keep_moments: bool = False, block_size: int = 0, samples_per_item: int = 0, guiding: bool = False,
                guide_record: bool = False, wave_paths: int = 0, short_stack: int = 0, refill_lanes: int = 0,
-               guide_fraction: float = 0.0, schedule: str = "auto", ray_sort: int = 0) -> None:
+               guide_fraction: float = 0.0, schedule: str = "auto", ray_sort: int = 0,
+               phase_timing: bool = False) -> None:
         """Traces ``samples`` paths per pixel; ``accumulate`` adds them to the previous batches.
         ``guide_fraction``: probability of sampling the network's mixture at a guided diffuse
         vertex (0 = the library's default, 0.5). ``schedule`` (plain renders): "auto",
-        "megakernel" or "wavefront"."""
+        "megakernel" or "wavefront". ``phase_timing`` (wavefront): device time of the trace,
+        logic, shading and inference launches in ``stats()`` (trace_ms, logic_ms, ...)."""
         if self._params is None:
             raise RuntimeError("render before upload")
         p = self._params.copy()
@@ -267,6 +269,7 @@ class GpuRenderer:
         opts.guide_fraction = guide_fraction
         opts.schedule = native.SCHEDULES[schedule]
         opts.ray_sort = ray_sort
+        opts.phase_timing = 1 if phase_timing else 0
         self._check(self._lib.tc_render(self._ctx, p.ctypes.data, ctypes.byref(opts)))
         self.width, self.height = int(p["width"][0]), int(p["height"][0])
         self.accumulated = (self.accumulated if accumulate else 0) + int(p["samples"][0])
