@@ -419,7 +419,8 @@ def equal_time_block(ref_spp: int, device: int, seeds: int = 3) -> dict:
     """Guided vs plain sampling at equal GPU time on the learned-guiding workload (window room,
     8,192 clutter triangles with 30% metal, 1280x720, 8 bounces): plain accumulates 256 spp in
     16-spp batches; guided records 16 spp, trains the recipe's Adam steps on the GPU and accumulates
-    guided batches. RMSE is against a plain FP64 reference of ``ref_spp`` samples per pixel, taken
+    guided batches, each recording its own training samples into the pool and followed by the
+    recipe's online Adam steps (their time counts). RMSE is against a plain FP64 reference of ``ref_spp`` samples per pixel, taken
     over 4 evenly spaced bands of 8 rows (40,960 pixels; the reference is rendered for those rows
     only, which keeps the 65,536-spp render within a minute); the trimmed RMSE leaves out the 0.1%
     largest pixel errors. Medians over ``seeds`` independent runs, each seed's figures beside them."""
@@ -431,13 +432,14 @@ def equal_time_block(ref_spp: int, device: int, seeds: int = 3) -> dict:
     ref_s = time.perf_counter() - t0
     keep = ["plain_seconds", "plain_rmse", "guided_seconds_to_plain_rmse", "time_fraction",
             "guided_rmse_at_plain_time", "plain_trimmed_rmse", "time_fraction_trimmed",
-            "guided_trimmed_rmse_at_plain_time", "train_seconds", "samples"]
+            "guided_trimmed_rmse_at_plain_time", "train_seconds", "samples", "pool_samples",
+            "online_train_seconds"]
     runs = []
     for seed in range(seeds):
         out = guiding_eval.equal_time_comparison(scene, ref_spp=ref_spp, plain_spp=256, batch=16, record_spp=16,
                                                  train_steps=guiding_eval.TRAIN_STEPS, train_batch=8192, seed=seed,
                                                  device=device, reference=reference, rows=rows)
-        runs.append({k: out[k] for k in keep})
+        runs.append({k: out.get(k) for k in keep})
 
     def median(key):
         vals = [r[key] for r in runs if r[key] is not None]
@@ -446,7 +448,8 @@ def equal_time_block(ref_spp: int, device: int, seeds: int = 3) -> dict:
     return {"workload": "window room, 8,192 clutter triangles (30% metal), 1280x720, 8 bounces",
             "reference_spp": ref_spp, "reference_rows": "4 bands of 8 rows (40,960 pixels)",
             "reference_seconds": ref_s, "plain_spp": 256, "record_spp": 16,
-            "train_steps": guiding_eval.TRAIN_STEPS, "seeds": seeds,
+            "train_steps": guiding_eval.TRAIN_STEPS, "online_steps": guiding_eval.ONLINE_STEPS,
+            "online_batch": guiding_eval.ONLINE_BATCH, "seeds": seeds,
             "time_fraction": median("time_fraction"), "time_fraction_trimmed": median("time_fraction_trimmed"),
             "plain_rmse": median("plain_rmse"), "plain_trimmed_rmse": median("plain_trimmed_rmse"),
             "per_seed": runs, "wall_seconds": time.perf_counter() - t0}

@@ -140,9 +140,13 @@ typedef struct tc_render_options {
   uint32_t samples_per_item; /* samples one lane traces for a pixel before taking new work; 0 = default */
   uint32_t keep_moments;     /* 1: also accumulate per-pixel sums of squared samples (FP64) */
   uint32_t guiding;          /* 1: learned path guiding at diffuse vertices (needs tc_guide_set_params) */
-  uint32_t guide_record;     /* 1: record (position, normal, direction, incident radiance) training
+  uint32_t guide_record;     /* record (position, normal, direction, incident radiance) training
                                 samples at every diffuse scatter of this batch and at every
-                                environment shadow ray that reaches the sky (plain sampling) */
+                                environment shadow ray that reaches the sky, into the context's
+                                sample pool (16,777,216 samples; later ones are dropped):
+                                1 = empty the pool first, 2 = add to it. Plain renders, and
+                                guided renders on the wavefront schedule (their samples weighted
+                                by the mixture pdf they were drawn with) */
   uint32_t wave_paths;       /* paths in flight: guided wavefront (0 = 2^23) or plain wavefront
                                 schedule (0 = 2^23) */
   uint32_t short_stack;      /* traversal stack entries per thread held in shared memory (0..16;
@@ -162,9 +166,8 @@ typedef struct tc_render_options {
                                 TC_SCHEDULE_WAVEFRONT (2) = per-path state in device memory and
                                 three launches per bounce (logic, material-sorted shading, tracing
                                 with one ray kind per warp; guided: the diffuse queue inferred
-                                between logic and shading), wave_paths slots (0 = 2^23). Recording
-                                renders, batched launches and captured animation frames use the
-                                megakernel. */
+                                between logic and shading), wave_paths slots (0 = 2^23). Batched
+                                launches and captured animation frames use the megakernel. */
   uint32_t ray_sort;         /* wavefront schedule: sort each iteration's queued rays by kind, direction
                                 octant and the leaf-order bucket of their origin's primitive before
                                 tracing (three small launches), so a warp's rays start near each other
@@ -426,18 +429,18 @@ int tc_guide_adam_step(tc_context* ctx, float lr);
 int tc_guide_train(tc_context* ctx, const float* samples, size_t n, uint32_t steps, uint32_t batch, float lr,
                    uint64_t seed, float* losses);
 
-/* Builds training samples from the diffuse scatters recorded by the last tc_render with
- * guide_record = 1 (weight = luminance of the radiance that arrived along each scattered
- * direction, or, for an environment shadow ray that reached the sky, its radiance times the BSDF
- * side's MIS share over the light pdf; normalised by the mean and clamped at 50x the mean;
- * directions that carried no radiance are dropped, as they add nothing to the weighted
- * likelihood) and runs `steps` Adam steps on batches of `batch` samples drawn at random. losses (optional) receives one value per
- * step and n_samples (optional) the number of samples. */
+/* Runs `steps` Adam steps on batches of `batch` samples drawn at random from the sample pool:
+ * the samples of every tc_render with guide_record since the last one with guide_record = 1
+ * (weight = luminance of the radiance that arrived along the scattered direction times
+ * cos / (pi p) for a direction drawn with pdf p, or, for an environment shadow ray that reached
+ * the sky, its radiance times the BSDF side's MIS share over the light pdf; normalised by the
+ * pool's mean weight and clamped at 50x the mean; directions that carried no radiance are
+ * dropped, as they add nothing to the weighted likelihood). losses (optional) receives one value
+ * per step and n_samples (optional) the number of samples in the pool. */
 int tc_guide_train_recorded(tc_context* ctx, uint32_t steps, uint32_t batch, float lr, uint64_t seed, float* losses,
                             uint32_t* n_samples);
 
-/* The training samples derived from the last guide_record batch, as tc_guide_train_recorded
- * sees them: 12 floats each (position + weight, normal + 0, direction + 0), weight = luminance of
+/* The sample pool, as tc_guide_train_recorded sees it: 12 floats each (position + weight, normal + 0, direction + 0), weight = luminance of
  * the radiance that arrived along the recorded direction. Only directions that carried radiance
  * are kept (in an unspecified order). Writes min(count, n_floats / 12) samples; *count receives
  * their number. out may be NULL to query the count. No reference counterpart (inspection of the

@@ -46,6 +46,8 @@ constexpr int kWfLag = 4;
 constexpr int kWfRing = kWfLag + 1;
 // Scenes with at least this many primitives build their hierarchy on the device by default.
 constexpr size_t kDeviceBuildMin = 4096;
+// Guide training samples the pool keeps across recording batches (48 bytes each: 768 MiB).
+constexpr uint32_t kGuidePoolSamples = 1u << 24;
 
 thread_local std::string g_thread_error;
 
@@ -127,8 +129,10 @@ struct tc_context {
   DevBuf g_params, g_m, g_v, g_grad, g_images, g_biases, g_status, g_in, g_out;
   // Guided wavefront buffers (two state buffers, queries, decoded mixtures, round counters).
   DevBuf w_state_a, w_state_b, w_query, w_mix, w_counts, w_prefix;
-  // Recorded training data of the last guide_record batch.
-  DevBuf rec_records, rec_count, rec_path_rad, rec_samples, rec_wsum;
+  // Recorded training data: the records of the last recording batch, and the sample pool every
+  // recording batch appends its positive-weight samples to (guide_record = 1 starts a new pool):
+  // rec_samples holds kGuidePoolSamples samples, rec_wsum their (count, weight sum).
+  DevBuf rec_records, rec_count, rec_path_rad, rec_samples, rec_wsum, wf_rec_ref;
   uint32_t rec_capacity = 0;
   bool has_records = false;
 
@@ -821,6 +825,10 @@ static int run_wavefront(tc_context* ctx, const tcb::RenderLaunch& L, uint32_t s
     w.sort_counts = ctx->wf_sort_counts.as<uint32_t>();
     w.sorted = ctx->wf_sorted.as<uint32_t>();
   }
+  if (L.g.records) {
+    TC_CUDA(ctx, ctx->wf_rec_ref.reserve(sizeof(uint2) * size_t(cap)));
+    w.rec_ref = ctx->wf_rec_ref.as<uint2>();
+  }
   if (guided) {
     // The diffuse queue's inference queries and decoded mixtures, one entry per slot.
     TC_CUDA(ctx, ctx->w_query.reserve(sizeof(float4) * 2 * size_t(cap)));
@@ -867,6 +875,8 @@ static int run_wavefront(tc_context* ctx, const tcb::RenderLaunch& L, uint32_t s
 // `timing` records the context's events around the kernels (left out while capturing a graph).
 // frame_index_dev / camera_dev, when set, make the kernels read those per-frame values from
 // device memory. On success ctx->accumulated is advanced.
+static int append_training_samples(tc_context* ctx, bool fresh, cudaStream_t st);
+
 static int enqueue_render(tc_context* ctx, const tc_gpu_render_params* p, const tc_render_options& o, cudaStream_t st,
                           bool timing, const uint32_t* frame_index_dev, const float* camera_dev,
                           unsigned long long* counters_host) {
@@ -875,7 +885,8 @@ static int enqueue_render(tc_context* ctx, const tc_gpu_render_params* p, const 
   const int block = o.block_size ? int(o.block_size) : 128;
   if (block % 32 != 0 || block < 32 || block > 256)
     return fail(ctx, TC_ERR_INVALID, "block_size must be a multiple of 32 in [32, 256]");
-  if (o.guiding && o.guide_record) return fail(ctx, TC_ERR_INVALID, "guiding and guide_record are exclusive");
+  if (o.guide_record > 2)
+    return fail(ctx, TC_ERR_INVALID, "guide_record must be 0, 1 (start a new sample pool) or 2 (add to the pool)");
   if (o.guiding && !ctx->has_guide) return fail(ctx, TC_ERR_STATE, "guided rendering needs tc_guide_set_params first");
   if (!(o.guide_fraction >= 0.0f && o.guide_fraction < 1.0f))
     return fail(ctx, TC_ERR_INVALID, "guide_fraction must be in [0, 1)");
@@ -917,12 +928,14 @@ static int enqueue_render(tc_context* ctx, const tc_gpu_render_params* p, const 
   int grid = per_sm * ctx->sm_count;
   if (mode != tcb::kModeGuided)
     grid = int(std::max<uint64_t>(1, std::min<uint64_t>(uint64_t(grid), (L.total_items + block - 1) / block)));
-  if (mode == tcb::kModeRecord) {
-    // One record per diffuse scatter and per unoccluded environment shadow ray (capped), and the
-    // final radiance of every path of the batch.
+  if (o.guide_record) {
+    // One record per diffuse scatter and per environment shadow ray, at most two per bounce
+    // (capped at 2^27 records, 8 GiB; records past the cap are dropped), and the final radiance
+    // of every path of the batch.
     const uint64_t paths = uint64_t(npix) * p->samples;
     if (paths > (1ull << 31)) return fail(ctx, TC_ERR_INVALID, "too many paths to record in one batch");
-    ctx->rec_capacity = uint32_t(std::min<uint64_t>(3 * paths, uint64_t(1) << 25));
+    ctx->rec_capacity =
+        uint32_t(std::min<uint64_t>(2 * uint64_t(std::max<uint32_t>(p->max_bounces, 1)) * paths, uint64_t(1) << 27));
     TC_CUDA(ctx, ctx->rec_records.reserve(sizeof(float4) * 4 * size_t(ctx->rec_capacity)));
     TC_CUDA(ctx, ctx->rec_count.reserve(sizeof(uint32_t)));
     TC_CUDA(ctx, ctx->rec_path_rad.reserve(sizeof(float4) * size_t(paths)));
@@ -934,7 +947,7 @@ static int enqueue_render(tc_context* ctx, const tc_gpu_render_params* p, const 
   }
   // Plain and guided renders called directly (not captured into a graph) may run as a wavefront.
   const bool direct = !camera_dev && !frame_index_dev;
-  const bool wf_mode = mode == tcb::kModePlain || mode == tcb::kModeGuided;
+  const bool wf_mode = mode == tcb::kModePlain || mode == tcb::kModeGuided || mode == tcb::kModeRecord;
   if (o.schedule > TC_SCHEDULE_WAVEFRONT) return fail(ctx, TC_ERR_INVALID, "schedule must be 0 (auto), 1 or 2");
   if (o.schedule == TC_SCHEDULE_WAVEFRONT && wf_mode && !direct)
     return fail(ctx, TC_ERR_INVALID, "the wavefront schedule renders direct calls only, not captured frames");
@@ -945,6 +958,8 @@ static int enqueue_render(tc_context* ctx, const tc_gpu_render_params* p, const 
   if (ctx->scene.tri_verts && !wavefront)
     return fail(ctx, TC_ERR_INVALID,
                 "the watertight triangle test is traced by tc_trace_closest and by plain wavefront renders only");
+  if (o.guiding && o.guide_record && !wavefront)
+    return fail(ctx, TC_ERR_INVALID, "guided renders record training samples on the wavefront schedule only");
   if (timing) TC_CUDA(ctx, cudaEventRecord(ctx->ev_kernel0, st));
   if (wavefront) {
     L.total_items = uint64_t(npix) * p->samples;  // one path per work item
@@ -1004,13 +1019,17 @@ static int enqueue_render(tc_context* ctx, const tc_gpu_render_params* p, const 
       }
     }
   }
+  if (o.guide_record) {
+    if (int rc = append_training_samples(ctx, o.guide_record == 1, st)) return rc;
+    ctx->stats.kernel_launches += 1;
+  }
   if (timing) TC_CUDA(ctx, cudaEventRecord(ctx->ev_kernel1, st));
   if (counters_host)
     TC_CUDA(ctx, cudaMemcpyAsync(counters_host, ctx->counters.ptr, 4 * sizeof(unsigned long long),
                                  cudaMemcpyDeviceToHost, st));
   if (timing) TC_CUDA(ctx, cudaEventRecord(ctx->ev_end, st));
   ctx->accumulated += p->samples;
-  if (mode == tcb::kModeRecord) ctx->has_records = true;
+  if (o.guide_record) ctx->has_records = true;
   return TC_OK;
 }
 
@@ -1939,21 +1958,28 @@ int tc_guide_train(tc_context* ctx, const float* samples, size_t n, uint32_t ste
 
 // Positive-weight training samples of the last recorded batch into rec_samples; their number and
 // weight sum come back to the host.
-static int prepare_training_samples(tc_context* ctx, uint32_t* count, float* wsum) {
-  cudaStream_t st = ctx->stream;
-  TC_CUDA(ctx, ctx->rec_samples.reserve(sizeof(float4) * 3 * size_t(ctx->rec_capacity)));
+// Appends the positive-weight training samples of the batch just recorded to the sample pool
+// (`fresh`: empties the pool first). Enqueued on `st` after the batch; no host synchronisation.
+static int append_training_samples(tc_context* ctx, bool fresh, cudaStream_t st) {
+  TC_CUDA(ctx, ctx->rec_samples.reserve(sizeof(float4) * 3 * size_t(kGuidePoolSamples)));
   TC_CUDA(ctx, ctx->rec_wsum.reserve(2 * sizeof(uint32_t)));
-  TC_CUDA(ctx, cudaMemsetAsync(ctx->rec_wsum.ptr, 0, 2 * sizeof(uint32_t), st));
+  if (fresh || !ctx->has_records) TC_CUDA(ctx, cudaMemsetAsync(ctx->rec_wsum.ptr, 0, 2 * sizeof(uint32_t), st));
   float* d_wsum = ctx->rec_wsum.as<float>();
   uint32_t* d_count = reinterpret_cast<uint32_t*>(d_wsum + 1);
   TC_CUDA(ctx, tcb::launch_guide_samples(ctx->rec_records.as<float4>(), ctx->rec_count.as<uint32_t>(), ctx->rec_capacity,
-                                         ctx->rec_path_rad.as<float4>(), ctx->rec_samples.as<float4>(), d_count,
-                                         d_wsum, st));
+                                         ctx->rec_path_rad.as<float4>(), ctx->rec_samples.as<float4>(),
+                                         kGuidePoolSamples, d_count, d_wsum, st));
+  return TC_OK;
+}
+
+// Number of samples in the pool and the sum of their weights (waits for the stream).
+static int pool_counts(tc_context* ctx, uint32_t* count, float* wsum) {
+  cudaStream_t st = ctx->stream;
   uint32_t host[2] = {0, 0};
   TC_CUDA(ctx, cudaMemcpyAsync(host, ctx->rec_wsum.ptr, sizeof(host), cudaMemcpyDeviceToHost, st));
   TC_CUDA(ctx, cudaStreamSynchronize(st));
   std::memcpy(wsum, &host[0], sizeof(float));
-  *count = std::min(host[1], ctx->rec_capacity);
+  *count = std::min(host[1], kGuidePoolSamples);
   return TC_OK;
 }
 
@@ -1968,7 +1994,7 @@ int tc_guide_train_recorded(tc_context* ctx, uint32_t steps, uint32_t batch, flo
   TC_CUDA(ctx, cudaEventRecord(ctx->ev_kernel0, st));
   uint32_t count = 0;
   float wsum = 0.0f;
-  if (int rc = prepare_training_samples(ctx, &count, &wsum)) return rc;
+  if (int rc = pool_counts(ctx, &count, &wsum)) return rc;
   if (n_samples) *n_samples = count;
   if (count == 0 || !(wsum > 0.0f)) return fail(ctx, TC_ERR_STATE, "the recorded batch carries no radiance to learn from");
   const float mean = wsum / float(count);
@@ -2005,7 +2031,7 @@ int tc_guide_recorded_samples(tc_context* ctx, float* out, size_t n_floats, uint
   cudaStream_t st = ctx->stream;
   uint32_t n = 0;
   float wsum = 0.0f;
-  if (int rc = prepare_training_samples(ctx, &n, &wsum)) return rc;
+  if (int rc = pool_counts(ctx, &n, &wsum)) return rc;
   if (count) *count = n;
   if (out) {
     const size_t m = std::min<size_t>(n_floats / 12, n);

@@ -130,13 +130,14 @@ enum WfCounter : int {
 };
 
 struct WavefrontLaunch {
-  RenderLaunch r;        // frame (r.f), work counter and launch counters; r.g is unused
+  RenderLaunch r;        // frame (r.f), work counter and launch counters; r.g: guiding (in_mix,
+                         // guide_fraction) and recording (records != null)
   uint32_t capacity;     // path slots
   uint32_t* state;       // state word
   float4* ray_o;         // (ray origin.xyz, solid-angle pdf of the last diffuse bounce or -1)
   float4* ray_d;         // (ray direction.xyz, -)
   float4* thr;           // (throughput.xyz, pixel)
-  float4* rad;           // (radiance.xyz, -)
+  float4* rad;           // (radiance.xyz, the path's work item)
   uint4* rng;            // PCG32 state and increment
   uint4* hit;            // (t bits, primitive record or kNoNode, tag, material word) of the extension ray
   float4* nee;           // 2 per slot: light and environment shadow-ray contributions
@@ -155,6 +156,9 @@ struct WavefrontLaunch {
   uint32_t* sort_counts; // kWfSortBins x kWfSortBlocks
   uint32_t* sorted;      // 3 x capacity entries: queue entry at each sorted position
   uint32_t prim_count;   // primitive records (bucket scale)
+  // Recording: per slot, the scatter record and the environment-NEE record of the diffuse vertex
+  // shaded last (kNoNode when none); the next logic launch completes or drops them.
+  uint2* rec_ref;
 };
 // Ray sorting: 2 kinds x 8 direction octants x 64 origin buckets, counted by kWfSortBlocks blocks.
 constexpr int kWfSortBuckets = 64;
@@ -190,12 +194,14 @@ int render_batch_max_blocks_per_sm(int block_size, bool guided = false);
 cudaError_t launch_job_prefix(const uint32_t* counts, const FrameJob* jobs, uint32_t n, uint32_t* prefix,
                               cudaStream_t stream);
 // Training samples (3 float4 each: position + weight, normal, direction) from recorded diffuse
-// scatters: weight = luminance of the radiance that arrived along the scattered direction. Only
-// positive-weight samples are written (compacted, order unspecified); *sample_count (zeroed by
-// the caller) receives their number and *weight_sum (zeroed) the sum of weights.
+// scatters and environment shadow rays: weight = luminance of the radiance that arrived along
+// the recorded direction, over the direction's sampling pdf. Only positive-weight samples are
+// appended (compacted, order unspecified) to `samples`, which holds `sample_capacity` of them:
+// *sample_count counts every positive-weight sample offered (so it may pass the capacity) and
+// *weight_sum adds the weights of those stored. The caller zeroes both to start a new pool.
 cudaError_t launch_guide_samples(const float4* records, const uint32_t* record_count, uint32_t capacity,
-                                 const float4* path_radiance, float4* samples, uint32_t* sample_count,
-                                 float* weight_sum, cudaStream_t stream);
+                                 const float4* path_radiance, float4* samples, uint32_t sample_capacity,
+                                 uint32_t* sample_count, float* weight_sum, cudaStream_t stream);
 // Device address of the library's static render scratch (kStaticScratchWords 64-bit words) in
 // the CUDA context current on `device`, which must be the current device. The caller keeps it
 // with the other resources of that context.

@@ -449,7 +449,8 @@ __device__ __forceinline__ bool prepare_light_shadow(const DevScene& s, Lane& ln
 
 // Environment-sampling shadow ray with the power heuristic (integrator.rs:208-244). At a guided
 // vertex the competing technique is the 50/50 BSDF / guide mixture, so its pdf enters the weight.
-template <int kMode>
+// kWeights (and record mode): also the ray's weight as a guide training sample (ln.nee_w).
+template <int kMode, bool kWeights = false>
 __device__ __forceinline__ bool prepare_env_shadow(const RenderLaunch& L, const FrameJob& J, Lane& ln) {
   const DevScene& s = J.scene;
   if (s.background != 2u || !s.env_sampleable) return false;
@@ -467,7 +468,7 @@ __device__ __forceinline__ bool prepare_env_shadow(const RenderLaunch& L, const 
   }
   const float mis = power_heuristic(pdf, indirect_pdf);
   ln.pend = ln.thr * ln.alb * rad * (cs * mis / (kPiF * pdf));
-  if constexpr (kMode == kModeRecord) {
+  if constexpr (kMode == kModeRecord || kWeights) {
     // As a training sample this direction stands for the share of the incident radiance that
     // the BSDF side carries (1 - mis), the share a guided direction has to find: NEE samples the
     // visible sky far more often than cosine sampling does, and the sun's share stays near 0.
@@ -1136,11 +1137,14 @@ __global__ void __launch_bounds__(kWfBlock) wf_logic_kernel(const WavefrontLaunc
       const float4 t4 = W.thr[slot];
       const bool nee_pending = (st & kWfNeePending) != 0u;
       const bool ext = (st & (kWfTerminate | kWfExtPending)) == kWfExtPending;
+      const bool recording = W.r.g.records != nullptr;
       float4 na = make_float4(0.f, 0.f, 0.f, 0.f), nb = na;
       uint4 h = make_uint4(0u, kNoNode, 0u, 0u);
+      uint2 rr = make_uint2(kNoNode, kNoNode);
       if (nee_pending) {
         na = W.nee[2 * size_t(slot)];
         nb = W.nee[2 * size_t(slot) + 1];
+        if (recording) rr = W.rec_ref[slot];
       }
       if (ext) h = W.hit[slot];
       V3 rad = mk(r4.x, r4.y, r4.z);
@@ -1148,6 +1152,16 @@ __global__ void __launch_bounds__(kWfBlock) wf_logic_kernel(const WavefrontLaunc
       if (nee_pending) {
         rad = rad + mk(na.x, na.y, na.z);
         rad = rad + mk(nb.x, nb.y, nb.z);
+        // Recording: the scatter record takes the radiance gathered up to and including this
+        // vertex's next-event estimates; the environment record stays only if its shadow ray
+        // reached the sky (the trace launch clears the whole entry, marker included, otherwise).
+        if (rr.x != kNoNode) {
+          float* dst = reinterpret_cast<float*>(W.r.g.records + 4 * size_t(rr.x) + 3);
+          dst[0] = rad.x;
+          dst[1] = rad.y;
+          dst[2] = rad.z;
+        }
+        if (rr.y != kNoNode && nb.w == 0.0f) reinterpret_cast<float*>(W.r.g.records + 4 * size_t(rr.y) + 3)[0] = 0.0f;
       }
       bool done = (st & kWfTerminate) != 0u;
       if (ext) {
@@ -1182,10 +1196,11 @@ __global__ void __launch_bounds__(kWfBlock) wf_logic_kernel(const WavefrontLaunc
           atomicAdd(q2 + 1, double(r2.y));
           atomicAdd(q2 + 2, double(r2.z));
         }
+        if (recording) W.r.g.path_radiance[__float_as_uint(r4.w)] = make_float4(rad.x, rad.y, rad.z, 0.0f);
         ++n_paths;
         free_slot = true;
       } else {
-        W.rad[slot] = make_float4(rad.x, rad.y, rad.z, 0.0f);
+        W.rad[slot] = make_float4(rad.x, rad.y, rad.z, r4.w);
       }
     }
     // Paths that go on join the queue of their material (the shade launch rewrites their state).
@@ -1243,7 +1258,7 @@ __global__ void __launch_bounds__(kWfBlock) wf_logic_kernel(const WavefrontLaunc
           W.ray_o[slot] = make_float4(ln.ro.x, ln.ro.y, ln.ro.z, -1.0f);
           W.ray_d[slot] = make_float4(ln.rd.x, ln.rd.y, ln.rd.z, 0.0f);
           W.thr[slot] = make_float4(1.0f, 1.0f, 1.0f, __uint_as_float(ln.pixel));
-          W.rad[slot] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+          W.rad[slot] = make_float4(0.0f, 0.0f, 0.0f, __uint_as_float(uint32_t(item)));
           W.rng[slot] = make_uint4(uint32_t(ln.rng.state), uint32_t(ln.rng.state >> 32), uint32_t(ln.rng.inc),
                                    uint32_t(ln.rng.inc >> 32));
           W.state[slot] = kWfAlive | kWfExtPending | kWfEmission | (uint32_t(ln.depth) & kWfDepthMask);
@@ -1308,6 +1323,9 @@ __global__ void __launch_bounds__(128) wf_shade_kernel(const WavefrontLaunch W) 
       }
     }
     bool shadow_l = false, shadow_e = false, extend = false;
+    bool rec_s = false, rec_e = false;  // recording: this vertex's scatter and environment records
+    V3 talb = mk(0.f, 0.f, 0.f);        // throughput x albedo before the scatter
+    float env_w = 0.0f;
     uint32_t h_rec = kNoNode;  // primitive record of the vertex (sort key of the rays it spawns)
     Lane ln;
     float4 c0 = make_float4(0.f, 0.f, 0.f, 0.f), c1 = c0;
@@ -1345,17 +1363,21 @@ __global__ void __launch_bounds__(128) wf_shade_kernel(const WavefrontLaunch W) 
           sl1 = make_float4(ln.rd.x, ln.rd.y, ln.rd.z, __uint_as_float(2u * slot));
           c0 = make_float4(ln.pend.x, ln.pend.y, ln.pend.z, 0.0f);
         }
-        if (prepare_env_shadow<kGuided ? kModeGuided : kModePlain>(W.r, J, ln)) {
+        if (prepare_env_shadow<kGuided ? kModeGuided : kModePlain, true>(W.r, J, ln)) {
           shadow_e = true;
           se0 = make_float4(ln.ro.x, ln.ro.y, ln.ro.z, ln.tmax);
           se1 = make_float4(ln.rd.x, ln.rd.y, ln.rd.z, __uint_as_float(2u * slot + 1u));
-          c1 = make_float4(ln.pend.x, ln.pend.y, ln.pend.z, 0.0f);
+          // w = 1 marks the entry as not (yet) occluded: an occluded shadow ray clears it.
+          c1 = make_float4(ln.pend.x, ln.pend.y, ln.pend.z, 1.0f);
+          env_w = ln.nee_w;
+          rec_e = env_w > 0.0f;
         }
         W.nee[2 * size_t(slot)] = c0;
         W.nee[2 * size_t(slot) + 1] = c1;
         nst |= kWfNeePending;
         ln.depth -= 1;
         if (ln.depth > 0) {
+          talb = ln.thr * ln.alb;
           if (kGuided && ln.mix_slot >= 0) {
             extend = take_guided_bounce(W.r.g, W.r.g.in_mix + 10 * size_t(ln.mix_slot), ln);
           } else {
@@ -1363,6 +1385,7 @@ __global__ void __launch_bounds__(128) wf_shade_kernel(const WavefrontLaunch W) 
             extend = true;
           }
           bsdf_pdf = ln.bsdf_pdf;
+          rec_s = extend;
         }
       } else {
         const bool on = kind == kMetal ? bounce_metal(ln, m, f) : (bounce_dielectric(ln, m, f), true);
@@ -1378,6 +1401,38 @@ __global__ void __launch_bounds__(128) wf_shade_kernel(const WavefrontLaunch W) 
       W.rng[slot] = make_uint4(uint32_t(ln.rng.state), uint32_t(ln.rng.state >> 32), uint32_t(ln.rng.inc),
                                uint32_t(ln.rng.inc >> 32));
       W.state[slot] = nst;
+    }
+    if (W.r.g.records != nullptr) {
+      // Training records of the diffuse vertices (render_kernel's record mode): the scatter
+      // (position + work item, normal + T.x, direction + T.y, radiance so far + T.z, with T the
+      // throughput times albedo before the scatter; the next logic launch fills in the radiance)
+      // and the environment shadow ray with its weight. T / (the scattered throughput) is
+      // cos / (pi p) for a direction drawn with pdf p, so (radiance gathered after the vertex) / T
+      // weighs a guided direction by cos L_i / p as the training loss wants.
+      const uint32_t cap = W.r.g.record_capacity;
+      const uint32_t ps = block_append(W.r.g.record_count, rec_s, sh);
+      const uint32_t pn = block_append(W.r.g.record_count, rec_e, sh);
+      if (valid && kind == kDiffuse) {
+        uint2 ref = make_uint2(kNoNode, kNoNode);
+        const float item = reinterpret_cast<const float*>(W.rad + slot)[3];
+        if (rec_s && ps < cap) {
+          float4* r = W.r.g.records + 4 * size_t(ps);
+          r[0] = make_float4(ln.hp.x, ln.hp.y, ln.hp.z, item);
+          r[1] = make_float4(ln.hn.x, ln.hn.y, ln.hn.z, talb.x);
+          r[2] = make_float4(ln.rd.x, ln.rd.y, ln.rd.z, talb.y);
+          r[3] = make_float4(0.0f, 0.0f, 0.0f, talb.z);
+          ref.x = ps;
+        }
+        if (rec_e && pn < cap) {
+          float4* r = W.r.g.records + 4 * size_t(pn);
+          r[0] = make_float4(ln.hp.x, ln.hp.y, ln.hp.z, __uint_as_float(kNeeRecord));
+          r[1] = make_float4(ln.hn.x, ln.hn.y, ln.hn.z, 0.0f);
+          r[2] = make_float4(se1.x, se1.y, se1.z, 0.0f);
+          r[3] = make_float4(env_w, 0.0f, 0.0f, 0.0f);
+          ref.y = pn;
+        }
+        W.rec_ref[slot] = ref;
+      }
     }
     const uint32_t pl = block_append(W.q + kWfShadowCount, shadow_l, sh);
     if (shadow_l) {
@@ -1648,13 +1703,15 @@ cudaError_t launch_wavefront_iteration(const WavefrontLaunch& w, bool moments, i
 }
 
 // ------------------------------------------------------------------------ training samples
-// Training samples from the recorded scatters. Only scatters whose direction carried radiance
-// are kept (compacted through one atomic per warp): a zero weight adds nothing to the weighted
-// likelihood, and in dim interiors most recorded directions carry none, so uniform draws over
-// all records would leave almost every batch slot empty.
+// Training samples from the recorded scatters, appended to the sample pool (`out`, `out_capacity`
+// samples; `out_count` and `weight_sum` keep running across batches). Only scatters whose
+// direction carried radiance are kept (compacted through one atomic per warp): a zero weight adds
+// nothing to the weighted likelihood, and in dim interiors most recorded directions carry none,
+// so uniform draws over all records would leave almost every batch slot empty. Samples past the
+// pool's capacity are dropped, and their weights left out of the sum.
 __global__ void guide_samples_kernel(const float4* __restrict__ rec, const uint32_t* __restrict__ count,
                                      uint32_t capacity, const float4* __restrict__ path_rad,
-                                     float4* __restrict__ out, uint32_t* __restrict__ out_count,
+                                     float4* __restrict__ out, uint32_t out_capacity, uint32_t* __restrict__ out_count,
                                      float* __restrict__ weight_sum) {
   const uint32_t n = min(*count, capacity);
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1689,20 +1746,25 @@ __global__ void guide_samples_kernel(const float4* __restrict__ rec, const uint3
   }
   if (keep) {
     const uint32_t slot = base + uint32_t(__popc(mask & ((1u << lane) - 1u)));
-    out[3 * size_t(slot)] = make_float4(a.x, a.y, a.z, w);
-    out[3 * size_t(slot) + 1] = make_float4(b.x, b.y, b.z, 0.0f);
-    out[3 * size_t(slot) + 2] = make_float4(c.x, c.y, c.z, 0.0f);
+    if (slot < out_capacity) {
+      out[3 * size_t(slot)] = make_float4(a.x, a.y, a.z, w);
+      out[3 * size_t(slot) + 1] = make_float4(b.x, b.y, b.z, 0.0f);
+      out[3 * size_t(slot) + 2] = make_float4(c.x, c.y, c.z, 0.0f);
+    } else {
+      w = 0.0f;
+    }
   }
   for (int o = 16; o > 0; o >>= 1) w += __shfl_down_sync(0xffffffffu, w, o);
   if (lane == 0 && w != 0.0f) atomicAdd(weight_sum, w);
 }
 
 cudaError_t launch_guide_samples(const float4* records, const uint32_t* record_count, uint32_t capacity,
-                                 const float4* path_radiance, float4* samples, uint32_t* sample_count,
-                                 float* weight_sum, cudaStream_t stream) {
+                                 const float4* path_radiance, float4* samples, uint32_t sample_capacity,
+                                 uint32_t* sample_count, float* weight_sum, cudaStream_t stream) {
   if (capacity == 0) return cudaSuccess;
   guide_samples_kernel<<<(capacity + 255) / 256, 256, 0, stream>>>(records, record_count, capacity, path_radiance,
-                                                                   samples, sample_count, weight_sum);
+                                                                   samples, sample_capacity, sample_count,
+                                                                   weight_sum);
   return cudaGetLastError();
 }
 

@@ -236,14 +236,16 @@ class GpuRenderer:
     def render(self, samples: Optional[int] = None, max_bounces: Optional[int] = None, width: Optional[int] = None,
                height: Optional[int] = None, frame_index: int = 0, accumulate: bool = False,
                keep_moments: bool = False, block_size: int = 0, samples_per_item: int = 0, guiding: bool = False,
-               guide_record: bool = False, wave_paths: int = 0, short_stack: int = 0, refill_lanes: int = 0,
+               guide_record: int = 0, wave_paths: int = 0, short_stack: int = 0, refill_lanes: int = 0,
                guide_fraction: float = 0.0, schedule: str = "auto", ray_sort: int = 0,
                phase_timing: bool = False) -> None:
         """Traces ``samples`` paths per pixel; ``accumulate`` adds them to the previous batches.
         ``guide_fraction``: probability of sampling the network's mixture at a guided diffuse
         vertex (0 = the library's default, 0.5). ``schedule`` (plain renders): "auto",
         "megakernel" or "wavefront". ``phase_timing`` (wavefront): device time of the trace,
-        logic, shading and inference launches in ``stats()`` (trace_ms, logic_ms, ...)."""
+        logic, shading and inference launches in ``stats()`` (trace_ms, logic_ms, ...).
+        ``guide_record``: training samples of this batch into the sample pool, 1 (or True) after
+        emptying it, 2 added to it."""
         if self._params is None:
             raise RuntimeError("render before upload")
         p = self._params.copy()
@@ -262,7 +264,7 @@ class GpuRenderer:
         opts.samples_per_item = samples_per_item
         opts.keep_moments = 1 if keep_moments else 0
         opts.guiding = 1 if guiding else 0
-        opts.guide_record = 1 if guide_record else 0
+        opts.guide_record = int(guide_record)
         opts.wave_paths = wave_paths
         opts.short_stack = short_stack
         opts.refill_lanes = refill_lanes
@@ -392,7 +394,7 @@ class GpuRenderer:
         return losses[:steps]
 
     def guide_train_recorded(self, steps: int, batch: int, lr: float = 1e-2, seed: int = 0):
-        """Adam steps on the samples recorded by the last render(guide_record=True)."""
+        """Adam steps on the sample pool (every render with guide_record since the last with 1)."""
         losses = np.empty(max(steps, 1), np.float32)
         n = ctypes.c_uint32()
         self._check(self._lib.tc_guide_train_recorded(self._ctx, steps, batch, lr, seed, losses.ctypes.data,
@@ -400,7 +402,7 @@ class GpuRenderer:
         return losses[:steps], int(n.value)
 
     def guide_recorded_samples(self) -> np.ndarray:
-        """Training samples of the last guide_record batch: (n, 12) position + weight, normal, direction."""
+        """The sample pool: (n, 12) position + weight, normal, direction."""
         count = ctypes.c_uint32()
         self._check(self._lib.tc_guide_recorded_samples(self._ctx, None, 0, ctypes.byref(count)))
         out = np.empty((count.value, 12), np.float32)
