@@ -35,7 +35,7 @@ TRAIN_STEPS = 200
 # mixture, weighted by cos / (pi p)) join the pool and the network takes ONLINE_STEPS more Adam
 # steps of ONLINE_BATCH samples on the whole pool, so the fit sharpens only as fast as its data
 # grows (window room, 3 seeds, trimmed time fraction: 0.87-0.96 and one seed that never reached
-# plain's error without it; 0.72-0.88 with 25 steps of 8,192; 0.73-0.79 with 100 of 32,768).
+# plain's error without it; 0.72-0.88 with 25 steps of 8,192; 0.72-0.81 with 100 of 32,768).
 ONLINE_STEPS = 100
 ONLINE_BATCH = 32768
 
