@@ -1089,36 +1089,55 @@ __device__ __forceinline__ uint32_t wf_sort_key(const WavefrontLaunch& W, V3 d, 
   return (shadow ? uint32_t(8 * kWfSortBuckets) : 0u) + octant * kWfSortBuckets + bucket;
 }
 
-// Appends the threads of the block whose `pred` holds to a queue counter with one atomic per
-// block (all the block's warps append to the same few counters in every launch, so per-warp atomics
-// would queue up at those addresses); returns each such thread's position. Every thread of the
-// block (at most kWfBlock threads) must call it together; `sh` is kWfBlock / 32 + 1 words of
-// shared memory.
+// Reserves room on N queue counters for the whole block at once: thread t asks for n[i] entries of
+// counter i and receives the first of them in pos[i]. One atomic per counter per block (all the
+// block's warps append to the same few counters in every launch, so per-warp atomics would queue
+// up at those addresses): warp-inclusive scans by shuffles, one pass over the warps' totals by N
+// threads, two barriers. Every thread of the block (whole warps, at most kWfBlock threads) calls
+// it together. `sh` holds N x kWfScanStride words; the next call may reuse it without a barrier in
+// between, because before that call's first barrier a warp writes only its own totals, which no
+// other warp reads.
 constexpr int kWfBlock = 256;
-__device__ __forceinline__ uint32_t block_append(uint32_t* counter, bool pred, uint32_t* sh) {
-  const unsigned m = __ballot_sync(0xffffffffu, pred);
+constexpr int kWfScanStride = kWfBlock / 32 + 1;
+template <int N>
+__device__ __forceinline__ void block_reserve(uint32_t* const (&counter)[N], const uint32_t (&n)[N],
+                                              uint32_t (&pos)[N], uint32_t* sh) {
+  const unsigned lane = threadIdx.x & 31u;
   const int warp = int(threadIdx.x >> 5);
-  if ((threadIdx.x & 31u) == 0) sh[warp] = uint32_t(__popc(m));
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    uint32_t run = 0;
-    for (int w = 0; w < int(blockDim.x >> 5); ++w) {
-      const uint32_t c = sh[w];
-      sh[w] = run;
-      run += c;
+  uint32_t incl[N];
+#pragma unroll
+  for (int i = 0; i < N; ++i) {
+    uint32_t v = n[i];
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t u = __shfl_up_sync(0xffffffffu, v, o);
+      if (lane >= unsigned(o)) v += u;
     }
-    sh[kWfBlock / 32] = run ? atomicAdd(counter, run) : 0u;
+    incl[i] = v;
+    if (lane == 31u) sh[i * kWfScanStride + warp] = v;
   }
   __syncthreads();
-  const uint32_t pos = sh[kWfBlock / 32] + sh[warp] + uint32_t(__popc(m & lanes_below()));
-  __syncthreads();  // sh is reused by the next call
-  return pos;
+  if (threadIdx.x < unsigned(N)) {
+    const int i = int(threadIdx.x);
+    uint32_t run = 0;
+    for (int w = 0; w < int(blockDim.x >> 5); ++w) {
+      const uint32_t c = sh[i * kWfScanStride + w];
+      sh[i * kWfScanStride + w] = run;
+      run += c;
+    }
+    sh[i * kWfScanStride + kWfScanStride - 1] = run ? atomicAdd(counter[i], run) : 0u;
+  }
+  __syncthreads();
+#pragma unroll
+  for (int i = 0; i < N; ++i)
+    pos[i] = sh[i * kWfScanStride + kWfScanStride - 1] + sh[i * kWfScanStride + warp] + (incl[i] - n[i]);
 }
 
 template <bool kMoments, bool kGuided>
 __global__ void __launch_bounds__(kWfBlock) wf_logic_kernel(const WavefrontLaunch W) {
-  __shared__ uint32_t sh[kWfBlock / 32 + 1];
+  __shared__ uint32_t sh[3 * kWfScanStride];
   __shared__ unsigned long long s_first;
+  __shared__ uint32_t s_started, s_ext;
   const FrameJob& J = W.r.f;
   const DevScene& s = J.scene;
   const uint32_t npix = J.width * J.height;
@@ -1204,10 +1223,14 @@ __global__ void __launch_bounds__(kWfBlock) wf_logic_kernel(const WavefrontLaunc
       }
     }
     // Paths that go on join the queue of their material (the shade launch rewrites their state).
-#pragma unroll
-    for (int k = 0; k < 3; ++k) {
-      const uint32_t pos = block_append(W.q + kWfMatCount + k, kind == k, sh);
-      if (kind == k) {
+    {
+      uint32_t* const counters[3] = {W.q + kWfMatCount, W.q + kWfMatCount + 1, W.q + kWfMatCount + 2};
+      const uint32_t want[3] = {kind == 0 ? 1u : 0u, kind == 1 ? 1u : 0u, kind == 2 ? 1u : 0u};
+      uint32_t at[3];
+      block_reserve<3>(counters, want, at, sh);
+      if (kind >= 0) {
+        const int k = kind;
+        const uint32_t pos = at[k];
         W.mat_q[size_t(k) * W.capacity + pos] = slot;
         if constexpr (kGuided) {
           if (k == kDiffuse) {
@@ -1228,7 +1251,9 @@ __global__ void __launch_bounds__(kWfBlock) wf_logic_kernel(const WavefrontLaunc
       }
     }
     // Free slots start new camera paths: consecutive work items are consecutive pixels of one
-    // sample, so a warp's new rays are neighbours. One atomic on the work counter per block.
+    // sample, so a warp's new rays are neighbours. Per block one atomic on the work counter and one
+    // on the extension queue for the paths that start: the block's first s_started free slots in
+    // block order (items past the frame's last one start nothing).
     bool started = false;
     {
       const unsigned want = __ballot_sync(0xffffffffu, free_slot);
@@ -1242,14 +1267,18 @@ __global__ void __launch_bounds__(kWfBlock) wf_logic_kernel(const WavefrontLaunc
           sh[w] = run;
           run += c;
         }
-        s_first = run ? atomicAdd(W.r.work_counter, (unsigned long long)run) : 0ull;
+        const unsigned long long first = run ? atomicAdd(W.r.work_counter, (unsigned long long)run) : 0ull;
+        const uint64_t left = first < W.r.total_items ? W.r.total_items - first : 0ull;
+        const uint32_t n = left < run ? uint32_t(left) : run;
+        s_first = first;
+        s_started = n;
+        s_ext = n ? atomicAdd(W.q + kWfExtCount, n) : 0u;
       }
       __syncthreads();
-      const unsigned long long first = s_first + sh[warp];
-      __syncthreads();
       if (free_slot) {
-        const uint64_t item = first + __popc(want & lanes_below());
-        if (item < W.r.total_items) {
+        const uint32_t rank = sh[warp] + uint32_t(__popc(want & lanes_below()));
+        if (rank < s_started) {
+          const uint64_t item = s_first + rank;
           const uint32_t chunk = uint32_t(item / npix);
           Lane ln;
           ln.pixel = uint32_t(item - uint64_t(chunk) * npix);
@@ -1262,16 +1291,14 @@ __global__ void __launch_bounds__(kWfBlock) wf_logic_kernel(const WavefrontLaunc
           W.rng[slot] = make_uint4(uint32_t(ln.rng.state), uint32_t(ln.rng.state >> 32), uint32_t(ln.rng.inc),
                                    uint32_t(ln.rng.inc >> 32));
           W.state[slot] = kWfAlive | kWfExtPending | kWfEmission | (uint32_t(ln.depth) & kWfDepthMask);
+          const uint32_t pos = s_ext + rank;
+          W.ext_q[pos] = slot;
+          if (W.sorted) W.ext_key[pos] = wf_sort_key(W, mk(0.f, 0.f, 0.f), kNoNode, false);
           started = true;
         } else if (st & kWfAlive) {
           W.state[slot] = 0u;
         }
       }
-    }
-    const uint32_t pos = block_append(W.q + kWfExtCount, started, sh);
-    if (started) {
-      W.ext_q[pos] = slot;
-      if (W.sorted) W.ext_key[pos] = wf_sort_key(W, mk(0.f, 0.f, 0.f), kNoNode, false);
     }
     n_live += (kind >= 0 || started) ? 1u : 0u;
   }
@@ -1296,11 +1323,13 @@ __global__ void __launch_bounds__(kWfBlock) wf_logic_kernel(const WavefrontLaunc
   }
 }
 
+// At most 80 registers (6 blocks of 128 per SM): the kernel waits on memory, so the warps it keeps
+// resident count for more than the few spilled words this costs.
 template <bool kGuided>
-__global__ void __launch_bounds__(128) wf_shade_kernel(const WavefrontLaunch W) {
+__global__ void __launch_bounds__(128, 6) wf_shade_kernel(const WavefrontLaunch W) {
   const FrameJob& J = W.r.f;
   const DevScene& s = J.scene;
-  __shared__ uint32_t sh[kWfBlock / 32 + 1];
+  __shared__ uint32_t sh[3 * kWfScanStride];
   const uint32_t n0 = W.q[kWfMatCount], n1 = W.q[kWfMatCount + 1], n2 = W.q[kWfMatCount + 2];
   const uint32_t total = n0 + n1 + n2;
   const uint32_t stride = gridDim.x * blockDim.x;
@@ -1402,7 +1431,15 @@ __global__ void __launch_bounds__(128) wf_shade_kernel(const WavefrontLaunch W) 
                                uint32_t(ln.rng.inc >> 32));
       W.state[slot] = nst;
     }
-    if (W.r.g.records != nullptr) {
+    // Queue positions for this step's shadow rays, extension rays and (recording) training records:
+    // one block-wide reservation on the three counters.
+    const bool recording = W.r.g.records != nullptr;
+    uint32_t* const counters[3] = {W.q + kWfShadowCount, W.q + kWfExtCount, W.r.g.record_count};
+    const uint32_t want[3] = {uint32_t(shadow_l) + uint32_t(shadow_e), extend ? 1u : 0u,
+                              recording ? uint32_t(rec_s) + uint32_t(rec_e) : 0u};
+    uint32_t at[3];
+    block_reserve<3>(counters, want, at, sh);
+    if (recording && valid && kind == kDiffuse) {
       // Training records of the diffuse vertices (render_kernel's record mode): the scatter
       // (position + work item, normal + T.x, direction + T.y, radiance so far + T.z, with T the
       // throughput times albedo before the scatter; the next logic launch fills in the radiance)
@@ -1410,44 +1447,41 @@ __global__ void __launch_bounds__(128) wf_shade_kernel(const WavefrontLaunch W) 
       // cos / (pi p) for a direction drawn with pdf p, so (radiance gathered after the vertex) / T
       // weighs a guided direction by cos L_i / p as the training loss wants.
       const uint32_t cap = W.r.g.record_capacity;
-      const uint32_t ps = block_append(W.r.g.record_count, rec_s, sh);
-      const uint32_t pn = block_append(W.r.g.record_count, rec_e, sh);
-      if (valid && kind == kDiffuse) {
-        uint2 ref = make_uint2(kNoNode, kNoNode);
-        const float item = reinterpret_cast<const float*>(W.rad + slot)[3];
-        if (rec_s && ps < cap) {
-          float4* r = W.r.g.records + 4 * size_t(ps);
-          r[0] = make_float4(ln.hp.x, ln.hp.y, ln.hp.z, item);
-          r[1] = make_float4(ln.hn.x, ln.hn.y, ln.hn.z, talb.x);
-          r[2] = make_float4(ln.rd.x, ln.rd.y, ln.rd.z, talb.y);
-          r[3] = make_float4(0.0f, 0.0f, 0.0f, talb.z);
-          ref.x = ps;
-        }
-        if (rec_e && pn < cap) {
-          float4* r = W.r.g.records + 4 * size_t(pn);
-          r[0] = make_float4(ln.hp.x, ln.hp.y, ln.hp.z, __uint_as_float(kNeeRecord));
-          r[1] = make_float4(ln.hn.x, ln.hn.y, ln.hn.z, 0.0f);
-          r[2] = make_float4(se1.x, se1.y, se1.z, 0.0f);
-          r[3] = make_float4(env_w, 0.0f, 0.0f, 0.0f);
-          ref.y = pn;
-        }
-        W.rec_ref[slot] = ref;
+      const uint32_t ps = at[2], pn = at[2] + (rec_s ? 1u : 0u);
+      uint2 ref = make_uint2(kNoNode, kNoNode);
+      const float item = reinterpret_cast<const float*>(W.rad + slot)[3];
+      if (rec_s && ps < cap) {
+        float4* r = W.r.g.records + 4 * size_t(ps);
+        r[0] = make_float4(ln.hp.x, ln.hp.y, ln.hp.z, item);
+        r[1] = make_float4(ln.hn.x, ln.hn.y, ln.hn.z, talb.x);
+        r[2] = make_float4(ln.rd.x, ln.rd.y, ln.rd.z, talb.y);
+        r[3] = make_float4(0.0f, 0.0f, 0.0f, talb.z);
+        ref.x = ps;
       }
+      if (rec_e && pn < cap) {
+        float4* r = W.r.g.records + 4 * size_t(pn);
+        r[0] = make_float4(ln.hp.x, ln.hp.y, ln.hp.z, __uint_as_float(kNeeRecord));
+        r[1] = make_float4(ln.hn.x, ln.hn.y, ln.hn.z, 0.0f);
+        r[2] = make_float4(se1.x, se1.y, se1.z, 0.0f);
+        r[3] = make_float4(env_w, 0.0f, 0.0f, 0.0f);
+        ref.y = pn;
+      }
+      W.rec_ref[slot] = ref;
     }
-    const uint32_t pl = block_append(W.q + kWfShadowCount, shadow_l, sh);
     if (shadow_l) {
+      const uint32_t pl = at[0];
       if (W.sorted) W.shadow_key[pl] = wf_sort_key(W, mk(sl1.x, sl1.y, sl1.z), h_rec, true);
       W.shadow_q[2 * size_t(pl)] = sl0;
       W.shadow_q[2 * size_t(pl) + 1] = sl1;
     }
-    const uint32_t pe = block_append(W.q + kWfShadowCount, shadow_e, sh);
     if (shadow_e) {
+      const uint32_t pe = at[0] + (shadow_l ? 1u : 0u);
       if (W.sorted) W.shadow_key[pe] = wf_sort_key(W, mk(se1.x, se1.y, se1.z), h_rec, true);
       W.shadow_q[2 * size_t(pe)] = se0;
       W.shadow_q[2 * size_t(pe) + 1] = se1;
     }
-    const uint32_t px = block_append(W.q + kWfExtCount, extend, sh);
     if (extend) {
+      const uint32_t px = at[1];
       W.ext_q[px] = slot;
       if (W.sorted) W.ext_key[px] = wf_sort_key(W, ln.rd, h_rec, false);
     }
