@@ -1135,13 +1135,14 @@ __device__ __forceinline__ void block_reserve(uint32_t* const (&counter)[N], con
 
 template <bool kMoments, bool kGuided>
 __global__ void __launch_bounds__(kWfBlock) wf_logic_kernel(const WavefrontLaunch W) {
-  __shared__ uint32_t sh[3 * kWfScanStride];
+  __shared__ uint32_t sh[4 * kWfScanStride];
   __shared__ unsigned long long s_first;
-  __shared__ uint32_t s_started, s_ext;
+  __shared__ uint32_t s_started;
   const FrameJob& J = W.r.f;
   const DevScene& s = J.scene;
   const uint32_t npix = J.width * J.height;
   uint32_t n_paths = 0, n_live = 0;
+
   // One slot per thread; whole warps are either in range or the last partial warp.
   {
     const uint32_t slot = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1222,82 +1223,89 @@ __global__ void __launch_bounds__(kWfBlock) wf_logic_kernel(const WavefrontLaunc
         W.rad[slot] = make_float4(rad.x, rad.y, rad.z, r4.w);
       }
     }
-    // Paths that go on join the queue of their material (the shade launch rewrites their state).
-    {
-      uint32_t* const counters[3] = {W.q + kWfMatCount, W.q + kWfMatCount + 1, W.q + kWfMatCount + 2};
-      const uint32_t want[3] = {kind == 0 ? 1u : 0u, kind == 1 ? 1u : 0u, kind == 2 ? 1u : 0u};
-      uint32_t at[3];
-      block_reserve<3>(counters, want, at, sh);
-      if (kind >= 0) {
-        const int k = kind;
-        const uint32_t pos = at[k];
-        W.mat_q[size_t(k) * W.capacity + pos] = slot;
-        if constexpr (kGuided) {
-          if (k == kDiffuse) {
-            // The query of the guide's inference launch, at the vertex's place in the diffuse
-            // queue: the surface point and shading normal the shade launch will scatter from.
-            // Vertices that only do next-event estimation (depth 1) get a query too, unused.
-            const uint4 h = W.hit[slot];
-            const float4 o4 = W.ray_o[slot], d4 = W.ray_d[slot];
-            TraceResult tr;
-            tr.t = __uint_as_float(h.x);
-            tr.rec = h.y;
-            tr.tag = h.z;
-            const Surface f = surface_at(s, mk(o4.x, o4.y, o4.z), mk(d4.x, d4.y, d4.z), tr);
-            W.query[2 * size_t(pos)] = make_float4(f.hp.x, f.hp.y, f.hp.z, 0.0f);
-            W.query[2 * size_t(pos) + 1] = make_float4(f.nrm.x, f.nrm.y, f.nrm.z, 0.0f);
-          }
-        }
-      }
+    // One block-wide pass reserves room for every append of this launch: threads 0-2 on the
+    // material queues (paths that go on; the shade launch rewrites their state), thread 3 on the
+    // work counter for free slots and then on the extension queue for the camera paths that do
+    // start (the block's first s_started free slots in block order: items past the frame's last
+    // one start nothing). Consecutive work items are consecutive pixels of one sample, so a warp's
+    // new rays are neighbours.
+    const int warp = int(threadIdx.x >> 5);
+    const unsigned m_mat[3] = {__ballot_sync(0xffffffffu, kind == 0), __ballot_sync(0xffffffffu, kind == 1),
+                               __ballot_sync(0xffffffffu, kind == 2)};
+    const unsigned m_free = __ballot_sync(0xffffffffu, free_slot);
+    if ((threadIdx.x & 31u) == 0) {
+#pragma unroll
+      for (int k = 0; k < 3; ++k) sh[k * kWfScanStride + warp] = uint32_t(__popc(m_mat[k]));
+      sh[3 * kWfScanStride + warp] = uint32_t(__popc(m_free));
     }
-    // Free slots start new camera paths: consecutive work items are consecutive pixels of one
-    // sample, so a warp's new rays are neighbours. Per block one atomic on the work counter and one
-    // on the extension queue for the paths that start: the block's first s_started free slots in
-    // block order (items past the frame's last one start nothing).
-    bool started = false;
-    {
-      const unsigned want = __ballot_sync(0xffffffffu, free_slot);
-      const int warp = int(threadIdx.x >> 5);
-      if ((threadIdx.x & 31u) == 0) sh[warp] = uint32_t(__popc(want));
-      __syncthreads();
-      if (threadIdx.x == 0) {
-        uint32_t run = 0;
-        for (int w = 0; w < int(blockDim.x >> 5); ++w) {
-          const uint32_t c = sh[w];
-          sh[w] = run;
-          run += c;
-        }
+    __syncthreads();
+    if (threadIdx.x < 4u) {
+      const int k = int(threadIdx.x);
+      uint32_t run = 0;
+      for (int w = 0; w < int(blockDim.x >> 5); ++w) {
+        const uint32_t c = sh[k * kWfScanStride + w];
+        sh[k * kWfScanStride + w] = run;
+        run += c;
+      }
+      uint32_t base = 0;
+      if (k < 3) {
+        base = run ? atomicAdd(W.q + kWfMatCount + k, run) : 0u;
+      } else {
         const unsigned long long first = run ? atomicAdd(W.r.work_counter, (unsigned long long)run) : 0ull;
         const uint64_t left = first < W.r.total_items ? W.r.total_items - first : 0ull;
         const uint32_t n = left < run ? uint32_t(left) : run;
         s_first = first;
         s_started = n;
-        s_ext = n ? atomicAdd(W.q + kWfExtCount, n) : 0u;
+        base = n ? atomicAdd(W.q + kWfExtCount, n) : 0u;
       }
-      __syncthreads();
-      if (free_slot) {
-        const uint32_t rank = sh[warp] + uint32_t(__popc(want & lanes_below()));
-        if (rank < s_started) {
-          const uint64_t item = s_first + rank;
-          const uint32_t chunk = uint32_t(item / npix);
-          Lane ln;
-          ln.pixel = uint32_t(item - uint64_t(chunk) * npix);
-          ln.sample = J.sample_base + chunk;
-          start_sample(J, ln);
-          W.ray_o[slot] = make_float4(ln.ro.x, ln.ro.y, ln.ro.z, -1.0f);
-          W.ray_d[slot] = make_float4(ln.rd.x, ln.rd.y, ln.rd.z, 0.0f);
-          W.thr[slot] = make_float4(1.0f, 1.0f, 1.0f, __uint_as_float(ln.pixel));
-          W.rad[slot] = make_float4(0.0f, 0.0f, 0.0f, __uint_as_float(uint32_t(item)));
-          W.rng[slot] = make_uint4(uint32_t(ln.rng.state), uint32_t(ln.rng.state >> 32), uint32_t(ln.rng.inc),
-                                   uint32_t(ln.rng.inc >> 32));
-          W.state[slot] = kWfAlive | kWfExtPending | kWfEmission | (uint32_t(ln.depth) & kWfDepthMask);
-          const uint32_t pos = s_ext + rank;
-          W.ext_q[pos] = slot;
-          if (W.sorted) W.ext_key[pos] = wf_sort_key(W, mk(0.f, 0.f, 0.f), kNoNode, false);
-          started = true;
-        } else if (st & kWfAlive) {
-          W.state[slot] = 0u;
+      sh[k * kWfScanStride + kWfScanStride - 1] = base;
+    }
+    __syncthreads();
+    if (kind >= 0) {
+      const int k = kind;
+      const uint32_t pos = sh[k * kWfScanStride + kWfScanStride - 1] + sh[k * kWfScanStride + warp] +
+                           uint32_t(__popc(m_mat[k] & lanes_below()));
+      W.mat_q[size_t(k) * W.capacity + pos] = slot;
+      if constexpr (kGuided) {
+        if (k == kDiffuse) {
+          // The query of the guide's inference launch, at the vertex's place in the diffuse
+          // queue: the surface point and shading normal the shade launch will scatter from.
+          // Vertices that only do next-event estimation (depth 1) get a query too, unused.
+          const uint4 h = W.hit[slot];
+          const float4 o4 = W.ray_o[slot], d4 = W.ray_d[slot];
+          TraceResult tr;
+          tr.t = __uint_as_float(h.x);
+          tr.rec = h.y;
+          tr.tag = h.z;
+          const Surface f = surface_at(s, mk(o4.x, o4.y, o4.z), mk(d4.x, d4.y, d4.z), tr);
+          W.query[2 * size_t(pos)] = make_float4(f.hp.x, f.hp.y, f.hp.z, 0.0f);
+          W.query[2 * size_t(pos) + 1] = make_float4(f.nrm.x, f.nrm.y, f.nrm.z, 0.0f);
         }
+      }
+    }
+    bool started = false;
+    if (free_slot) {
+      const uint32_t rank = sh[3 * kWfScanStride + warp] + uint32_t(__popc(m_free & lanes_below()));
+      if (rank < s_started) {
+        const uint64_t item = s_first + rank;
+        const uint32_t chunk = uint32_t(item / npix);
+        Lane ln;
+        ln.pixel = uint32_t(item - uint64_t(chunk) * npix);
+        ln.sample = J.sample_base + chunk;
+        start_sample(J, ln);
+        W.ray_o[slot] = make_float4(ln.ro.x, ln.ro.y, ln.ro.z, -1.0f);
+        W.ray_d[slot] = make_float4(ln.rd.x, ln.rd.y, ln.rd.z, 0.0f);
+        W.thr[slot] = make_float4(1.0f, 1.0f, 1.0f, __uint_as_float(ln.pixel));
+        W.rad[slot] = make_float4(0.0f, 0.0f, 0.0f, __uint_as_float(uint32_t(item)));
+        W.rng[slot] = make_uint4(uint32_t(ln.rng.state), uint32_t(ln.rng.state >> 32), uint32_t(ln.rng.inc),
+                                 uint32_t(ln.rng.inc >> 32));
+        W.state[slot] = kWfAlive | kWfExtPending | kWfEmission | (uint32_t(ln.depth) & kWfDepthMask);
+        const uint32_t pos = sh[3 * kWfScanStride + kWfScanStride - 1] + rank;
+        W.ext_q[pos] = slot;
+        if (W.sorted) W.ext_key[pos] = wf_sort_key(W, mk(0.f, 0.f, 0.f), kNoNode, false);
+        started = true;
+      } else if (st & kWfAlive) {
+        W.state[slot] = 0u;
       }
     }
     n_live += (kind >= 0 || started) ? 1u : 0u;
