@@ -92,6 +92,7 @@ struct tc_context {
   tcb::DevScene scene{};
   DevBuf pairs, prims, materials, lights, attributes, texels;
   DevBuf env_rgb, env_marginal, env_conditional, env_pdf, env_row_sums, env_total;
+  DevBuf env_alias_cond, env_alias_marg, env_alias_q, env_alias_idx;  // alias tables and their build scratch
   uint32_t sphere_count = 0, triangle_count = 0, material_count = 0, light_count = 0, bvh_prims = 0;
   uint32_t bvh_depth = 0;
   size_t pair_count = 0;
@@ -631,16 +632,23 @@ int tc_upload_scene(tc_context* ctx, const tc_scene_data* sd) {
     TC_CUDA(ctx, ctx->env_pdf.reserve(sizeof(float) * n));
     TC_CUDA(ctx, ctx->env_row_sums.reserve(sizeof(double) * eh));
     TC_CUDA(ctx, ctx->env_total.reserve(sizeof(double)));
+    const size_t span = std::max<size_t>(ew, eh);
+    TC_CUDA(ctx, ctx->env_alias_cond.reserve(sizeof(uint2) * n));
+    TC_CUDA(ctx, ctx->env_alias_marg.reserve(sizeof(uint2) * eh));
+    TC_CUDA(ctx, ctx->env_alias_q.reserve(sizeof(double) * span * (size_t(eh) + 1)));
+    TC_CUDA(ctx, ctx->env_alias_idx.reserve(2 * sizeof(uint32_t) * span * (size_t(eh) + 1)));
     TC_CUDA(ctx, tcb::launch_env_tables(ctx->env_rgb.as<float4>(), ew, eh, sd->params.environment_intensity,
                                         ctx->env_marginal.as<float>(), ctx->env_conditional.as<float>(),
                                         ctx->env_pdf.as<float>(), ctx->env_row_sums.as<double>(),
-                                        ctx->env_total.as<double>(), st));
+                                        ctx->env_total.as<double>(), ctx->env_alias_q.as<double>(),
+                                        ctx->env_alias_idx.as<uint32_t>(), ctx->env_alias_cond.as<uint2>(),
+                                        ctx->env_alias_marg.as<uint2>(), st));
     double total = 0.0;
     TC_CUDA(ctx, cudaMemcpyAsync(&total, ctx->env_total.ptr, sizeof(double), cudaMemcpyDeviceToHost, st));
     TC_CUDA(ctx, cudaStreamSynchronize(st));
     s.env_rgb = ctx->env_rgb.as<float4>();
-    s.env_marginal = ctx->env_marginal.as<float>();
-    s.env_conditional = ctx->env_conditional.as<float>();
+    s.env_alias_marg = ctx->env_alias_marg.as<uint2>();
+    s.env_alias_cond = ctx->env_alias_cond.as<uint2>();
     s.env_pdf = ctx->env_pdf.as<float>();
     s.env_width = ew;
     s.env_height = eh;

@@ -24,8 +24,8 @@ struct DevScene {
   // per-texel solid-angle density numerator p(x,y)*W*H/(2*pi^2) (W*H), all FP32 built from FP64
   // prefix sums.
   const float4* env_rgb;
-  const float* env_marginal;
-  const float* env_conditional;
+  const uint2* env_alias_marg;   // alias table over rows (env_height entries)
+  const uint2* env_alias_cond;   // per row, alias table over its columns (env_width entries each)
   const float* env_pdf;
   uint32_t env_width, env_height;
   float env_intensity;
@@ -212,6 +212,7 @@ cudaError_t launch_resolve(const double* accum, uint32_t pixels, double inv_samp
 // Environment importance tables from RGB texels; `row_sums` is FP64 scratch of H entries.
 cudaError_t launch_env_tables(const float4* rgb, uint32_t w, uint32_t h, float intensity, float* marginal,
                               float* conditional, float* pdf, double* row_sums, double* total_out,
+                              double* alias_q, uint32_t* alias_idx, uint2* cond_alias, uint2* marg_alias,
                               cudaStream_t stream);
 
 }  // namespace tcb

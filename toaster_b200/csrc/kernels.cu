@@ -125,29 +125,31 @@ __device__ float env_pdf(const DevScene& s, V3 d) {
   return (p > 0.0f && st > 0.0f) ? p / st : 0.0f;
 }
 
-// First index in [0, n) whose CDF value is > x (the reference's partition_point(c <= x)).
-__device__ __forceinline__ uint32_t upper_bound(const float* cdf, uint32_t n, float x) {
-  uint32_t lo = 0, hi = n;
-  while (lo < hi) {
-    const uint32_t mid = (lo + hi) >> 1;
-    if (__ldg(cdf + mid) <= x) lo = mid + 1;
-    else hi = mid;
-  }
-  return lo;
-}
-
-// environment.rs:159-189 with the flat CDF split into a marginal row CDF and conditional column
-// CDFs: the same texel probabilities, found with two short searches instead of one long one.
+// environment.rs:159-189: a texel drawn with the importance distribution's probability, then a
+// uniform point inside it. The reference inverts one flat CDF by binary search; here the texel
+// comes from two Walker alias tables (the marginal over rows, then the row's conditional over
+// columns: two dependent loads instead of a search of about twenty), with the same texel
+// probabilities. u1 draws the row, u2 the column, and the column draw's leftover fraction
+// (uniform in [0, 1) given the column) places the point across the texel; u3 places it down.
 __device__ bool env_sample(const DevScene& s, float u1, float u2, float u3, V3& dir, V3& rad, float& pdf) {
   if (!s.env_sampleable) return false;
-  const float sel = unit_interval(u1);
-  const uint32_t y = min(upper_bound(s.env_marginal, s.env_height, sel), s.env_height - 1);
-  const float lo = y ? __ldg(s.env_marginal + y - 1) : 0.0f;
-  const float hi = __ldg(s.env_marginal + y);
-  const float sel2 = unit_interval((sel - lo) / (hi - lo));
-  const float* row = s.env_conditional + size_t(y) * s.env_width;
-  const uint32_t x = min(upper_bound(row, s.env_width, sel2), s.env_width - 1);
-  const float u = (float(x) + unit_interval(u2)) / float(s.env_width);
+  const float fy = unit_interval(u1) * float(s.env_height);
+  uint32_t y = min(uint32_t(fy), s.env_height - 1);
+  const uint2 ry = __ldg(s.env_alias_marg + y);
+  if (!(fy - float(y) < __uint_as_float(ry.x))) y = ry.y;
+  const float fx = unit_interval(u2) * float(s.env_width);
+  uint32_t x = min(uint32_t(fx), s.env_width - 1);
+  const float g = fx - float(x);
+  const uint2 rx = __ldg(s.env_alias_cond + size_t(y) * s.env_width + x);
+  const float keep = __uint_as_float(rx.x);
+  float jx;
+  if (g < keep) {
+    jx = g / keep;
+  } else {
+    x = rx.y;
+    jx = (g - keep) / (1.0f - keep);
+  }
+  const float u = (float(x) + unit_interval(jx)) / float(s.env_width);
   const float v = (float(y) + unit_interval(u3)) / float(s.env_height);
   const float theta = kPiF * v;
   const float phi = 2.0f * kPiF * (u - 0.5f - s.env_rotation_turns);
@@ -1974,14 +1976,71 @@ __global__ void env_pdf_kernel(const float* __restrict__ marginal, const float* 
   pdf[i] = float(p * double(w) * double(h) / (2.0 * CUDART_PI * CUDART_PI));
 }
 
+// Walker alias tables of the importance distribution (Vose's construction, one thread per table):
+// table y < h is row y's distribution over its columns, table h the marginal over rows. The
+// weights are the FP32 CDF differences env_pdf_kernel turns into densities, so the sampler draws
+// each texel with exactly the probability its density reports. An entry is (probability of
+// keeping the drawn index, as float bits; the index taken otherwise). Scratch per table: max(w, h)
+// doubles and 2 x max(w, h) indices.
+__global__ void env_alias_kernel(const float* __restrict__ marginal, const float* __restrict__ conditional, uint32_t w,
+                                 uint32_t h, double* __restrict__ scratch_q, uint32_t* __restrict__ scratch_idx,
+                                 uint2* __restrict__ cond_alias, uint2* __restrict__ marg_alias) {
+  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t > h) return;
+  const uint32_t span = max(w, h);
+  const bool marg = t == h;
+  const uint32_t n = marg ? h : w;
+  const float* cdf = marg ? marginal : conditional + size_t(t) * w;
+  uint2* out = marg ? marg_alias : cond_alias + size_t(t) * w;
+  double* q = scratch_q + size_t(t) * span;
+  uint32_t* small = scratch_idx + size_t(t) * 2 * span;
+  uint32_t* large = small + span;
+  double sum = 0.0;
+  for (uint32_t i = 0; i < n; ++i) {
+    const double p = fmax(double(cdf[i]) - (i ? double(cdf[i - 1]) : 0.0), 0.0);
+    q[i] = p;
+    sum += p;
+  }
+  if (!(sum > 0.0) || !isfinite(sum)) {
+    for (uint32_t i = 0; i < n; ++i) out[i] = make_uint2(__float_as_uint(1.0f), i);
+    return;
+  }
+  const double scale = double(n) / sum;
+  uint32_t ns = 0, nl = 0;
+  for (uint32_t i = 0; i < n; ++i) {
+    q[i] *= scale;
+    if (q[i] < 1.0) small[ns++] = i;
+    else large[nl++] = i;
+  }
+  while (ns && nl) {
+    const uint32_t sm = small[--ns], lg = large[--nl];
+    out[sm] = make_uint2(__float_as_uint(float(q[sm])), lg);
+    q[lg] = (q[lg] + q[sm]) - 1.0;
+    if (q[lg] < 1.0) small[ns++] = lg;
+    else large[nl++] = lg;
+  }
+  // Leftovers hold probability 1 up to rounding.
+  while (nl) {
+    const uint32_t lg = large[--nl];
+    out[lg] = make_uint2(__float_as_uint(1.0f), lg);
+  }
+  while (ns) {
+    const uint32_t sm = small[--ns];
+    out[sm] = make_uint2(__float_as_uint(1.0f), sm);
+  }
+}
+
 cudaError_t launch_env_tables(const float4* rgb, uint32_t w, uint32_t h, float intensity, float* marginal,
                               float* conditional, float* pdf, double* row_sums, double* total_out,
+                              double* alias_q, uint32_t* alias_idx, uint2* cond_alias, uint2* marg_alias,
                               cudaStream_t stream) {
   if (w == 0 || h == 0) return cudaSuccess;
   env_rows_kernel<<<h, kEnvBlock, 0, stream>>>(rgb, w, h, double(intensity), conditional, row_sums);
   env_marginal_kernel<<<1, kEnvBlock, 0, stream>>>(row_sums, h, marginal, total_out);
   const size_t n = size_t(w) * h;
   env_pdf_kernel<<<unsigned((n + 255) / 256), 256, 0, stream>>>(marginal, conditional, w, h, total_out, pdf);
+  env_alias_kernel<<<(h + 1 + 63) / 64, 64, 0, stream>>>(marginal, conditional, w, h, alias_q, alias_idx, cond_alias,
+                                                        marg_alias);
   return cudaGetLastError();
 }
 
