@@ -64,6 +64,18 @@ __device__ __forceinline__ uint32_t pack_bf16x2(float lo, float hi) {
   const __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
   return *reinterpret_cast<const uint32_t*>(&v);
 }
+// max(lo, 0) and max(hi, 0) rounded to BF16 and packed, in one conversion (the ReLU of the
+// hidden layers). The first source operand goes to the upper half.
+__device__ __forceinline__ uint32_t pack_relu_bf16x2(float lo, float hi) {
+  uint32_t r;
+  asm("cvt.rn.relu.bf16x2.f32 %0, %1, %2;" : "=r"(r) : "f"(hi), "f"(lo));
+  return r;
+}
+__device__ __forceinline__ float tanh_fast(float x) {
+  float r;
+  asm("tanh.approx.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
 
 // Encoding of one query written as row `row` of a K = 80 K-major tile (row-group stride 1280 B).
 __device__ void encode_row(uint8_t* tile, int row, bool valid, float px, float py, float pz, float nx, float ny,
@@ -125,12 +137,12 @@ __device__ __forceinline__ void epilogue_hidden(uint32_t lane_tmem, const float*
     for (int h = 0; h < 2; ++h) {
       float r[8];
 #pragma unroll
-      for (int j = 0; j < 8; ++j) r[j] = fmaxf(v[8 * h + j] + bias[c + 8 * h + j], 0.0f);
+      for (int j = 0; j < 8; ++j) r[j] = v[8 * h + j] + bias[c + 8 * h + j];
       uint4 o;
-      o.x = pack_bf16x2(r[0], r[1]);
-      o.y = pack_bf16x2(r[2], r[3]);
-      o.z = pack_bf16x2(r[4], r[5]);
-      o.w = pack_bf16x2(r[6], r[7]);
+      o.x = pack_relu_bf16x2(r[0], r[1]);
+      o.y = pack_relu_bf16x2(r[2], r[3]);
+      o.z = pack_relu_bf16x2(r[4], r[5]);
+      o.w = pack_relu_bf16x2(r[6], r[7]);
       *reinterpret_cast<uint4*>(dst + kmajor_offset(row, c + 8 * h, 64)) = o;
     }
   }
@@ -187,11 +199,14 @@ __device__ void decode_mixture(const float* y, float4* out) {
   const float inv = 1.0f / wsum;
 #pragma unroll
   for (int j = 0; j < 8; ++j) {
-    const float kappa = expf(fminf(fmaxf(y[4 * j + 1], kKappaLo), kKappaHi));
-    const float ct = tanhf(y[4 * j + 2]);
+    // Hardware approximations (relative error about 2^-11 for tanh, 2^-21 absolute for sin/cos on
+    // [-pi, pi]): the decoded mixture is what both the sampler and its pdf read, so any rounding
+    // here changes the proposal distribution, never the estimator's expectation.
+    const float kappa = __expf(fminf(fmaxf(y[4 * j + 1], kKappaLo), kKappaHi));
+    const float ct = tanh_fast(y[4 * j + 2]);
     const float st = sqrtf(fmaxf(0.0f, 1.0f - ct * ct));
     float sp, cp;
-    sincospif(tanhf(y[4 * j + 3]), &sp, &cp);
+    __sincosf(3.14159265358979f * tanh_fast(y[4 * j + 3]), &sp, &cp);
     out[j] = make_float4(st * cp, st * sp, ct, kappa);
   }
   out[8] = make_float4(w[0] * inv, w[1] * inv, w[2] * inv, w[3] * inv);
