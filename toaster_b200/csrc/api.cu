@@ -635,8 +635,10 @@ int tc_upload_scene(tc_context* ctx, const tc_scene_data* sd) {
     const size_t span = std::max<size_t>(ew, eh);
     TC_CUDA(ctx, ctx->env_alias_cond.reserve(sizeof(uint2) * n));
     TC_CUDA(ctx, ctx->env_alias_marg.reserve(sizeof(uint2) * eh));
-    TC_CUDA(ctx, ctx->env_alias_q.reserve(sizeof(double) * span * (size_t(eh) + 1)));
-    TC_CUDA(ctx, ctx->env_alias_idx.reserve(2 * sizeof(uint32_t) * span * (size_t(eh) + 1)));
+    if (!tcb::env_alias_in_shared(ew, eh)) {
+      TC_CUDA(ctx, ctx->env_alias_q.reserve(sizeof(double) * span * (size_t(eh) + 1)));
+      TC_CUDA(ctx, ctx->env_alias_idx.reserve(2 * sizeof(uint32_t) * span * (size_t(eh) + 1)));
+    }
     TC_CUDA(ctx, tcb::launch_env_tables(ctx->env_rgb.as<float4>(), ew, eh, sd->params.environment_intensity,
                                         ctx->env_marginal.as<float>(), ctx->env_conditional.as<float>(),
                                         ctx->env_pdf.as<float>(), ctx->env_row_sums.as<double>(),

@@ -210,6 +210,11 @@ cudaError_t render_static_scratch(int device, unsigned long long** out);
 cudaError_t launch_resolve(const double* accum, uint32_t pixels, double inv_samples, float4* out,
                            cudaStream_t stream);
 // Environment importance tables from RGB texels; `row_sums` is FP64 scratch of H entries.
+// Whether launch_env_tables builds each alias table in shared memory (max(w, h) x 16 bytes); otherwise
+// it needs alias_q ((h + 1) x max(w, h) doubles) and alias_idx (2 x as many indices).
+inline bool env_alias_in_shared(uint32_t w, uint32_t h) {
+  return size_t(w > h ? w : h) * (sizeof(double) + 2 * sizeof(uint32_t)) <= 200u * 1024u;
+}
 cudaError_t launch_env_tables(const float4* rgb, uint32_t w, uint32_t h, float intensity, float* marginal,
                               float* conditional, float* pdf, double* row_sums, double* total_out,
                               double* alias_q, uint32_t* alias_idx, uint2* cond_alias, uint2* marg_alias,

@@ -1976,39 +1976,47 @@ __global__ void env_pdf_kernel(const float* __restrict__ marginal, const float* 
   pdf[i] = float(p * double(w) * double(h) / (2.0 * CUDART_PI * CUDART_PI));
 }
 
-// Walker alias tables of the importance distribution (Vose's construction, one thread per table):
-// table y < h is row y's distribution over its columns, table h the marginal over rows. The
-// weights are the FP32 CDF differences env_pdf_kernel turns into densities, so the sampler draws
-// each texel with exactly the probability its density reports. An entry is (probability of
-// keeping the drawn index, as float bits; the index taken otherwise). Scratch per table: max(w, h)
-// doubles and 2 x max(w, h) indices.
-__global__ void env_alias_kernel(const float* __restrict__ marginal, const float* __restrict__ conditional, uint32_t w,
-                                 uint32_t h, double* __restrict__ scratch_q, uint32_t* __restrict__ scratch_idx,
-                                 uint2* __restrict__ cond_alias, uint2* __restrict__ marg_alias) {
-  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t > h) return;
+// Walker alias tables of the importance distribution (Vose's construction): table y < h is row
+// y's distribution over its columns, table h the marginal over rows. The weights are the FP32 CDF
+// differences env_pdf_kernel turns into densities, so the sampler draws each texel with exactly the
+// probability its density reports. An entry is (probability of keeping the drawn index, as float
+// bits; the index taken otherwise). One warp per table: the lanes read and sum the weights, lane 0
+// runs the construction (it is sequential) on the table's working set, held in shared memory
+// (max(w, h) doubles and 2 x max(w, h) indices) or, for maps too wide for it, in `scratch_q` /
+// `scratch_idx` (the same amounts per table).
+__global__ void __launch_bounds__(32) env_alias_kernel(const float* __restrict__ marginal,
+                                                       const float* __restrict__ conditional, uint32_t w, uint32_t h,
+                                                       bool in_shared, double* __restrict__ scratch_q,
+                                                       uint32_t* __restrict__ scratch_idx, uint2* __restrict__ cond_alias,
+                                                       uint2* __restrict__ marg_alias) {
+  extern __shared__ __align__(16) uint8_t env_sm[];
+  const uint32_t t = blockIdx.x, lane = threadIdx.x;
   const uint32_t span = max(w, h);
   const bool marg = t == h;
   const uint32_t n = marg ? h : w;
   const float* cdf = marg ? marginal : conditional + size_t(t) * w;
   uint2* out = marg ? marg_alias : cond_alias + size_t(t) * w;
-  double* q = scratch_q + size_t(t) * span;
-  uint32_t* small = scratch_idx + size_t(t) * 2 * span;
+  double* q = in_shared ? reinterpret_cast<double*>(env_sm) : scratch_q + size_t(t) * span;
+  uint32_t* small = in_shared ? reinterpret_cast<uint32_t*>(q + span) : scratch_idx + size_t(t) * 2 * span;
   uint32_t* large = small + span;
-  double sum = 0.0;
-  for (uint32_t i = 0; i < n; ++i) {
+  double part = 0.0;
+  for (uint32_t i = lane; i < n; i += 32) {
     const double p = fmax(double(cdf[i]) - (i ? double(cdf[i - 1]) : 0.0), 0.0);
     q[i] = p;
-    sum += p;
+    part += p;
   }
+  for (int o = 16; o > 0; o >>= 1) part += __shfl_xor_sync(0xffffffffu, part, o);
+  const double sum = part;
   if (!(sum > 0.0) || !isfinite(sum)) {
-    for (uint32_t i = 0; i < n; ++i) out[i] = make_uint2(__float_as_uint(1.0f), i);
+    for (uint32_t i = lane; i < n; i += 32) out[i] = make_uint2(__float_as_uint(1.0f), i);
     return;
   }
   const double scale = double(n) / sum;
+  for (uint32_t i = lane; i < n; i += 32) q[i] *= scale;
+  __syncwarp();
+  if (lane != 0) return;
   uint32_t ns = 0, nl = 0;
   for (uint32_t i = 0; i < n; ++i) {
-    q[i] *= scale;
     if (q[i] < 1.0) small[ns++] = i;
     else large[nl++] = i;
   }
@@ -2039,8 +2047,16 @@ cudaError_t launch_env_tables(const float4* rgb, uint32_t w, uint32_t h, float i
   env_marginal_kernel<<<1, kEnvBlock, 0, stream>>>(row_sums, h, marginal, total_out);
   const size_t n = size_t(w) * h;
   env_pdf_kernel<<<unsigned((n + 255) / 256), 256, 0, stream>>>(marginal, conditional, w, h, total_out, pdf);
-  env_alias_kernel<<<(h + 1 + 63) / 64, 64, 0, stream>>>(marginal, conditional, w, h, alias_q, alias_idx, cond_alias,
-                                                        marg_alias);
+  // The working set of one table in shared memory when it fits (maps up to 12,800 texels wide).
+  const size_t table_bytes = size_t(std::max(w, h)) * (sizeof(double) + 2 * sizeof(uint32_t));
+  const bool in_shared = env_alias_in_shared(w, h);
+  if (in_shared) {
+    const cudaError_t e =
+        cudaFuncSetAttribute(env_alias_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(table_bytes));
+    if (e != cudaSuccess) return e;
+  }
+  env_alias_kernel<<<h + 1, 32, in_shared ? table_bytes : 0, stream>>>(marginal, conditional, w, h, in_shared,
+                                                                       alias_q, alias_idx, cond_alias, marg_alias);
   return cudaGetLastError();
 }
 
