@@ -225,15 +225,27 @@ __global__ void __launch_bounds__(128, 1) guide_infer_kernel(const float4* __res
   uint8_t* s_w = smem;
   uint8_t* s_a = smem + kImgFwdBytes;
   float* s_bias = reinterpret_cast<float*>(smem + kImgFwdBytes + 128 * 80 * 2);
-  __shared__ __align__(8) uint64_t mbar;
+  __shared__ __align__(8) uint64_t mbar, mbar_w;
   __shared__ uint32_t tmem_base;
   const int tid = threadIdx.x, warp = tid >> 5;
-  for (int i = tid; i < int(kImgFwdBytes / 16); i += 128)
-    reinterpret_cast<uint4*>(s_w)[i] = reinterpret_cast<const uint4*>(img)[i];
-  for (int i = tid; i < 224; i += 128) s_bias[i] = biases[i];
+  // The weight images and biases arrive by two bulk copies completing on mbar_w.
+  if (tid == 0) {
+    umma::mbar_init(&mbar, 1);
+    umma::mbar_init(&mbar_w, 1);
+    umma::fence_mbar_init();
+    umma::mbar_arrive_expect_tx(&mbar_w, kImgFwdBytes + 224 * 4);
+    umma::bulk_copy_g2s(s_w, img, kImgFwdBytes, &mbar_w);
+    umma::bulk_copy_g2s(s_bias, biases, 224 * 4, &mbar_w);
+  }
   if (warp == 0) umma::tmem_alloc(&tmem_base, 64);
-  if (tid == 0) umma::mbar_init(&mbar, 1);
   sync_for_mma();
+  if (!__syncthreads_and(umma::mbar_wait(&mbar_w, 0))) {
+    if (tid == 0) atomicExch(status, 1);
+    umma::fence_before_sync();
+    __syncthreads();
+    if (warp == 0) umma::tmem_dealloc(tmem_base, 64);
+    return;
+  }
   const uint32_t tmem = tmem_base;
   const uint32_t lane_tmem = tmem + (uint32_t(warp * 32) << 16);
   uint32_t phase = 0;
@@ -413,20 +425,30 @@ __global__ void __launch_bounds__(128, 1) guide_train_kernel(const float4* __res
   uint8_t* s_dz = smem + kTrainDZ;
   float* s_bias = reinterpret_cast<float*>(smem + kTrainBias);
   float* s_db = reinterpret_cast<float*>(smem + kTrainDB);
-  __shared__ __align__(8) uint64_t mbar;
+  __shared__ __align__(8) uint64_t mbar, mbar_w;
   __shared__ uint32_t tmem_base;
   __shared__ float s_loss;
   const int tid = threadIdx.x, warp = tid >> 5;
-  for (int i = tid; i < int(kImgBytes / 16); i += 128)
-    reinterpret_cast<uint4*>(s_w)[i] = reinterpret_cast<const uint4*>(img)[i];
-  for (int i = tid; i < 224; i += 128) {
-    s_bias[i] = biases[i];
-    s_db[i] = 0.0f;
+  // The weight images (forward and transposed) and biases arrive by two bulk copies completing on mbar_w.
+  if (tid == 0) {
+    umma::mbar_init(&mbar, 1);
+    umma::mbar_init(&mbar_w, 1);
+    umma::fence_mbar_init();
+    umma::mbar_arrive_expect_tx(&mbar_w, kImgBytes + 224 * 4);
+    umma::bulk_copy_g2s(s_w, img, kImgBytes, &mbar_w);
+    umma::bulk_copy_g2s(s_bias, biases, 224 * 4, &mbar_w);
+    s_loss = 0.0f;
   }
-  if (tid == 0) s_loss = 0.0f;
+  for (int i = tid; i < 224; i += 128) s_db[i] = 0.0f;
   if (warp == 0) umma::tmem_alloc(&tmem_base, 512);
-  if (tid == 0) umma::mbar_init(&mbar, 1);
   sync_for_mma();
+  if (!__syncthreads_and(umma::mbar_wait(&mbar_w, 0))) {
+    if (tid == 0) atomicExch(status, 1);
+    umma::fence_before_sync();
+    __syncthreads();
+    if (warp == 0) umma::tmem_dealloc(tmem_base, 512);
+    return;
+  }
   const uint32_t tmem = tmem_base;
   const uint32_t lane = uint32_t(warp * 32) << 16;
   uint32_t phase = 0;

@@ -99,6 +99,22 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, uint32
     if (mbar_try_wait(bar, parity)) return true;
   return false;
 }
+// Makes an initialised mbarrier visible to the asynchronous (bulk copy) proxy.
+__device__ __forceinline__ void fence_mbar_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+// Arrives on `bar` (one of its expected arrivals) and adds `bytes` to the transaction count the
+// current phase waits for.
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes) : "memory");
+}
+// Bulk asynchronous copy (no tensor map, no multicast) of `bytes` from this GPU's global memory to
+// this CTA's shared memory, completing as transaction bytes on `bar`. Both addresses 16-byte
+// aligned, `bytes` a multiple of 16.
+__device__ __forceinline__ void bulk_copy_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(smem_addr(dst)),
+      "l"(src), "r"(bytes), "r"(smem_addr(bar))
+      : "memory");
+}
 
 // Offset of element (r, k) in the canonical K-major layout with LBO = 128 B (K groups adjacent)
 // and SBO = (k_extent / 8) * 128 B.
