@@ -271,18 +271,21 @@ int tc_update_geometry(tc_context* ctx, const tc_scene_data* scene, const tc_sce
  * path_tracer.rs:900-923). options may be NULL. */
 int tc_render(tc_context* ctx, const tc_gpu_render_params* params, const tc_render_options* options);
 
-/* One persistent launch over n independent frames of possibly different scenes and sizes:
- * contexts[i] holds scene i (from tc_upload_scene) and renders params[i] under the same
- * progressive contract as tc_render. Work items of all frames share one queue, so small frames
- * fill the GPU together instead of one launch (and one tail) each. No reference counterpart: the
- * reference renders scenes one dispatch at a time (dispatch.rs:28-60). All contexts must be on
- * one device and distinct; the launch runs on contexts[0]'s stream after the others' pending
- * work, and tc_get_stats(contexts[0]) reports the whole batch. Options may set block_size and
- * samples_per_item; moments and recording are rejected. With options->guiding every context needs
- * guide parameters (tc_guide_set_params) and all frames one sample count: the batch then runs the
- * guided wavefront over all frames at once, in waves of whole samples per pixel (wave_paths, 0 =
- * 2^23 paths), each frame's suspended paths in a region of their own that the frame's own
- * network infers. Synchronous. */
+/* n independent frames of possibly different scenes and sizes: contexts[i] holds scene i (from
+ * tc_upload_scene) and renders params[i] under the same progressive contract as tc_render. Frames
+ * too small to fill the GPU share one persistent launch: their work items share one queue, so
+ * they fill the GPU together instead of one launch (and one tail) each. With options->schedule
+ * TC_SCHEDULE_AUTO, a frame of at least 2^20 paths (which fills the GPU by itself) is rendered by
+ * its own wavefront call instead, after the shared launch; TC_SCHEDULE_MEGAKERNEL puts every frame
+ * in the shared launch, TC_SCHEDULE_WAVEFRONT every frame with at least one bounce in a call of its own.
+ * No reference counterpart: the reference renders scenes one dispatch at a time
+ * (dispatch.rs:28-60). All contexts must be on one device and distinct; the work runs on
+ * contexts[0]'s stream after the others' pending work, and tc_get_stats(contexts[0]) reports the
+ * whole batch. Options may set block_size and samples_per_item; moments and recording are
+ * rejected. With options->guiding every context needs guide parameters (tc_guide_set_params); the
+ * frames of the shared launch need one sample count and run the guided wavefront over all of them
+ * at once, in waves of whole samples per pixel (wave_paths, 0 = 2^23 paths), each frame's
+ * suspended paths in a region of their own that the frame's own network infers. Synchronous. */
 int tc_render_batch(tc_context* const* contexts, const tc_gpu_render_params* params, size_t n,
                     const tc_render_options* options);
 

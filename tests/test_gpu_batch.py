@@ -48,6 +48,29 @@ def test_batch_matches_individual_renders(native_lib):
             r.close()
 
 
+def test_batch_gives_large_frames_their_own_wavefront_call(native_lib):
+    # A frame of 2^20 paths fills the GPU by itself: the automatic schedule renders it with a
+    # wavefront call of its own and the small frames in the shared launch; either way every frame
+    # takes its own paths, so each matches its own single render.
+    sc = [configs.mixed(width=1024, height=1024, samples=1), configs.plain_small(),
+          configs.room_with_window(width=96, height=54, samples=4, clutter=1024)]
+    rs = [GpuRenderer(0) for _ in sc]
+    try:
+        for r, s in zip(rs, sc):
+            r.upload(scene_to_gpu(s))
+        for schedule, single in (("auto", ["wavefront", "auto", "auto"]), ("megakernel", ["megakernel"] * 3)):
+            st = render_batch(rs, frame_index=21, schedule=schedule)
+            assert st["paths"] == sum(s.width * s.height * s.samples for s in sc)
+            assert (st["kernel_launches"] > 1) == (schedule == "auto")
+            batched = [r.readback_sums()[0] for r in rs]
+            for r, b, one in zip(rs, batched, single):
+                r.render(frame_index=21, schedule=one)
+                assert close(b, r.readback_sums()[0]) > 0.999
+    finally:
+        for r in rs:
+            r.close()
+
+
 def test_batch_rejects_duplicates_and_options(native_lib):
     r = GpuRenderer(0)
     try:

@@ -56,8 +56,10 @@ def host_display_rgba8(hdr: np.ndarray, exposure_stops: float = 0.0) -> np.ndarr
 
 def uneven(count: int = 16, samples: int = 32, max_bounces: int = 8, repeats: int = 3, device: int = 0,
            min_width: int = 320, max_width: int = 1280) -> dict:
-    """One batched launch over `count` uneven scenes against one launch per scene: device time of
-    the path kernels (CUDA events) and host time of the synchronous calls (each call waits)."""
+    """One batched call over `count` uneven scenes against one call per scene: device time of
+    the path kernels (CUDA events) and host time of the synchronous calls (each call waits). The
+    batched call runs with the automatic schedule (frames of 2^20 paths or more in wavefront calls
+    of their own) and as one shared launch of the megakernel over every frame."""
     scenes = configs.uneven_batch(count=count, samples=samples, max_bounces=max_bounces, min_width=min_width,
                                   max_width=max_width)
     rs = [GpuRenderer(device) for _ in scenes]
@@ -65,13 +67,19 @@ def uneven(count: int = 16, samples: int = 32, max_bounces: int = 8, repeats: in
         for r, s in zip(rs, scenes):
             r.upload(scene_to_gpu(s))
         paths = sum(s.width * s.height * s.samples for s in scenes)
-        render_batch(rs, frame_index=0)  # warm-up
-        batched, batched_host = [], []
-        for k in range(repeats):
-            t0 = time.perf_counter()
-            st = render_batch(rs, frame_index=1 + k)
-            batched_host.append((time.perf_counter() - t0) * 1e3)
-            batched.append(st["kernel_ms"])
+
+        def batched_run(schedule):
+            render_batch(rs, frame_index=0, schedule=schedule)  # warm-up
+            dev, host = [], []
+            for k in range(repeats):
+                t0 = time.perf_counter()
+                st = render_batch(rs, frame_index=1 + k, schedule=schedule)
+                host.append((time.perf_counter() - t0) * 1e3)
+                dev.append(st["kernel_ms"])
+            return float(np.median(dev)), float(np.median(host))
+
+        b, bh = batched_run("auto")
+        b1, b1h = batched_run("megakernel")
         for r in rs:
             r.render(frame_index=0)
         single, single_host = [], []
@@ -83,13 +91,13 @@ def uneven(count: int = 16, samples: int = 32, max_bounces: int = 8, repeats: in
                 tot += r.stats()["kernel_ms"]
             single_host.append((time.perf_counter() - t0) * 1e3)
             single.append(tot)
-        b, u = float(np.median(batched)), float(np.median(single))
-        bh, uh = float(np.median(batched_host)), float(np.median(single_host))
+        u, uh = float(np.median(single)), float(np.median(single_host))
         return {"scenes": count, "triangles": [s.triangle_count for s in scenes],
                 "resolutions": [f"{s.width}x{s.height}" for s in scenes], "spp": samples, "max_bounces": max_bounces,
                 "paths": paths, "batched_ms": b, "unbatched_ms": u, "batched_mpaths_per_s": paths / (b * 1e3),
                 "unbatched_mpaths_per_s": paths / (u * 1e3), "speedup": u / b,
-                "batched_host_ms": bh, "unbatched_host_ms": uh, "host_speedup": uh / bh}
+                "batched_host_ms": bh, "unbatched_host_ms": uh, "host_speedup": uh / bh,
+                "one_launch_ms": b1, "one_launch_mpaths_per_s": paths / (b1 * 1e3), "one_launch_host_ms": b1h}
     finally:
         for r in rs:
             r.close()
@@ -117,6 +125,9 @@ def uneven_guided(count: int = 16, samples: int = 32, max_bounces: int = 8, repe
         paths = sum(s.width * s.height * s.samples for s in scenes)
         render_batch(rs, frame_index=1, guiding=True)  # warm-up
         batched = [render_batch(rs, frame_index=2 + k, guiding=True)["kernel_ms"] for k in range(repeats)]
+        render_batch(rs, frame_index=1, guiding=True, schedule="megakernel")
+        one_launch = [render_batch(rs, frame_index=2 + k, guiding=True, schedule="megakernel")["kernel_ms"]
+                      for k in range(repeats)]
         per_scene = {"guided": [], "plain": []}
         totals = {"guided": [], "plain": []}
         for key, guided in (("guided", True), ("plain", False)):
@@ -134,6 +145,8 @@ def uneven_guided(count: int = 16, samples: int = 32, max_bounces: int = 8, repe
         g, pl = float(np.median(totals["guided"])), float(np.median(totals["plain"]))
         return {"scenes": count, "spp": samples, "max_bounces": max_bounces, "paths": paths,
                 "train_ms_all_scenes": train_ms, "batched_guided_ms": b, "unbatched_guided_ms": g,
+                "one_launch_guided_ms": float(np.median(one_launch)),
+                "one_launch_guided_mpaths_per_s": paths / (float(np.median(one_launch)) * 1e3),
                 "unbatched_plain_ms": pl, "batched_guided_mpaths_per_s": paths / (b * 1e3),
                 "unbatched_guided_mpaths_per_s": paths / (g * 1e3), "unbatched_plain_mpaths_per_s": paths / (pl * 1e3),
                 "guided_scene_ms_p50": float(np.percentile(per_scene["guided"], 50)),

@@ -1095,6 +1095,10 @@ int tc_render(tc_context* ctx, const tc_gpu_render_params* p, const tc_render_op
   return finish_render_stats(ctx, counters, uint64_t(p->width) * p->height * p->samples, true);
 }
 
+static int render_batch_shared(tc_context* lead, tc_context* const* contexts, const tc_gpu_render_params* params,
+                               const std::vector<size_t>& idx, const tc_render_options& o, int block, cudaStream_t st,
+                               unsigned long long* counters_host, uint64_t* paths_out, uint32_t* launches_out);
+
 int tc_render_batch(tc_context* const* contexts, const tc_gpu_render_params* params, size_t n,
                     const tc_render_options* opt) {
   if (!contexts || !params || n == 0) return fail(nullptr, TC_ERR_INVALID, "batch is empty or null");
@@ -1125,26 +1129,101 @@ int tc_render_batch(tc_context* const* contexts, const tc_gpu_render_params* par
     }
     if (o.guiding && !c->has_guide)
       return fail(lead, TC_ERR_STATE, "frame " + std::to_string(i) + ": guided rendering needs tc_guide_set_params first");
-    if (o.guiding && params[i].samples != params[0].samples)
-      return fail(lead, TC_ERR_INVALID, "guided batched frames must share one sample count");
   }
+  // Frames of at least kWavefrontMinPaths paths fill the GPU on their own: with the automatic
+  // schedule each of them gets its own wavefront call (on the batch's stream, into its own
+  // context's buffers), and the other frames share one batched launch of the path kernel, where
+  // batching pays (frames too small to fill the SMs). TC_SCHEDULE_MEGAKERNEL puts every frame in
+  // the batched launch, TC_SCHEDULE_WAVEFRONT every frame the wavefront can take (1 to
+  // kWfDepthMask bounces) in its own call.
+  if (o.schedule > TC_SCHEDULE_WAVEFRONT) return fail(lead, TC_ERR_INVALID, "schedule must be 0 (auto), 1 or 2");
+  std::vector<size_t> own, shared;
+  for (size_t i = 0; i < n; ++i) {
+    const uint64_t fp = uint64_t(params[i].width) * params[i].height * params[i].samples;
+    const bool wf_ok = params[i].max_bounces > 0 && params[i].max_bounces <= tcb::kWfDepthMask;
+    const bool wf = wf_ok && (o.schedule == TC_SCHEDULE_WAVEFRONT ||
+                              (o.schedule == TC_SCHEDULE_AUTO && fp >= kWavefrontMinPaths));
+    (wf ? own : shared).push_back(i);
+  }
+  for (size_t i : shared)
+    if (o.guiding && params[i].samples != params[shared[0]].samples)
+      return fail(lead, TC_ERR_INVALID, "guided frames of one batched launch must share one sample count");
   TC_CUDA(lead, cudaSetDevice(lead->device));
   cudaStream_t st = lead->stream;
   TC_CUDA(lead, cudaEventRecord(lead->ev_begin, st));
-  std::vector<tcb::FrameJob> jobs(n);
-  uint64_t items = 0, paths = 0;
   for (size_t i = 0; i < n; ++i) {
     tc_context* c = contexts[i];
-    const tc_gpu_render_params* p = &params[i];
     if (c != lead) {  // the batch writes this context's buffers: order after its own stream
       TC_CUDA(lead, cudaEventRecord(c->ev_begin, c->stream));
       TC_CUDA(lead, cudaStreamWaitEvent(st, c->ev_begin, 0));
     }
+  }
+  TC_CUDA(lead, cudaEventRecord(lead->ev_kernel0, st));
+  uint32_t launches = 0;
+  unsigned long long counters[4] = {0, 0, 0, 0};
+  uint64_t paths = 0;
+  if (!shared.empty())
+    if (int rc = render_batch_shared(lead, contexts, params, shared, o, block, st, counters, &paths, &launches))
+      return rc;
+  // Own wavefront calls after the shared launch (whose counters are already on their way to the host).
+  std::vector<std::array<unsigned long long, 4>> own_counters(own.size());
+  for (size_t k = 0; k < own.size(); ++k) {
+    const size_t i = own[k];
+    tc_context* c = contexts[i];
+    tc_render_options oi = o;
+    oi.schedule = TC_SCHEDULE_WAVEFRONT;
+    if (int rc = enqueue_render(c, &params[i], oi, st, false, nullptr, nullptr, own_counters[k].data())) {
+      if (c != lead) lead->error = "frame " + std::to_string(i) + ": " + c->error;
+      return rc;
+    }
+    launches += c->stats.kernel_launches;
+  }
+  TC_CUDA(lead, cudaEventRecord(lead->ev_kernel1, st));
+  TC_CUDA(lead, cudaEventRecord(lead->ev_end, st));
+  TC_CUDA(lead, cudaStreamSynchronize(st));
+  if (counters[0] != paths)
+    return fail(lead, TC_ERR_DEVICE_STATUS, "batched path kernel completed " + std::to_string(counters[0]) + " of " +
+                                                std::to_string(paths) + " paths");
+  for (size_t k = 0; k < own.size(); ++k) {
+    const size_t i = own[k];
+    const uint64_t fp = uint64_t(params[i].width) * params[i].height * params[i].samples;
+    if (own_counters[k][0] != fp)
+      return fail(lead, TC_ERR_DEVICE_STATUS, "frame " + std::to_string(i) + ": path kernel completed " +
+                                                  std::to_string(own_counters[k][0]) + " of " + std::to_string(fp) +
+                                                  " paths");
+    for (int j = 0; j < 4; ++j) counters[j] += own_counters[k][j];
+  }
+  for (size_t i : shared) contexts[i]->accumulated += params[i].samples;
+  lead->stats.paths = counters[0];
+  lead->stats.extension_rays = counters[1];
+  lead->stats.shadow_rays = counters[2];
+  lead->stats.rays = counters[1] + counters[2];
+  lead->stats.kernel_launches = launches;
+  clear_phase_stats(lead->stats);
+  cudaEventElapsedTime(&lead->stats.kernel_ms, lead->ev_kernel0, lead->ev_kernel1);
+  cudaEventElapsedTime(&lead->stats.total_ms, lead->ev_begin, lead->ev_end);
+  return TC_OK;
+}
+
+// The batched launch over the frames `idx` of a batch (validated by tc_render_batch): one
+// persistent path-kernel launch over all their work items (guided: the suspend -> per-frame
+// inference -> resume rounds). Enqueues on `st`, copies the launch's counters to `counters_host`
+// (stream-ordered), returns the frames' path count and the kernel launches.
+static int render_batch_shared(tc_context* lead, tc_context* const* contexts, const tc_gpu_render_params* params,
+                               const std::vector<size_t>& idx, const tc_render_options& o, int block, cudaStream_t st,
+                               unsigned long long* counters_host, uint64_t* paths_out, uint32_t* launches_out) {
+  const size_t n = idx.size();
+  std::vector<tcb::FrameJob> jobs(n);
+  uint64_t items = 0, paths = 0;
+  for (size_t k = 0; k < n; ++k) {
+    const size_t i = idx[k];
+    tc_context* c = contexts[i];
+    const tc_gpu_render_params* p = &params[i];
     if (int rc = prepare_accumulation(c, p, false, st)) {
       lead->error = "frame " + std::to_string(i) + ": " + c->error;
       return rc;
     }
-    tcb::FrameJob& J = jobs[i];
+    tcb::FrameJob& J = jobs[k];
     J = tcb::FrameJob{};
     J.scene = c->scene;
     J.accum = c->accum.as<double>();
@@ -1164,19 +1243,21 @@ int tc_render_batch(tc_context* const* contexts, const tc_gpu_render_params* par
   // Guided: waves of whole samples per pixel over all frames; frame i owns the region
   // [ws * pix_begin_i, ws * (pix_begin_i + pixels_i)) of the wave's suspended-path buffers.
   uint64_t total_pix = 0;
-  for (size_t i = 0; i < n; ++i) {
-    jobs[i].pix_begin = uint32_t(total_pix);
-    total_pix += uint64_t(params[i].width) * params[i].height;
+  for (size_t k = 0; k < n; ++k) {
+    jobs[k].pix_begin = uint32_t(total_pix);
+    total_pix += uint64_t(params[idx[k]].width) * params[idx[k]].height;
   }
+  const uint32_t spp = params[idx[0]].samples;  // guided batched frames share it
   uint32_t ws = 0, rounds = 0;
   if (o.guiding) {
     const uint32_t wave_cap = o.wave_paths ? o.wave_paths : (1u << 23);
-    ws = uint32_t(std::max<uint64_t>(1, std::min<uint64_t>(params[0].samples, wave_cap / total_pix)));
+    ws = uint32_t(std::max<uint64_t>(1, std::min<uint64_t>(spp, wave_cap / total_pix)));
     if (uint64_t(ws) * total_pix > (1ull << 31)) return fail(lead, TC_ERR_INVALID, "batched guided frames are too large");
-    for (size_t i = 0; i < n; ++i) {
-      jobs[i].wave_offset = ws * jobs[i].pix_begin;
-      jobs[i].wave_capacity = ws * params[i].width * params[i].height;
-      rounds = std::max(rounds, params[i].max_bounces > 1 ? params[i].max_bounces - 1 : 0u);
+    for (size_t k = 0; k < n; ++k) {
+      const tc_gpu_render_params& pk = params[idx[k]];
+      jobs[k].wave_offset = ws * jobs[k].pix_begin;
+      jobs[k].wave_capacity = ws * pk.width * pk.height;
+      rounds = std::max(rounds, pk.max_bounces > 1 ? pk.max_bounces - 1 : 0u);
     }
   }
   TC_CUDA(lead, upload(lead->batch_jobs, jobs.data(), jobs.size(), st));
@@ -1193,11 +1274,10 @@ int tc_render_batch(tc_context* const* contexts, const tc_gpu_render_params* par
   const int per_sm = tcb::render_batch_max_blocks_per_sm(block, o.guiding != 0);
   if (per_sm <= 0) return fail(lead, TC_ERR_CUDA, "batched render kernel cannot be resident with this block size");
   const int grid = per_sm * lead->sm_count;
-  TC_CUDA(lead, cudaEventRecord(lead->ev_kernel0, st));
-  lead->stats.kernel_launches = 0;
+  uint32_t launches = 0;
   if (!o.guiding) {
     TC_CUDA(lead, tcb::launch_render_batch(L, block, grid, st));
-    lead->stats.kernel_launches = 1;
+    launches = 1;
   } else {
     // Rounds of (batched path kernel -> each frame's network infers its frame's queries -> prefix
     // of the per-frame counts -> batched resume), as the single-frame guided wavefront does.
@@ -1217,8 +1297,8 @@ int tc_render_batch(tc_context* const* contexts, const tc_gpu_render_params* par
     L.g.guide_fraction = o.guide_fraction > 0.0f ? o.guide_fraction : 0.5f;
     L.g.capacity = uint32_t(cap);
     L.g.out_query = query;
-    for (uint32_t first = 0; first < params[0].samples; first += ws) {
-      const uint32_t wsz = std::min(ws, params[0].samples - first);
+    for (uint32_t first = 0; first < spp; first += ws) {
+      const uint32_t wsz = std::min(ws, spp - first);
       TC_CUDA(lead, cudaMemsetAsync(counts, 0, sizeof(uint32_t) * (rounds + 1) * n, st));
       tcb::RenderLaunch R = L;
       R.total_items = uint64_t(wsz) * total_pix;
@@ -1229,14 +1309,14 @@ int tc_render_batch(tc_context* const* contexts, const tc_gpu_render_params* par
       R.g.job_out_count = counts;
       TC_CUDA(lead, cudaMemsetAsync(lead->work_counter.ptr, 0, sizeof(unsigned long long), st));
       TC_CUDA(lead, tcb::launch_render_batch(R, block, grid, st, true));
-      lead->stats.kernel_launches += 1 + rounds * uint32_t(n + 2);
+      launches += 1 + rounds * uint32_t(n + 2);
       for (uint32_t r = 0; r < rounds; ++r) {
         std::swap(state_in, state_out);
-        for (size_t i = 0; i < n; ++i)
-          TC_CUDA(lead, tcb::guide_launch_infer(contexts[i]->guide, query + 2 * size_t(jobs[i].wave_offset),
-                                                jobs[i].wave_capacity,
-                                                mix + size_t(tcb::kGuideDecodedF4) * jobs[i].wave_offset,
-                                                lead->sm_count, st, counts + size_t(r) * n + i));
+        for (size_t k = 0; k < n; ++k)
+          TC_CUDA(lead, tcb::guide_launch_infer(contexts[idx[k]]->guide, query + 2 * size_t(jobs[k].wave_offset),
+                                                jobs[k].wave_capacity,
+                                                mix + size_t(tcb::kGuideDecodedF4) * jobs[k].wave_offset,
+                                                lead->sm_count, st, counts + size_t(r) * n + k));
         uint32_t* pre = prefix + size_t(r) * (n + 1);
         TC_CUDA(lead, tcb::launch_job_prefix(counts + size_t(r) * n, L.jobs, uint32_t(n), pre, st));
         R.g.resume = 1;
@@ -1250,22 +1330,10 @@ int tc_render_batch(tc_context* const* contexts, const tc_gpu_render_params* par
       }
     }
   }
-  TC_CUDA(lead, cudaEventRecord(lead->ev_kernel1, st));
-  unsigned long long counters[4] = {0, 0, 0, 0};
-  TC_CUDA(lead, cudaMemcpyAsync(counters, lead->counters.ptr, sizeof(counters), cudaMemcpyDeviceToHost, st));
-  TC_CUDA(lead, cudaEventRecord(lead->ev_end, st));
-  TC_CUDA(lead, cudaStreamSynchronize(st));
-  for (size_t i = 0; i < n; ++i) contexts[i]->accumulated += params[i].samples;
-  lead->stats.paths = counters[0];
-  lead->stats.extension_rays = counters[1];
-  lead->stats.shadow_rays = counters[2];
-  lead->stats.rays = counters[1] + counters[2];
-  clear_phase_stats(lead->stats);
-  cudaEventElapsedTime(&lead->stats.kernel_ms, lead->ev_kernel0, lead->ev_kernel1);
-  cudaEventElapsedTime(&lead->stats.total_ms, lead->ev_begin, lead->ev_end);
-  if (counters[0] != paths)
-    return fail(lead, TC_ERR_DEVICE_STATUS, "batched path kernel completed " + std::to_string(counters[0]) + " of " +
-                                                std::to_string(paths) + " paths");
+  TC_CUDA(lead, cudaMemcpyAsync(counters_host, lead->counters.ptr, 4 * sizeof(unsigned long long),
+                               cudaMemcpyDeviceToHost, st));
+  *paths_out = paths;
+  *launches_out = launches;
   return TC_OK;
 }
 

@@ -73,10 +73,14 @@ class Animation:
 
 def render_batch(renderers, samples=None, frame_index: int = 0, accumulate: bool = False, block_size: int = 0,
                  samples_per_item: int = 0, short_stack: int = 0, refill_lanes: int = 0, guiding: bool = False,
-                 guide_fraction: float = 0.0, wave_paths: int = 0) -> dict:
-    """One persistent launch over the uploaded scenes of several renderers (same device).
+                 guide_fraction: float = 0.0, wave_paths: int = 0, schedule: str = "auto") -> dict:
+    """The uploaded scenes of several renderers (same device) in one call: frames too small to
+    fill the GPU share one persistent launch; with ``schedule`` "auto" a frame of at least 2^20
+    paths gets a wavefront call of its own ("megakernel": every frame in the shared launch,
+    "wavefront": every frame in a call of its own).
 
-    ``samples`` may be one count or one per renderer (one count for all when ``guiding``).
+    ``samples`` may be one count or one per renderer (one count for the shared launch's frames
+    when ``guiding``).
     ``guiding``: every renderer needs guide parameters; each frame's queries go to its own
     network, in rounds of (batched path kernel, per-frame inference, batched resume). Returns the
     batch's stats (paths, rays, kernel and total milliseconds)."""
@@ -104,6 +108,7 @@ def render_batch(renderers, samples=None, frame_index: int = 0, accumulate: bool
     opts.guiding = 1 if guiding else 0
     opts.guide_fraction = guide_fraction
     opts.wave_paths = wave_paths
+    opts.schedule = native.SCHEDULES[schedule]
     native.check(lib, renderers[0]._ctx, lib.tc_render_batch(ctxs, params.ctypes.data, n, ctypes.byref(opts)))
     for i, r in enumerate(renderers):
         r.width, r.height = int(params[i]["width"]), int(params[i]["height"])
