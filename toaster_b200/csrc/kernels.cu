@@ -1,18 +1,28 @@
 // CUDA kernels of the toaster B200 path tracer (sm_100a).
 //
 //   trace_closest_kernel  closest-hit parity hook: one ray per thread, exact traversal
-//   render_kernel         persistent path-tracing megakernel (camera rays, BSDFs, NEE over area
-//                         lights and the environment, MIS, FP64 per-pixel accumulation)
-//   env_* kernels         FP64 prefix sums for the 2-D environment importance distribution
+//   wf_logic_kernel       wavefront schedule, one slot per thread: shadow-ray results, the last
+//                         hit (miss, emission or the slot's material queue), finished paths into
+//                         the FP64 sums, new camera paths in free slots
+//   wf_shade_kernel       wavefront schedule: the material queues in order (BSDF, light and
+//                         environment NEE, the next ray), guided or recording when asked
+//   wf_trace_kernel       wavefront schedule: extension rays then shadow rays, 32 per warp
+//   wf_sort_* kernels     optional ray sorting before tracing (kind, octant, origin bucket)
+//   render_kernel         persistent path-tracing megakernel (small frames, batched launches,
+//                         captured animation frames)
+//   env_* kernels         FP64 prefix sums and Walker alias tables of the environment's
+//                         importance distribution
 //   resolve_kernel        FP64 sums -> linear-HDR float4 averages
 //
-// The estimator is the one of crates/toaster-cpu/src/integrator.rs:99-244, written as an
-// iterative state machine so that every lane issues exactly one ray per loop iteration
+// The estimator is the one of crates/toaster-cpu/src/integrator.rs:99-244. The megakernel writes
+// it as an iterative state machine so that every lane issues exactly one ray per loop iteration
 // (extension, light shadow or environment shadow). All lanes therefore run the traversal loop
 // together. Optionally (the kPause instantiation) a warp pauses it as soon as too few lanes are
 // still traversing: the finished lanes consume their hit and produce their next ray while the
 // others keep their traversal state (dynamic ray fetching). Idle lanes are refilled with new
 // (pixel, sample-range) work items through one warp-aggregated atomic (ballot + popc + shuffle).
+// The wavefront schedule splits the same estimator into the three launches above over per-path
+// state in device memory; both draw a path's random numbers in the same order.
 #include <cuda_runtime.h>
 #include <math_constants.h>
 #include <stdint.h>
