@@ -777,8 +777,9 @@ int tc_set_camera(tc_context* ctx, const tc_gpu_camera* cam) {
   return TC_OK;
 }
 
-// Plain render as a wavefront (tcb::WavefrontLaunch): iterations of logic, shade and trace
-// launches until no slot holds a path and no work is left. The host waits, kWfLag iterations
+// A render as a wavefront (tcb::WavefrontLaunch): plain or guided (the diffuse queue inferred
+// between logic and shade), recording training records when L.g.records is set. Iterations of
+// logic, shade and trace launches until no slot holds a path and no work is left. The host waits, kWfLag iterations
 // behind the last one it enqueued, for the live-slot count of an earlier iteration, so the GPU
 // always has queued work; the iterations launched after the last path finished find nothing to do.
 static int run_wavefront(tc_context* ctx, const tcb::RenderLaunch& L, uint32_t slots, uint32_t max_bounces,
