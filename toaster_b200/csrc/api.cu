@@ -149,6 +149,7 @@ struct tc_context {
   DevBuf wf_state, wf_ray_o, wf_ray_d, wf_thr, wf_rad, wf_rng, wf_hit, wf_nee, wf_shadow_q, wf_ext_q, wf_mat_q, wf_q;
   DevBuf wf_ext_key, wf_shadow_key, wf_sort_counts, wf_sorted;
   uint32_t* wf_live_host = nullptr;
+  unsigned long long* wf_work_host = nullptr;  // the work counter, read back beside each live count
   cudaEvent_t wf_events[kWfRing] = {};
   // Phase timing (tc_render_options.phase_timing): kWfMarks events per iteration of the last
   // wavefront render, wf_marks_used iterations of them recorded.
@@ -460,6 +461,7 @@ int tc_destroy(tc_context* ctx) {
   for (auto& m : ctx->wf_marks)
     for (cudaEvent_t e : m) cudaEventDestroy(e);
   if (ctx->wf_live_host) cudaFreeHost(ctx->wf_live_host);
+  if (ctx->wf_work_host) cudaFreeHost(ctx->wf_work_host);
   if (ctx->jpeg_params) nvjpegEncoderParamsDestroy(ctx->jpeg_params);
   if (ctx->jpeg_state) nvjpegEncoderStateDestroy(ctx->jpeg_state);
   if (ctx->jpeg) nvjpegDestroy(ctx->jpeg);
@@ -807,6 +809,8 @@ static int run_wavefront(tc_context* ctx, const tcb::RenderLaunch& L, uint32_t s
   if (!ctx->wf_live_host) {
     TC_CUDA(ctx, cudaHostAlloc(reinterpret_cast<void**>(&ctx->wf_live_host), sizeof(uint32_t) * kWfRing,
                                cudaHostAllocDefault));
+    TC_CUDA(ctx, cudaHostAlloc(reinterpret_cast<void**>(&ctx->wf_work_host), sizeof(unsigned long long) * kWfRing,
+                               cudaHostAllocDefault));
     for (cudaEvent_t& e : ctx->wf_events) TC_CUDA(ctx, cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
   }
   tcb::WavefrontLaunch w{};
@@ -871,11 +875,14 @@ static int run_wavefront(tc_context* ctx, const tcb::RenderLaunch& L, uint32_t s
     const int k = int(it % kWfRing);
     TC_CUDA(ctx, cudaMemcpyAsync(ctx->wf_live_host + k, w.q + tcb::kWfLive, sizeof(uint32_t), cudaMemcpyDeviceToHost,
                                  st));
+    TC_CUDA(ctx, cudaMemcpyAsync(ctx->wf_work_host + k, L.work_counter, sizeof(unsigned long long),
+                                 cudaMemcpyDeviceToHost, st));
     TC_CUDA(ctx, cudaEventRecord(ctx->wf_events[k], st));
     if (it >= uint64_t(kWfLag)) {
       const int j = int((it - kWfLag) % kWfRing);
       TC_CUDA(ctx, cudaEventSynchronize(ctx->wf_events[j]));
       if (ctx->wf_live_host[j] == 0) break;
+      if (ctx->wf_work_host[j] >= items) w.work_done = 1u;
     }
   }
   return TC_OK;

@@ -159,6 +159,9 @@ struct WavefrontLaunch {
   // Recording: per slot, the scatter record and the environment-NEE record of the diffuse vertex
   // shaded last (kNoNode when none); the next logic launch completes or drops them.
   uint2* rec_ref;
+  // 1 once every work item has been handed out (the host learns it from an earlier iteration's
+  // counter): a logic block with no live slot then has nothing to do.
+  uint32_t work_done;
 };
 // Ray sorting: 2 kinds x 8 direction octants x 64 origin buckets, counted by kWfSortBlocks blocks.
 constexpr int kWfSortBuckets = 64;

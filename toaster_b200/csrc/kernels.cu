@@ -1160,6 +1160,8 @@ __global__ void __launch_bounds__(kWfBlock) wf_logic_kernel(const WavefrontLaunc
     const uint32_t slot = blockIdx.x * blockDim.x + threadIdx.x;
     const bool valid = slot < W.capacity;
     const uint32_t st = valid ? W.state[slot] : 0u;
+    // Once all work is handed out, a block without a live slot starts and finishes nothing.
+    if (W.work_done && !__syncthreads_or((st & kWfAlive) != 0u)) return;
     bool free_slot = valid && !(st & kWfAlive);
     int kind = -1;
     if (st & kWfAlive) {
