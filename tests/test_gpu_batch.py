@@ -140,6 +140,30 @@ def test_guided_batch_matches_individual_guided_renders(native_lib):
             r.close()
 
 
+def test_guided_batch_with_a_large_frame(native_lib):
+    # The 2^20-path frame gets a guided wavefront call of its own, the small frame the shared
+    # guided launch; only the shared launch's frames need one sample count.
+    from toaster_b200 import guiding_eval
+
+    sc = [configs.mixed(width=1024, height=1024, samples=1),
+          configs.room_with_window(width=64, height=36, samples=8, clutter=1024)]
+    rs = [GpuRenderer(0) for _ in sc]
+    try:
+        for i, (r, s) in enumerate(zip(rs, sc)):
+            r.upload(scene_to_gpu(s))
+            r.guide_set_params(guiding_eval.initial_params(5 + i), configs.scene_bounds(s))
+        st = render_batch(rs, frame_index=5, guiding=True)
+        assert st["paths"] == sum(s.width * s.height * s.samples for s in sc)
+        batched = [r.readback_sums()[0] for r in rs]
+        for r, b, schedule in zip(rs, batched, ("wavefront", "auto")):
+            r.render(frame_index=5, guiding=True, schedule=schedule)
+            assert close(b, r.readback_sums()[0]) > 0.999
+            assert b.sum() > 0
+    finally:
+        for r in rs:
+            r.close()
+
+
 def test_guided_batch_needs_networks_and_one_sample_count(native_lib):
     from toaster_b200 import guiding_eval
 
